@@ -1,0 +1,1150 @@
+/*
+ * mg_host.c -- C host layer of the B200 multigrid Poisson--Helmholtz solver.
+ *
+ * Grid and field management (the device counterpart of grid/multigrid.h and
+ * grid/cartesian-common.h), and the control flow of Basilisk's poisson.h:
+ * poisson() (poisson.h:402-441), mg_solve() (poisson.h:139-235) and
+ * mg_cycle() (poisson.h:32-90).  Every arithmetic operation on field data
+ * runs on the device through the launchers of mg_kernels.cu; this file only
+ * sequences them, adapts nrelax and reads one 8-byte residual maximum back
+ * per cycle.  There is no CPU fallback: without a CUDA device every entry
+ * point fails with BMG_ENODEV.
+ */
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <math.h>
+#include <cuda_runtime_api.h>
+
+#include "basilisk_mg.h"
+#include "mg_launch.h"
+
+int NITERMAX = 100, NITERMIN = 1;   /* poisson.h:102 */
+double TOLERANCE = 1e-3;            /* poisson.h:103 */
+
+static __thread int last_error = BMG_OK;
+static bmg_grid * current_grid = NULL;
+
+#define XO64 4
+#define XO32 8
+
+typedef struct {
+  int used;
+  int face_dim;         /* -1: cell field; d: component d of a face vector */
+  int is_const;
+  double cval;
+  double * buf;         /* all levels */
+  double * lv[BMG_MAXLEVEL + 1];
+  int bctype[6];
+  double bccval[6];
+  double * bcval[6];    /* device, n^(dim-1) values of the finest level */
+} field_t;
+
+struct bmg_grid {
+  int dim, depth, device;
+  double L0, X0, Y0, Z0;
+  int periodic[3];
+  int relax, precision, use_graphs, timing;
+  cudaStream_t stream;
+  int own_stream;
+  bmg_geom g64[BMG_MAXLEVEL + 1], g32[BMG_MAXLEVEL + 1];
+  size_t off64[BMG_MAXLEVEL + 2], off32[BMG_MAXLEVEL + 2];
+  field_t * fields;
+  int nfields, cap;
+  /* workspace (allocated on first solve) */
+  double * ws64;        /* da, da2, res: 3 all-level FP64 arrays */
+  float * ws32;         /* da, da2, res, alpha x/y/z, lambda: FP32 levels */
+  double * bproj;       /* zero-mean copy of b (mixed form, singular problems) */
+  unsigned long long * d_maxres;
+  double * d_sum, * d_partials;
+  int npartials;
+  double * h_pinned;
+  bmg_counters counters;
+  cudaEvent_t ev0, ev1;
+  struct graph_entry * graphs;     /* captured V-cycles, see run_cycle() */
+  unsigned long long clock;
+};
+
+const char * bmg_error_string (int s)
+{
+  switch (s) {
+  case BMG_OK: return "ok";
+  case BMG_EINVAL: return "invalid argument";
+  case BMG_ECUDA: return "CUDA runtime error";
+  case BMG_ENOMEM: return "device allocation failed";
+  case BMG_ENAN: return "residual is not finite";
+  case BMG_ENOTCONV: return "tolerance not reached";
+  case BMG_EUNSUPPORTED: return "unsupported callbacks (only bmg_relax/bmg_residual run on the device)";
+  case BMG_ENODEV: return "no CUDA device";
+  }
+  return "unknown status";
+}
+
+int bmg_last_error (void) { return last_error; }
+
+static int fail (int s) { last_error = s; return s; }
+
+#define CK(call) do { cudaError_t e_ = (call); if (e_ != cudaSuccess) { \
+      fprintf (stderr, "bmg: %s failed: %s (%s:%d)\n", #call,           \
+               cudaGetErrorString (e_), __FILE__, __LINE__);             \
+      return fail (e_ == cudaErrorMemoryAllocation ? BMG_ENOMEM : BMG_ECUDA); } } while (0)
+#define CL(call) do { int e_ = (call); if (e_) { \
+      fprintf (stderr, "bmg: launch %s failed: %s (%s:%d)\n", #call,     \
+               cudaGetErrorString ((cudaError_t) e_), __FILE__, __LINE__); \
+      return fail (BMG_ECUDA); } } while (0)
+
+/* captured V-cycles: the launch sequence of one mg_solve iteration is a
+   pure function of its parameters (cycle_key), so each distinct key is
+   captured once into a CUDA graph and replayed afterwards */
+#define NGRAPH 16
+typedef struct { double bytes; long long launches, sweeps; } work_t;
+struct graph_entry {
+  int valid;
+  unsigned long long stamp;
+  void * key;            /* malloc'd copy of the cycle_key */
+  size_t keylen;
+  cudaGraphExec_t exec;
+  work_t w;
+};
+
+static void graphs_clear (struct bmg_grid * g)
+{
+  if (!g->graphs) return;
+  for (int i = 0; i < NGRAPH; i++)
+    if (g->graphs[i].valid) {
+      cudaGraphExecDestroy (g->graphs[i].exec);
+      free (g->graphs[i].key);
+      g->graphs[i].valid = 0;
+    }
+}
+
+/* ------------------------------------------------------------------ */
+/* geometry                                                            */
+/* ------------------------------------------------------------------ */
+
+static int roundup (int v, int m) { return (v + m - 1)/m*m; }
+
+static bmg_geom make_geom (int dim, int l, int xo, int align)
+{
+  bmg_geom g;
+  memset (&g, 0, sizeof g);
+  g.n = 1 << l;
+  g.xo = xo;
+  g.P = roundup (xo + g.n + 1, align);
+  if (dim == 1) { g.plane = 1; g.size = g.P; }
+  else if (dim == 2) { g.plane = g.P; g.size = (long long) (g.n + 2)*g.P; }
+  else { g.plane = (long long) (g.n + 2)*g.P; g.size = (long long) (g.n + 2)*g.plane; }
+  return g;
+}
+
+static void init_geometry (bmg_grid * g)
+{
+  size_t o64 = 0, o32 = 0;
+  for (int l = 0; l <= g->depth; l++) {
+    g->g64[l] = make_geom (g->dim, l, XO64, 16);
+    g->g32[l] = make_geom (g->dim, l, XO32, 32);
+    g->off64[l] = o64; g->off32[l] = o32;
+    o64 += roundup ((int) 0, 1) + (size_t) ((g->g64[l].size + 63)/64*64);
+    o32 += (size_t) ((g->g32[l].size + 63)/64*64);
+  }
+  g->off64[g->depth + 1] = o64;
+  g->off32[g->depth + 1] = o32;
+}
+
+static size_t total64 (const bmg_grid * g) { return g->off64[g->depth + 1]; }
+static size_t total32 (const bmg_grid * g) { return g->off32[g->depth + 1]; }
+
+static long long ncells (const bmg_grid * g, int l)
+{
+  long long n = 1;
+  for (int d = 0; d < g->dim; d++) n *= (1 << l);
+  return n;
+}
+
+static double delta_of (const bmg_grid * g, int l)
+{
+  return g->L0*(1./(1 << l));    /* cartesian-common.h:11, multigrid.h:14 */
+}
+
+/* ------------------------------------------------------------------ */
+/* grid                                                                */
+/* ------------------------------------------------------------------ */
+
+int bmg_grid_new (bmg_grid ** out, int dim, int depth)
+{
+  if (!out || dim < 1 || dim > 3 || depth < 0 || depth > BMG_MAXLEVEL)
+    return fail (BMG_EINVAL);
+  if (dim == 3 && depth > 10) return fail (BMG_EINVAL);
+  int ndev = 0;
+  if (cudaGetDeviceCount (&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError ();
+    return fail (BMG_ENODEV);
+  }
+  bmg_grid * g = calloc (1, sizeof (bmg_grid));
+  if (!g) return fail (BMG_ENOMEM);
+  g->dim = dim; g->depth = depth; g->L0 = 1.;
+  g->relax = BMG_RELAX_RBGS; g->precision = BMG_FP64; g->use_graphs = 1;
+  CK (cudaGetDevice (&g->device));
+  CK (cudaStreamCreateWithFlags (&g->stream, cudaStreamNonBlocking));
+  g->own_stream = 1;
+  init_geometry (g);
+  g->cap = 16;
+  g->fields = calloc (g->cap, sizeof (field_t));
+  g->nfields = 1;   /* handle 0 means "unset" */
+  CK (cudaMalloc ((void **) &g->d_maxres, 2*sizeof (unsigned long long)));
+  g->npartials = bmg_sum_partials (dim, g->g64[depth]);
+  CK (cudaMalloc ((void **) &g->d_partials, (g->npartials + 1)*sizeof (double)));
+  CK (cudaMalloc ((void **) &g->d_sum, 2*sizeof (double)));
+  CK (cudaMallocHost ((void **) &g->h_pinned, 4*sizeof (double)));
+  CK (cudaEventCreate (&g->ev0));
+  CK (cudaEventCreate (&g->ev1));
+  g->graphs = calloc (NGRAPH, sizeof (struct graph_entry));
+  *out = g;
+  current_grid = g;
+  return fail (BMG_OK);
+}
+
+void bmg_grid_free (bmg_grid * g)
+{
+  if (!g) return;
+  cudaSetDevice (g->device);
+  cudaStreamSynchronize (g->stream);
+  graphs_clear (g);
+  free (g->graphs);
+  for (int i = 1; i < g->nfields; i++)
+    if (g->fields[i].used) {
+      cudaFree (g->fields[i].buf);
+      for (int s = 0; s < 6; s++) cudaFree (g->fields[i].bcval[s]);
+    }
+  free (g->fields);
+  cudaFree (g->ws64); cudaFree (g->ws32); cudaFree (g->bproj);
+  cudaFree (g->d_maxres); cudaFree (g->d_partials); cudaFree (g->d_sum);
+  cudaFreeHost (g->h_pinned);
+  cudaEventDestroy (g->ev0); cudaEventDestroy (g->ev1);
+  if (g->own_stream) cudaStreamDestroy (g->stream);
+  if (current_grid == g) current_grid = NULL;
+  free (g);
+}
+
+int bmg_grid_select (bmg_grid * g) { if (!g) return fail (BMG_EINVAL); current_grid = g; return BMG_OK; }
+bmg_grid * bmg_grid_current (void) { return current_grid; }
+
+int bmg_grid_info (const bmg_grid * g, int * dim, int * depth)
+{
+  if (!g) return fail (BMG_EINVAL);
+  if (dim) *dim = g->dim;
+  if (depth) *depth = g->depth;
+  return BMG_OK;
+}
+
+int bmg_origin (bmg_grid * g, double x, double y, double z)
+{
+  if (!g) return fail (BMG_EINVAL);
+  g->X0 = x; g->Y0 = y; g->Z0 = z;
+  return BMG_OK;
+}
+
+int bmg_size (bmg_grid * g, double L0)
+{
+  if (!g || !(L0 > 0.)) return fail (BMG_EINVAL);
+  g->L0 = L0;
+  return BMG_OK;
+}
+
+static int refresh_bc_ghosts (bmg_grid * g, int h);
+
+/* periodic (cartesian-common.h:920-933): both sides of the direction, for
+   every field of the grid */
+int bmg_periodic (bmg_grid * g, int dir)
+{
+  if (!g || dir < 0 || dir >= 2*g->dim) return fail (BMG_EINVAL);
+  int d = dir/2;
+  g->periodic[d] = 1;
+  for (int i = 1; i < g->nfields; i++)
+    if (g->fields[i].used) {
+      g->fields[i].bctype[2*d] = g->fields[i].bctype[2*d + 1] = BMG_PERIODIC;
+      if (g->fields[i].face_dim < 0 && !g->fields[i].is_const) {
+        int s = refresh_bc_ghosts (g, i);
+        if (s) return s;
+      }
+    }
+  graphs_clear (g);
+  return BMG_OK;
+}
+
+int bmg_set_relax (bmg_grid * g, int relax)
+{
+  if (!g || (relax != BMG_RELAX_RBGS && relax != BMG_RELAX_JACOBI)) return fail (BMG_EINVAL);
+  g->relax = relax;
+  return BMG_OK;
+}
+
+int bmg_set_precision (bmg_grid * g, int p)
+{
+  if (!g || (p != BMG_FP64 && p != BMG_MIXED)) return fail (BMG_EINVAL);
+  g->precision = p;
+  return BMG_OK;
+}
+
+int bmg_set_stream (bmg_grid * g, void * stream)
+{
+  if (!g) return fail (BMG_EINVAL);
+  cudaSetDevice (g->device);
+  cudaStreamSynchronize (g->stream);
+  if (g->own_stream && stream) { cudaStreamDestroy (g->stream); g->own_stream = 0; }
+  if (stream) g->stream = (cudaStream_t) stream;
+  else if (!g->own_stream) {
+    CK (cudaStreamCreateWithFlags (&g->stream, cudaStreamNonBlocking));
+    g->own_stream = 1;
+  }
+  graphs_clear (g);
+  return BMG_OK;
+}
+
+int bmg_synchronize (bmg_grid * g)
+{
+  if (!g) return fail (BMG_EINVAL);
+  CK (cudaStreamSynchronize (g->stream));
+  return BMG_OK;
+}
+
+int bmg_set_graphs (bmg_grid * g, int on) { if (!g) return fail (BMG_EINVAL); g->use_graphs = on; return BMG_OK; }
+int bmg_set_timing (bmg_grid * g, int on) { if (!g) return fail (BMG_EINVAL); g->timing = on; return BMG_OK; }
+
+int bmg_get_counters (bmg_grid * g, bmg_counters * c)
+{
+  if (!g || !c) return fail (BMG_EINVAL);
+  *c = g->counters;
+  return BMG_OK;
+}
+
+int bmg_reset_counters (bmg_grid * g)
+{
+  if (!g) return fail (BMG_EINVAL);
+  memset (&g->counters, 0, sizeof g->counters);
+  return BMG_OK;
+}
+
+/* ------------------------------------------------------------------ */
+/* fields                                                              */
+/* ------------------------------------------------------------------ */
+
+static int new_field (bmg_grid * g, int face_dim, int is_const, double v, int * handle)
+{
+  if (g->nfields == g->cap) {
+    int cap = 2*g->cap;
+    field_t * f = realloc (g->fields, cap*sizeof (field_t));
+    if (!f) return fail (BMG_ENOMEM);
+    memset (f + g->cap, 0, (cap - g->cap)*sizeof (field_t));
+    g->fields = f; g->cap = cap;
+  }
+  int h = g->nfields++;
+  field_t * f = &g->fields[h];
+  memset (f, 0, sizeof *f);
+  f->used = 1; f->face_dim = face_dim; f->is_const = is_const; f->cval = v;
+  for (int s = 0; s < 6; s++)
+    f->bctype[s] = g->periodic[s/2] ? BMG_PERIODIC : BMG_NEUMANN; /* symmetry */
+  if (!is_const) {
+    CK (cudaSetDevice (g->device));
+    CK (cudaMalloc ((void **) &f->buf, total64 (g)*sizeof (double)));
+    CK (cudaMemsetAsync (f->buf, 0, total64 (g)*sizeof (double), g->stream));
+    for (int l = 0; l <= g->depth; l++) f->lv[l] = f->buf + g->off64[l];
+  }
+  *handle = h;
+  return BMG_OK;
+}
+
+static field_t * field_get (bmg_grid * g, int h)
+{
+  if (!g || h <= 0 || h >= g->nfields || !g->fields[h].used) return NULL;
+  return &g->fields[h];
+}
+
+int bmg_scalar_new (bmg_grid * g, bmg_scalar * s)
+{
+  if (!g || !s) return fail (BMG_EINVAL);
+  return new_field (g, -1, 0, 0., &s->i);
+}
+
+int bmg_face_vector_new (bmg_grid * g, bmg_vector * v)
+{
+  if (!g || !v) return fail (BMG_EINVAL);
+  int h[3] = {0, 0, 0};
+  for (int d = 0; d < g->dim; d++) {
+    int s = new_field (g, d, 0, 0., &h[d]);
+    if (s) return s;
+  }
+  v->x.i = h[0]; v->y.i = h[1]; v->z.i = h[2];
+  return BMG_OK;
+}
+
+int bmg_const_scalar (bmg_grid * g, double value, bmg_scalar * s)
+{
+  if (!g || !s) return fail (BMG_EINVAL);
+  return new_field (g, -1, 1, value, &s->i);
+}
+
+int bmg_const_face_vector (bmg_grid * g, double value, bmg_vector * v)
+{
+  if (!g || !v) return fail (BMG_EINVAL);
+  int h[3] = {0, 0, 0};
+  for (int d = 0; d < g->dim; d++) {
+    int s = new_field (g, d, 1, value, &h[d]);
+    if (s) return s;
+  }
+  v->x.i = h[0]; v->y.i = h[1]; v->z.i = h[2];
+  return BMG_OK;
+}
+
+int bmg_field_delete (bmg_grid * g, bmg_scalar s)
+{
+  field_t * f = field_get (g, s.i);
+  if (!f) return fail (BMG_EINVAL);
+  cudaSetDevice (g->device);
+  cudaStreamSynchronize (g->stream);
+  cudaFree (f->buf);
+  for (int k = 0; k < 6; k++) cudaFree (f->bcval[k]);
+  memset (f, 0, sizeof *f);
+  graphs_clear (g);
+  return BMG_OK;
+}
+
+static size_t field_count (const bmg_grid * g, int l, int face_dim)
+{
+  size_t c = 1;
+  for (int d = 0; d < g->dim; d++) c *= (size_t) (1 << l) + (d == face_dim);
+  return c;
+}
+
+/* staging: compact values on the device (copied from the host if needed) */
+static int stage_in (bmg_grid * g, const double * values, size_t count, int memory,
+                     const double ** dptr, double ** tmp)
+{
+  *tmp = NULL;
+  if (memory == BMG_DEVICE) { *dptr = values; return BMG_OK; }
+  CK (cudaMallocAsync ((void **) tmp, count*sizeof (double), g->stream));
+  CK (cudaMemcpyAsync (*tmp, values, count*sizeof (double), cudaMemcpyHostToDevice, g->stream));
+  *dptr = *tmp;
+  return BMG_OK;
+}
+
+static int refresh_bc_ghosts (bmg_grid * g, int h);
+
+int bmg_field_set_level (bmg_grid * g, bmg_scalar s, int level, const double * values,
+                         size_t count, int memory)
+{
+  field_t * f = field_get (g, s.i);
+  if (!f || f->is_const || !values || level < 0 || level > g->depth ||
+      count != field_count (g, level, f->face_dim))
+    return fail (BMG_EINVAL);
+  CK (cudaSetDevice (g->device));
+  const double * d; double * tmp;
+  int st = stage_in (g, values, count, memory, &d, &tmp);
+  if (st) return st;
+  CL (bmg_launch_pack (g->dim, BMG_ST_F64, g->g64[level], f->face_dim, d, f->lv[level], g->stream));
+  if (f->face_dim >= 0 && g->periodic[f->face_dim])
+    /* periodic face vectors: the last face is the image of the first
+       (periodic_boundary_level_x copies face vectors, multigrid.h:644-647) */
+    CL (bmg_launch_face_wrap (g->dim, g->g64[level], f->face_dim, f->lv[level], g->stream));
+  if (tmp) CK (cudaFreeAsync (tmp, g->stream));
+  if (f->face_dim < 0 && level == g->depth) {
+    int r = refresh_bc_ghosts (g, s.i);
+    if (r) return r;
+  }
+  CK (cudaStreamSynchronize (g->stream));
+  return BMG_OK;
+}
+
+int bmg_field_set (bmg_grid * g, bmg_scalar s, const double * values, size_t count, int memory)
+{
+  if (!g) return fail (BMG_EINVAL);
+  return bmg_field_set_level (g, s, g->depth, values, count, memory);
+}
+
+int bmg_field_get_level (bmg_grid * g, bmg_scalar s, int level, double * values,
+                         size_t count, int memory)
+{
+  field_t * f = field_get (g, s.i);
+  if (!f || f->is_const || !values || level < 0 || level > g->depth ||
+      count != field_count (g, level, f->face_dim))
+    return fail (BMG_EINVAL);
+  CK (cudaSetDevice (g->device));
+  double * d = values, * tmp = NULL;
+  if (memory != BMG_DEVICE) {
+    CK (cudaMallocAsync ((void **) &tmp, count*sizeof (double), g->stream));
+    d = tmp;
+  }
+  CL (bmg_launch_unpack (g->dim, g->g64[level], f->face_dim, f->lv[level], d, g->stream));
+  if (tmp) {
+    CK (cudaMemcpyAsync (values, tmp, count*sizeof (double), cudaMemcpyDeviceToHost, g->stream));
+    CK (cudaFreeAsync (tmp, g->stream));
+  }
+  CK (cudaStreamSynchronize (g->stream));
+  return BMG_OK;
+}
+
+int bmg_field_get (bmg_grid * g, bmg_scalar s, double * values, size_t count, int memory)
+{
+  if (!g) return fail (BMG_EINVAL);
+  return bmg_field_get_level (g, s, g->depth, values, count, memory);
+}
+
+static void bcdesc_of (const bmg_grid * g, const field_t * f, bmg_bcdesc * bc)
+{
+  memset (bc, 0, sizeof *bc);
+  for (int d = 0; d < 3; d++) bc->periodic[d] = d < g->dim ? g->periodic[d] : 0;
+  for (int s = 0; s < 6; s++) {
+    bc->type[s] = f ? f->bctype[s] : BMG_NEUMANN;
+    bc->val[s] = f ? f->bcval[s] : NULL;
+    bc->cval[s] = f ? f->bccval[s] : 0.;
+  }
+  bc->Delta = delta_of (g, g->depth);
+}
+
+/* ghosts of a cell field's finest level from its (inhomogeneous) BCs */
+static int refresh_bc_ghosts (bmg_grid * g, int h)
+{
+  field_t * f = &g->fields[h];
+  bmg_bcdesc bc;
+  bcdesc_of (g, f, &bc);
+  CL (bmg_launch_apply_bc (g->dim, BMG_ST_F64, g->g64[g->depth], f->lv[g->depth], &bc, 0, g->stream));
+  return BMG_OK;
+}
+
+int bmg_bc (bmg_grid * g, bmg_scalar s, int side, int type, double value,
+            const double * values, int memory)
+{
+  field_t * f = field_get (g, s.i);
+  if (!f || side < 0 || side >= 2*g->dim ||
+      (type != BMG_NEUMANN && type != BMG_DIRICHLET) || f->face_dim >= 0)
+    return fail (BMG_EINVAL);
+  if (g->periodic[side/2]) return fail (BMG_EINVAL);
+  CK (cudaSetDevice (g->device));
+  f->bctype[side] = type;
+  f->bccval[side] = value;
+  if (f->bcval[side]) { CK (cudaFree (f->bcval[side])); f->bcval[side] = NULL; }
+  if (values) {
+    size_t n = 1;
+    for (int d = 1; d < g->dim; d++) n *= (size_t) 1 << g->depth;
+    CK (cudaMalloc ((void **) &f->bcval[side], n*sizeof (double)));
+    CK (cudaMemcpyAsync (f->bcval[side], values, n*sizeof (double),
+                         memory == BMG_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                         g->stream));
+  }
+  if (!f->is_const) {
+    int r = refresh_bc_ghosts (g, s.i);
+    if (r) return r;
+  }
+  CK (cudaStreamSynchronize (g->stream));
+  graphs_clear (g);
+  return BMG_OK;
+}
+
+/* ------------------------------------------------------------------ */
+/* workspace                                                           */
+/* ------------------------------------------------------------------ */
+
+enum { WS_DA = 0, WS_DA2 = 1, WS_RES = 2 };
+enum { W32_DA = 0, W32_DA2, W32_RES, W32_AX, W32_AY, W32_AZ, W32_LAMBDA, W32_N };
+
+static double * ws64 (bmg_grid * g, int which, int l)
+{
+  return g->ws64 + which*total64 (g) + g->off64[l];
+}
+
+static float * ws32 (bmg_grid * g, int which, int l)
+{
+  return g->ws32 + which*total32 (g) + g->off32[l];
+}
+
+static int ensure_workspace (bmg_grid * g, int mixed)
+{
+  if (!g->ws64) {
+    CK (cudaMalloc ((void **) &g->ws64, 3*total64 (g)*sizeof (double)));
+    CK (cudaMemsetAsync (g->ws64, 0, 3*total64 (g)*sizeof (double), g->stream));
+  }
+  if (mixed && !g->ws32) {
+    CK (cudaMalloc ((void **) &g->ws32, W32_N*total32 (g)*sizeof (float)));
+    CK (cudaMemsetAsync (g->ws32, 0, W32_N*total32 (g)*sizeof (float), g->stream));
+  }
+  return BMG_OK;
+}
+
+/* ------------------------------------------------------------------ */
+/* the solver proper                                                   */
+/* ------------------------------------------------------------------ */
+
+/* coefficients of one solve, per level and storage type */
+typedef struct {
+  bmg_coef alpha64[BMG_MAXLEVEL + 1][3], lambda64[BMG_MAXLEVEL + 1];
+  bmg_coef alpha32[BMG_MAXLEVEL + 1][3], lambda32[BMG_MAXLEVEL + 1];
+  int alpha_stored, lambda_stored;
+} coefs_t;
+
+/* the level arrays a cycle works on */
+typedef struct {
+  void * da[BMG_MAXLEVEL + 1];
+  void * da2[BMG_MAXLEVEL + 1];    /* Jacobi ping-pong partner */
+  void * res[BMG_MAXLEVEL + 1];
+  int st[BMG_MAXLEVEL + 1];        /* storage type of each level */
+} levels_t;
+
+static bmg_geom geom_st (const bmg_grid * g, int l, int st)
+{
+  return st == BMG_ST_F64 ? g->g64[l] : g->g32[l];
+}
+
+static double es_of (int st) { return st == BMG_ST_F64 ? 8. : 4.; }
+
+static int resolve_coefs (bmg_grid * g, bmg_vector alpha, bmg_scalar lambda, coefs_t * c)
+{
+  memset (c, 0, sizeof *c);
+  int ah[3] = {alpha.x.i, alpha.y.i, alpha.z.i};
+  if (!ah[0]) {
+    /* unityf (poisson.h:410-411) */
+    for (int l = 0; l <= g->depth; l++)
+      for (int d = 0; d < 3; d++) { c->alpha64[l][d].c = 1.; c->alpha32[l][d].c = 1.; }
+  }
+  else {
+    for (int d = 0; d < g->dim; d++) {
+      field_t * f = field_get (g, ah[d]);
+      if (!f || f->face_dim != d) return fail (BMG_EINVAL);
+      for (int l = 0; l <= g->depth; l++) {
+        if (f->is_const) { c->alpha64[l][d].c = f->cval; c->alpha32[l][d].c = f->cval; }
+        else c->alpha64[l][d].p = f->lv[l];
+      }
+      if (!f->is_const) c->alpha_stored = 1;
+    }
+  }
+  if (!lambda.i) {
+    for (int l = 0; l <= g->depth; l++) { c->lambda64[l].c = 0.; c->lambda32[l].c = 0.; }
+  }
+  else {
+    field_t * f = field_get (g, lambda.i);
+    if (!f || f->face_dim >= 0) return fail (BMG_EINVAL);
+    for (int l = 0; l <= g->depth; l++) {
+      if (f->is_const) { c->lambda64[l].c = f->cval; c->lambda32[l].c = f->cval; }
+      else c->lambda64[l].p = f->lv[l];
+    }
+    if (!f->is_const) c->lambda_stored = 1;
+  }
+  return BMG_OK;
+}
+
+/* restriction ({alpha, lambda}) (poisson.h:418-420) */
+static int restrict_coefs (bmg_grid * g, const coefs_t * c)
+{
+  for (int l = g->depth - 1; l >= 0; l--) {
+    if (c->alpha_stored) {
+      const double * fine[3] = {0, 0, 0};
+      double * coarse[3] = {0, 0, 0};
+      for (int d = 0; d < g->dim; d++) {
+        fine[d] = (const double *) c->alpha64[l + 1][d].p;
+        coarse[d] = (double *) c->alpha64[l][d].p;
+      }
+      CL (bmg_launch_restrict_face (g->dim, g->g64[l + 1], g->g64[l], fine, coarse, g->stream));
+    }
+    if (c->lambda_stored)
+      CL (bmg_launch_restrict (g->dim, BMG_ST_F64, BMG_ST_F64, g->g64[l + 1], g->g64[l],
+                               c->lambda64[l + 1].p, (void *) c->lambda64[l].p, g->stream));
+  }
+  return BMG_OK;
+}
+
+/* FP32 copies of the coefficients for the inner cycles of the mixed form */
+static int convert_coefs (bmg_grid * g, coefs_t * c)
+{
+  for (int l = 0; l <= g->depth; l++) {
+    for (int d = 0; d < g->dim; d++)
+      if (c->alpha64[l][d].p) {
+        float * dst = ws32 (g, W32_AX + d, l);
+        CL (bmg_launch_convert (g->dim, g->g64[l], g->g32[l], d, c->alpha64[l][d].p, dst, g->stream));
+        c->alpha32[l][d].p = dst;
+      }
+    if (c->lambda64[l].p) {
+      float * dst = ws32 (g, W32_LAMBDA, l);
+      CL (bmg_launch_convert (g->dim, g->g64[l], g->g32[l], -1, c->lambda64[l].p, dst, g->stream));
+      c->lambda32[l].p = dst;
+    }
+  }
+  return BMG_OK;
+}
+
+static double relax_arrays (const bmg_grid * g, const coefs_t * c)
+{
+  return 3. + (c->alpha_stored ? g->dim : 0) + (c->lambda_stored ? 1 : 0);
+}
+
+/* one residual of the finest level into res (storage st); with sync, the
+   maximum is read back into *maxres */
+static int residual_max (bmg_grid * g, field_t * a, const double * b, const coefs_t * c,
+                         void * res, int st, double * maxres, int sync, work_t * w)
+{
+  int L = g->depth;
+  CK (cudaMemsetAsync (g->d_maxres, 0, sizeof (unsigned long long), g->stream));
+  CL (bmg_launch_residual (g->dim, st, g->g64[L], geom_st (g, L, st), a->lv[L], b,
+                           c->alpha64[L], c->lambda64[L], delta_of (g, L), res,
+                           g->d_maxres, g->stream));
+  w->launches += 1;
+  w->bytes += ncells (g, L)*(8.*(2. + (c->alpha_stored ? g->dim : 0) +
+                                 (c->lambda_stored ? 1 : 0)) + es_of (st));
+  if (sync) {
+    CK (cudaMemcpyAsync (g->h_pinned, g->d_maxres, sizeof (double), cudaMemcpyDeviceToHost, g->stream));
+    CK (cudaStreamSynchronize (g->stream));
+    *maxres = g->h_pinned[0];
+  }
+  return BMG_OK;
+}
+
+/* the launches of one mg_cycle (poisson.h:32-90).  Each level's final
+   iterate of da is returned in fin[] (the Jacobi sweeps alternate between
+   the da and da2 buffers). */
+static int cycle_launches (bmg_grid * g, field_t * a, const levels_t * lv, const coefs_t * c,
+                           const bmg_bcdesc * dabc, int nrelax, int minlevel, int maxlevel,
+                           void ** fin, work_t * w)
+{
+  const int dim = g->dim, L = g->depth;
+  cudaStream_t s = g->stream;
+  double bytes = 0.;
+  long long launches = 0, sweeps = 0;
+  /* restriction (res) down to minlevel (multigrid-common.h:368-404) */
+  for (int l = L - 1; l >= minlevel; l--) {
+    CL (bmg_launch_restrict (dim, lv->st[l + 1], lv->st[l], geom_st (g, l + 1, lv->st[l + 1]),
+                             geom_st (g, l, lv->st[l]), lv->res[l + 1], lv->res[l], s));
+    bytes += ncells (g, l + 1)*es_of (lv->st[l + 1]) + ncells (g, l)*es_of (lv->st[l]);
+    launches++;
+  }
+  void * cur[BMG_MAXLEVEL + 1], * oth[BMG_MAXLEVEL + 1];
+  const double narr = relax_arrays (g, c);
+  for (int l = minlevel; l <= maxlevel; l++) {
+    const int st = lv->st[l];
+    const bmg_geom gl = geom_st (g, l, st);
+    cur[l] = lv->da[l]; oth[l] = lv->da2[l];
+    if (l == minlevel) {
+      /* zero on the coarsest level (poisson.h:54-58) */
+      CL (bmg_launch_prolong (dim, st, st, gl, gl, NULL, cur[l], dabc, 1, s));
+      bytes += ncells (g, l)*es_of (st);
+    }
+    else {
+      /* bilinear from the coarser level (poisson.h:64-68) */
+      const int stc = lv->st[l - 1];
+      CL (bmg_launch_prolong (dim, stc, st, geom_st (g, l - 1, stc), gl, cur[l - 1], cur[l], dabc, 0, s));
+      bytes += ncells (g, l - 1)*es_of (stc) + ncells (g, l)*es_of (st);
+    }
+    launches++;
+    const bmg_coef * al = st == BMG_ST_F64 ? c->alpha64[l] : c->alpha32[l];
+    const bmg_coef la = st == BMG_ST_F64 ? c->lambda64[l] : c->lambda32[l];
+    for (int i = 0; i < nrelax; i++) {
+      if (g->relax == BMG_RELAX_JACOBI) {
+        CL (bmg_launch_relax (dim, st, BMG_SWEEP_JACOBI, gl, oth[l], cur[l], lv->res[l], al, la,
+                              delta_of (g, l), dabc, s));
+        void * t = cur[l]; cur[l] = oth[l]; oth[l] = t;
+        launches++;
+      }
+      else {
+        CL (bmg_launch_relax (dim, st, BMG_SWEEP_RED, gl, cur[l], cur[l], lv->res[l], al, la,
+                              delta_of (g, l), dabc, s));
+        CL (bmg_launch_relax (dim, st, BMG_SWEEP_BLACK, gl, cur[l], cur[l], lv->res[l], al, la,
+                              delta_of (g, l), dabc, s));
+        launches += 2;
+      }
+      bytes += narr*ncells (g, l)*es_of (st);
+      sweeps++;
+    }
+  }
+  /* a += da on the finest level, with the BCs of a (poisson.h:84-89) */
+  {
+    bmg_bcdesc abc;
+    bcdesc_of (g, a, &abc);
+    const int st = lv->st[L];
+    CL (bmg_launch_correct (dim, st, g->g64[L], geom_st (g, L, st), a->lv[L], cur[L], &abc, s));
+    bytes += ncells (g, L)*(16. + es_of (st));
+    launches++;
+  }
+  for (int l = 0; l <= L; l++)
+    fin[l] = (l >= minlevel && l <= maxlevel) ? cur[l] : lv->da[l];
+  w->bytes += bytes;
+  w->launches += launches;
+  w->sweeps += sweeps;
+  return BMG_OK;
+}
+
+/* everything that determines the launches of one solver iteration */
+typedef struct {
+  int nrelax, minlevel, relax, precision, dim, depth;
+  cudaStream_t stream;
+  const void * a, * b;
+  levels_t lv;
+  coefs_t c;
+  bmg_bcdesc dabc, abc;
+  const void * maxres, * pinned;
+} cycle_key;
+
+/* one mg_solve iteration: mg_cycle, the residual with its maximum, and the
+   read-back of that maximum into pinned memory; replayed from a CUDA graph
+   when one was captured for the same key. */
+static int run_cycle (bmg_grid * g, field_t * a, const double * bdata, const levels_t * lv,
+                      const coefs_t * c, const bmg_bcdesc * dabc, int nrelax, int minlevel)
+{
+  const int L = g->depth;
+  cycle_key key;
+  memset (&key, 0, sizeof key);
+  key.nrelax = nrelax; key.minlevel = minlevel; key.relax = g->relax;
+  key.precision = g->precision; key.dim = g->dim; key.depth = L;
+  key.stream = g->stream; key.a = a->lv[L]; key.b = bdata;
+  key.lv = *lv; key.c = *c; key.dabc = *dabc;
+  bcdesc_of (g, a, &key.abc);
+  key.maxres = g->d_maxres; key.pinned = g->h_pinned;
+
+  work_t w = {0., 0, 0};
+  void * fin[BMG_MAXLEVEL + 1];
+  if (g->use_graphs) {
+    struct graph_entry * e = NULL, * victim = &g->graphs[0];
+    for (int i = 0; i < NGRAPH; i++) {
+      struct graph_entry * q = &g->graphs[i];
+      if (q->valid && q->keylen == sizeof key && !memcmp (q->key, &key, sizeof key)) { e = q; break; }
+      if (!q->valid || q->stamp < victim->stamp) victim = q;
+    }
+    if (!e) {
+      if (victim->valid) {
+        cudaGraphExecDestroy (victim->exec);
+        free (victim->key);
+        victim->valid = 0;
+      }
+      cudaGraph_t graph;
+      CK (cudaStreamBeginCapture (g->stream, cudaStreamCaptureModeThreadLocal));
+      int r = cycle_launches (g, a, lv, c, dabc, nrelax, minlevel, L, fin, &victim->w);
+      double dummy;
+      if (!r) r = residual_max (g, a, bdata, c, lv->res[L], lv->st[L], &dummy, 0, &victim->w);
+      cudaError_t me = cudaMemcpyAsync (g->h_pinned, g->d_maxres, sizeof (double),
+                                        cudaMemcpyDeviceToHost, g->stream);
+      cudaError_t ee = cudaStreamEndCapture (g->stream, &graph);
+      if (r) return r;
+      CK (me);
+      CK (ee);
+      cudaError_t ie = cudaGraphInstantiate (&victim->exec, graph, 0);
+      cudaGraphDestroy (graph);
+      CK (ie);
+      victim->key = malloc (sizeof key);
+      memcpy (victim->key, &key, sizeof key);
+      victim->keylen = sizeof key;
+      victim->valid = 1;
+      e = victim;
+    }
+    e->stamp = ++g->clock;
+    CK (cudaGraphLaunch (e->exec, g->stream));
+    w = e->w;
+  }
+  else {
+    int r = cycle_launches (g, a, lv, c, dabc, nrelax, minlevel, L, fin, &w);
+    if (r) return r;
+    double dummy;
+    r = residual_max (g, a, bdata, c, lv->res[L], lv->st[L], &dummy, 0, &w);
+    if (r) return r;
+    CK (cudaMemcpyAsync (g->h_pinned, g->d_maxres, sizeof (double), cudaMemcpyDeviceToHost,
+                         g->stream));
+  }
+  g->counters.bytes += w.bytes;
+  g->counters.launches += w.launches;
+  g->counters.sweeps += w.sweeps;
+  return BMG_OK;
+}
+
+static int is_singular (const bmg_grid * g, const field_t * a, const coefs_t * c)
+{
+  if (c->lambda_stored || c->lambda64[g->depth].c != 0.) return 0;
+  for (int s = 0; s < 2*g->dim; s++)
+    if (a->bctype[s] == BMG_DIRICHLET) return 0;
+  return 1;
+}
+
+/* mg_solve (poisson.h:139-235) with the Poisson callbacks */
+static int solve (bmg_grid * g, field_t * a, field_t * b, coefs_t * c, int nrelax,
+                  field_t * resout, int minlevel, double tolerance, mgstats * out)
+{
+  const int L = g->depth;
+  const int mixed = g->precision == BMG_MIXED;
+  int r = ensure_workspace (g, mixed);
+  if (r) return r;
+  if (minlevel > L) minlevel = L;
+  if (minlevel < 0) minlevel = 0;
+  if (mixed) { r = convert_coefs (g, c); if (r) return r; }
+
+  levels_t lv;
+  for (int l = 0; l <= L; l++) {
+    int st = (mixed && l != minlevel) ? BMG_ST_F32 : BMG_ST_F64;
+    lv.st[l] = st;
+    if (st == BMG_ST_F64) {
+      lv.da[l] = ws64 (g, WS_DA, l); lv.da2[l] = ws64 (g, WS_DA2, l); lv.res[l] = ws64 (g, WS_RES, l);
+    }
+    else {
+      lv.da[l] = ws32 (g, W32_DA, l); lv.da2[l] = ws32 (g, W32_DA2, l); lv.res[l] = ws32 (g, W32_RES, l);
+    }
+  }
+  bmg_bcdesc dabc;
+  bcdesc_of (g, a, &dabc);
+
+  mgstats s;
+  memset (&s, 0, sizeof s);
+  /* sum of the r.h.s. (poisson.h:162-167) */
+  CL (bmg_launch_sum (g->dim, g->g64[L], b->lv[L], g->d_partials, g->npartials, g->d_sum, g->stream));
+  CK (cudaMemcpyAsync (g->h_pinned + 1, g->d_sum, sizeof (double), cudaMemcpyDeviceToHost, g->stream));
+  CK (cudaStreamSynchronize (g->stream));
+  s.sum = g->h_pinned[1];
+  s.nrelax = nrelax > 0 ? nrelax : 4;
+
+  /* mixed form, singular problem: FP64 zero-mean projection of b */
+  const double * bdata = b->lv[L];
+  if (mixed && is_singular (g, a, c)) {
+    if (!g->bproj) CK (cudaMalloc ((void **) &g->bproj, g->g64[L].size*sizeof (double)));
+    CK (cudaMemcpyAsync (g->bproj, b->lv[L], g->g64[L].size*sizeof (double),
+                         cudaMemcpyDeviceToDevice, g->stream));
+    CL (bmg_launch_shift (g->dim, g->g64[L], g->bproj, g->d_sum, 1./(double) ncells (g, L), g->stream));
+    bdata = g->bproj;
+  }
+
+  double resb;
+  work_t w0 = {0., 0, 0};
+  r = residual_max (g, a, bdata, c, lv.res[L], lv.st[L], &s.resb, 1, &w0);
+  if (r) return r;
+  resb = s.resa = s.resb;
+  if (tolerance == 0.)
+    tolerance = TOLERANCE;
+  int status = BMG_OK;
+  for (s.i = 0; s.i < NITERMAX && (s.i < NITERMIN || s.resa > tolerance); s.i++) {
+    if (g->timing) CK (cudaEventRecord (g->ev0, g->stream));
+    r = run_cycle (g, a, bdata, &lv, c, &dabc, s.nrelax, minlevel);
+    if (r) return r;
+    if (g->timing) CK (cudaEventRecord (g->ev1, g->stream));
+    CK (cudaStreamSynchronize (g->stream));
+    s.resa = g->h_pinned[0];
+    g->counters.cycles++;
+    if (g->timing) {
+      float ms = 0.f;
+      CK (cudaEventElapsedTime (&ms, g->ev0, g->ev1));
+      g->counters.cycle_ms += ms;
+    }
+    if (!isfinite (s.resa)) { status = BMG_ENAN; s.i++; break; }
+    /* nrelax adaptation (poisson.h:198-204) */
+    if (s.resa > tolerance) {
+      if (resb/s.resa < 1.2 && s.nrelax < 100)
+        s.nrelax++;
+      else if (resb/s.resa > 10 && s.nrelax > 2)
+        s.nrelax--;
+    }
+    resb = s.resa;
+  }
+  s.minlevel = minlevel;
+  if (s.resa > tolerance) {
+    fprintf (stderr,
+             "WARNING: convergence for %s not reached after %d iterations\n"
+             "  res: %g sum: %g nrelax: %d\n", "a",
+             s.i, s.resa, s.sum, s.nrelax), fflush (stderr);
+    if (status == BMG_OK) status = BMG_ENOTCONV;
+  }
+  if (resout && !resout->is_const && resout->face_dim < 0) {
+    if (lv.st[L] == BMG_ST_F64)
+      CK (cudaMemcpyAsync (resout->lv[L], lv.res[L], g->g64[L].size*sizeof (double),
+                           cudaMemcpyDeviceToDevice, g->stream));
+    else {
+      /* widen the FP32 residual: recompute it in FP64 into the caller's field */
+      double dummy;
+      work_t wr = {0., 0, 0};
+      r = residual_max (g, a, bdata, c, resout->lv[L], BMG_ST_F64, &dummy, 0, &wr);
+      if (r) return r;
+    }
+    CK (cudaStreamSynchronize (g->stream));
+  }
+  *out = s;
+  return fail (status);
+}
+
+/* ------------------------------------------------------------------ */
+/* reference-facing entry points                                       */
+/* ------------------------------------------------------------------ */
+
+static int check_cell (bmg_grid * g, int h, field_t ** f)
+{
+  *f = field_get (g, h);
+  if (!*f || (*f)->is_const || (*f)->face_dim >= 0) return fail (BMG_EINVAL);
+  return BMG_OK;
+}
+
+int bmg_poisson (bmg_grid * g, struct Poisson p, mgstats * out)
+{
+  mgstats zero;
+  memset (&zero, 0, sizeof zero);
+  if (out) *out = zero;
+  if (!g || !out) return fail (BMG_EINVAL);
+  CK (cudaSetDevice (g->device));
+  field_t * a, * b, * res = NULL;
+  if (check_cell (g, p.a.i, &a) || check_cell (g, p.b.i, &b)) return fail (BMG_EINVAL);
+  if (p.res && p.res[0].i && check_cell (g, p.res[0].i, &res)) return fail (BMG_EINVAL);
+  coefs_t c;
+  int r = resolve_coefs (g, p.alpha, p.lambda, &c);
+  if (r) return r;
+  r = restrict_coefs (g, &c);
+  if (r) return r;
+  /* TOLERANCE override and restore (poisson.h:426-438) */
+  double defaultol = TOLERANCE;
+  if (p.tolerance)
+    TOLERANCE = p.tolerance;
+  r = solve (g, a, b, &c, p.nrelax, res, p.minlevel > 1 ? p.minlevel : 1, 0., out);
+  if (p.tolerance)
+    TOLERANCE = defaultol;
+  return fail (r);
+}
+
+mgstats poisson (struct Poisson p)
+{
+  mgstats s;
+  bmg_poisson (current_grid, p, &s);
+  return s;
+}
+
+/* bmg_relax / bmg_residual: the Poisson callbacks (poisson.h:271-391) */
+void bmg_relax (bmg_scalar * da, bmg_scalar * res, int l, void * data)
+{
+  bmg_grid * g = current_grid;
+  struct Poisson * p = (struct Poisson *) data;
+  field_t * fa, * fr;
+  if (!g || !p || !da || !res || check_cell (g, da[0].i, &fa) || check_cell (g, res[0].i, &fr) ||
+      l < 0 || l > g->depth) { fail (BMG_EINVAL); return; }
+  coefs_t c;
+  if (resolve_coefs (g, p->alpha, p->lambda, &c)) return;
+  bmg_bcdesc bc;
+  bcdesc_of (g, fa, &bc);
+  if (g->relax == BMG_RELAX_JACOBI) {
+    if (ensure_workspace (g, 0)) return;
+    double * tmp = ws64 (g, WS_DA2, l);
+    if (bmg_launch_relax (g->dim, BMG_ST_F64, BMG_SWEEP_JACOBI, g->g64[l], tmp, fa->lv[l],
+                          fr->lv[l], c.alpha64[l], c.lambda64[l], delta_of (g, l), &bc, g->stream) ||
+        cudaMemcpyAsync (fa->lv[l], tmp, g->g64[l].size*sizeof (double), cudaMemcpyDeviceToDevice,
+                         g->stream) != cudaSuccess) { fail (BMG_ECUDA); return; }
+  }
+  else if (bmg_launch_relax (g->dim, BMG_ST_F64, BMG_SWEEP_RED, g->g64[l], fa->lv[l], fa->lv[l],
+                             fr->lv[l], c.alpha64[l], c.lambda64[l], delta_of (g, l), &bc, g->stream) ||
+           bmg_launch_relax (g->dim, BMG_ST_F64, BMG_SWEEP_BLACK, g->g64[l], fa->lv[l], fa->lv[l],
+                             fr->lv[l], c.alpha64[l], c.lambda64[l], delta_of (g, l), &bc, g->stream)) {
+    fail (BMG_ECUDA); return;
+  }
+  if (cudaStreamSynchronize (g->stream) != cudaSuccess) { fail (BMG_ECUDA); return; }
+  fail (BMG_OK);
+}
+
+double bmg_residual (bmg_scalar * al, bmg_scalar * bl, bmg_scalar * resl, void * data)
+{
+  bmg_grid * g = current_grid;
+  struct Poisson * p = (struct Poisson *) data;
+  field_t * a, * b, * res;
+  if (!g || !p || !al || !bl || !resl || check_cell (g, al[0].i, &a) ||
+      check_cell (g, bl[0].i, &b) || check_cell (g, resl[0].i, &res)) {
+    fail (BMG_EINVAL);
+    return NAN;
+  }
+  coefs_t c;
+  if (resolve_coefs (g, p->alpha, p->lambda, &c)) return NAN;
+  double m = NAN;
+  work_t w = {0., 0, 0};
+  if (residual_max (g, a, b->lv[g->depth], &c, res->lv[g->depth], BMG_ST_F64, &m, 1, &w)) return NAN;
+  fail (BMG_OK);
+  return m;
+}
+
+mgstats mg_solve (struct MGSolve p)
+{
+  mgstats s;
+  memset (&s, 0, sizeof s);
+  bmg_grid * g = current_grid;
+  if (!g || !p.a || !p.b) { fail (BMG_EINVAL); return s; }
+  if (p.residual != bmg_residual || p.relax != bmg_relax || !p.data) {
+    fail (BMG_EUNSUPPORTED);
+    return s;
+  }
+  if (cudaSetDevice (g->device) != cudaSuccess) { fail (BMG_ECUDA); return s; }
+  struct Poisson * pp = (struct Poisson *) p.data;
+  field_t * a, * b, * res = NULL;
+  if (check_cell (g, p.a[0].i, &a) || check_cell (g, p.b[0].i, &b)) return s;
+  if (p.res && p.res[0].i && check_cell (g, p.res[0].i, &res)) return s;
+  coefs_t c;
+  if (resolve_coefs (g, pp->alpha, pp->lambda, &c)) return s;
+  /* mg_solve uses the coefficients as they are on each level; poisson()
+     restricts them beforehand (poisson.h:420) */
+  solve (g, a, b, &c, p.nrelax, res, p.minlevel, p.tolerance, &s);
+  return s;
+}
+
+void mg_cycle (bmg_scalar * al, bmg_scalar * resl, bmg_scalar * dal,
+               void (* relax) (bmg_scalar *, bmg_scalar *, int, void *),
+               void * data, int nrelax, int minlevel, int maxlevel)
+{
+  bmg_grid * g = current_grid;
+  if (!g || !al || !resl || !dal || !data) { fail (BMG_EINVAL); return; }
+  if (relax != bmg_relax) { fail (BMG_EUNSUPPORTED); return; }
+  if (cudaSetDevice (g->device) != cudaSuccess) { fail (BMG_ECUDA); return; }
+  struct Poisson * p = (struct Poisson *) data;
+  field_t * a, * res, * da;
+  if (check_cell (g, al[0].i, &a) || check_cell (g, resl[0].i, &res) ||
+      check_cell (g, dal[0].i, &da)) return;
+  coefs_t c;
+  if (resolve_coefs (g, p->alpha, p->lambda, &c)) return;
+  if (ensure_workspace (g, 0)) return;
+  if (maxlevel > g->depth) maxlevel = g->depth;
+  minlevel = minlevel < maxlevel ? minlevel : maxlevel;   /* poisson.h:48 */
+  if (minlevel < 0) minlevel = 0;
+  levels_t lv;
+  for (int l = 0; l <= g->depth; l++) {
+    lv.st[l] = BMG_ST_F64;
+    lv.da[l] = da->lv[l];
+    lv.da2[l] = ws64 (g, WS_DA2, l);
+    lv.res[l] = res->lv[l];
+  }
+  bmg_bcdesc dabc;
+  bcdesc_of (g, da, &dabc);
+  void * fin[BMG_MAXLEVEL + 1];
+  work_t w = {0., 0, 0};
+  if (cycle_launches (g, a, &lv, &c, &dabc, nrelax, minlevel, maxlevel, fin, &w)) return;
+  /* Jacobi may leave a level's final iterate in the workspace partner */
+  for (int l = minlevel; l <= maxlevel; l++)
+    if (fin[l] != da->lv[l])
+      if (cudaMemcpyAsync (da->lv[l], fin[l], g->g64[l].size*sizeof (double),
+                           cudaMemcpyDeviceToDevice, g->stream) != cudaSuccess) { fail (BMG_ECUDA); return; }
+  if (cudaStreamSynchronize (g->stream) != cudaSuccess) { fail (BMG_ECUDA); return; }
+  g->counters.bytes += w.bytes;
+  g->counters.launches += w.launches;
+  g->counters.sweeps += w.sweeps;
+  g->counters.cycles++;
+  fail (BMG_OK);
+}
+
+int bmg_restriction (bmg_grid * g, const bmg_scalar * list)
+{
+  if (!g || !list) return fail (BMG_EINVAL);
+  CK (cudaSetDevice (g->device));
+  for (const bmg_scalar * s = list; s->i; s++) {
+    field_t * f = field_get (g, s->i);
+    if (!f) return fail (BMG_EINVAL);
+    if (f->is_const) continue;
+    if (f->face_dim >= 0) {
+      /* a face component: restrict the whole vector it belongs to; the
+         components of one vector are consecutive handles */
+      if (f->face_dim != 0) continue;
+      const double * fine[3] = {0, 0, 0};
+      double * coarse[3] = {0, 0, 0};
+      for (int l = g->depth - 1; l >= 0; l--) {
+        for (int d = 0; d < g->dim; d++) {
+          field_t * fd = field_get (g, s->i + d);
+          if (!fd || fd->face_dim != d) return fail (BMG_EINVAL);
+          fine[d] = fd->lv[l + 1]; coarse[d] = fd->lv[l];
+        }
+        CL (bmg_launch_restrict_face (g->dim, g->g64[l + 1], g->g64[l], fine, coarse, g->stream));
+      }
+    }
+    else
+      for (int l = g->depth - 1; l >= 0; l--)
+        CL (bmg_launch_restrict (g->dim, BMG_ST_F64, BMG_ST_F64, g->g64[l + 1], g->g64[l],
+                                 f->lv[l + 1], f->lv[l], g->stream));
+  }
+  CK (cudaStreamSynchronize (g->stream));
+  return fail (BMG_OK);
+}

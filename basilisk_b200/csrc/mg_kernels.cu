@@ -1,0 +1,922 @@
+/*
+ * mg_kernels.cu -- sm_100a stencil kernels of the multigrid
+ * Poisson--Helmholtz solver, and their C launchers.
+ *
+ * One kernel per operation of the reference's V-cycle (Basilisk poisson.h,
+ * grid/multigrid.h, grid/multigrid-common.h), each templated on the
+ * dimension and on the storage type (double for the plain form, float for
+ * the inner cycles of the mixed form):
+ *
+ *   k_relax        relax (poisson.h:271-338): red/black Gauss-Seidel sweep
+ *                  in place, or the -DJACOBI weighted-Jacobi update
+ *                  (poisson.h:325-328) from one buffer into another
+ *   k_prolong      bilinear prolongation (multigrid-common.h:124-140) or the
+ *                  coarsest-level zero (poisson.h:54-58)
+ *   k_restrict     restriction_average (multigrid-common.h:26-32)
+ *   k_restrict_face face_average (multigrid-common.h:42-58)
+ *   k_residual     residual (poisson.h:373-389) fused with the max|res|
+ *                  reduction (warp shuffles, one atomic per block)
+ *   k_correct      a += da (poisson.h:84-89) fused with the boundary
+ *                  conditions of a (the automatic BC of stencils.h:228+)
+ *
+ * Ghost cells are written by the thread that writes the interior cell they
+ * mirror, in the same kernel: box conditions one layer deep in the
+ * reference's side order with corners composed dimension by dimension
+ * (grid/multigrid.h:543-594), periodic images (grid/multigrid.h:638-695),
+ * and the level-0 rule that a periodic level-0 cell is its own neighbour in
+ * every direction (grid/multigrid.h:655-664).  No kernel needs a separate
+ * boundary pass.
+ *
+ * Arithmetic follows the reference's evaluation order; the library is
+ * compiled with --fmad=false so that the FP64 results are bit-identical to
+ * a C build of the same expressions.
+ */
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "mg_launch.h"
+
+namespace {
+
+/* ---------------------------------------------------------------- */
+/* layout                                                            */
+/* ---------------------------------------------------------------- */
+
+template <int DIM>
+__device__ __forceinline__ long long cidx (const bmg_geom & g, int i, int j, int k)
+{
+  if (DIM == 1) return (long long) g.xo + i;
+  if (DIM == 2) return (long long) (i + 1)*g.P + g.xo + j;
+  return (long long) (i + 1)*g.plane + (long long) (j + 1)*g.P + g.xo + k;
+}
+
+template <int DIM>
+__device__ __forceinline__ long long cstride (const bmg_geom & g, int e)
+{
+  if (DIM == 1) return 1;
+  if (DIM == 2) return e == 0 ? (long long) g.P : 1;
+  return e == 0 ? g.plane : e == 1 ? (long long) g.P : 1;
+}
+
+/* thread -> interior cell; the contiguous axis maps to threadIdx.x */
+template <int DIM>
+__device__ __forceinline__ bool cell_of_thread (int n, int & i, int & j, int & k)
+{
+  if (DIM == 1) {
+    i = blockIdx.x*blockDim.x + threadIdx.x; j = k = 0;
+    return i < n;
+  }
+  if (DIM == 2) {
+    j = blockIdx.x*blockDim.x + threadIdx.x;
+    i = blockIdx.y*blockDim.y + threadIdx.y; k = 0;
+    return i < n && j < n;
+  }
+  k = blockIdx.x*blockDim.x + threadIdx.x;
+  j = blockIdx.y*blockDim.y + threadIdx.y;
+  i = blockIdx.z*blockDim.z + threadIdx.z;
+  return i < n && j < n && k < n;
+}
+
+template <int DIM> dim3 block_shape ()
+{
+  if (DIM == 1) return dim3 (256, 1, 1);
+  if (DIM == 2) return dim3 (32, 8, 1);
+  return dim3 (32, 4, 2);
+}
+
+template <int DIM> dim3 grid_shape (int n)
+{
+  dim3 b = block_shape<DIM> ();
+  dim3 g ((n + b.x - 1)/b.x, 1, 1);
+  if (DIM >= 2) g.y = (n + b.y - 1)/b.y;
+  if (DIM >= 3) g.z = (n + b.z - 1)/b.z;
+  return g;
+}
+
+template <typename T>
+struct Coef {
+  const T * p;
+  T c;
+  __device__ __forceinline__ T at (long long id) const { return p ? p[id] : c; }
+};
+
+template <typename T>
+Coef<T> coef_of (const bmg_coef & c)
+{
+  Coef<T> r;
+  r.p = (const T *) c.p;
+  r.c = (T) c.c;
+  return r;
+}
+
+/* homogeneous boundary factors of a field: ghost = fac*cell for box sides
+   (dirichlet_homogeneous -s[], neumann_homogeneous s[], common.h:958,960) */
+struct BCH {
+  int periodic[3];
+  int fac[6];
+};
+
+BCH bch_of (const bmg_bcdesc * bc)
+{
+  BCH h;
+  for (int e = 0; e < 3; e++) h.periodic[e] = bc ? bc->periodic[e] : 0;
+  for (int s = 0; s < 6; s++)
+    h.fac[s] = (bc && bc->type[s] == 1 /* BMG_DIRICHLET */) ? -1 : 1;
+  return h;
+}
+
+template <int DIM>
+__device__ __forceinline__ bool on_boundary (int n, int i, int j, int k)
+{
+  bool b = (i == 0 || i == n - 1);
+  if (DIM > 1) b = b || j == 0 || j == n - 1;
+  if (DIM > 2) b = b || k == 0 || k == n - 1;
+  return b;
+}
+
+/* write the ghost images of cell (i, j, k) of value v, homogeneous BCs */
+template <int DIM, typename T>
+__device__ void ghosts_homog (T * f, const bmg_geom & g, int i, int j, int k,
+                              T v, const BCH & bc)
+{
+  const int n = g.n;
+  if (!on_boundary<DIM> (n, i, j, k)) return;
+  const int c[3] = {i, j, k};
+  int pos[3][3];
+  T fac[3][3];
+  int cnt[3];
+  const bool l0p = (n == 1) && (bc.periodic[0] || bc.periodic[1] || bc.periodic[2]);
+#pragma unroll
+  for (int e = 0; e < 3; e++) {
+    pos[e][0] = c[e]; fac[e][0] = T(1); cnt[e] = 1;
+    if (e < DIM) {
+      if (c[e] == 0) {
+        if (bc.periodic[e]) { pos[e][cnt[e]] = n; fac[e][cnt[e]] = T(1); }
+        else { pos[e][cnt[e]] = -1; fac[e][cnt[e]] = l0p ? T(1) : T(bc.fac[2*e + 1]); }
+        cnt[e]++;
+      }
+      if (c[e] == n - 1) {
+        if (bc.periodic[e]) { pos[e][cnt[e]] = -1; fac[e][cnt[e]] = T(1); }
+        else { pos[e][cnt[e]] = n; fac[e][cnt[e]] = l0p ? T(1) : T(bc.fac[2*e]); }
+        cnt[e]++;
+      }
+    }
+  }
+  for (int a = 0; a < cnt[0]; a++)
+    for (int b = 0; b < cnt[1]; b++)
+      for (int d = 0; d < cnt[2]; d++) {
+        if (a == 0 && b == 0 && d == 0) continue;
+        f[cidx<DIM> (g, pos[0][a], pos[1][b], pos[2][d])] = v*fac[0][a]*fac[1][b]*fac[2][d];
+      }
+}
+
+/* boundary value of side s at the tangential indices of cell (i, j, k) */
+template <int DIM>
+__device__ __forceinline__ double bc_data (const bmg_bcdesc & bc, int s, int n,
+                                           int i, int j, int k)
+{
+  const double * v = bc.val[s];
+  if (!v) return bc.cval[s];
+  int e = s/2;
+  long long t = 0;
+  if (DIM == 2) t = e == 0 ? j : i;
+  if (DIM == 3) t = e == 0 ? (long long) j*n + k : e == 1 ? (long long) i*n + k : (long long) i*n + j;
+  return v[t];
+}
+
+/* ghost images with the inhomogeneous BCs of a field on the finest level:
+   dirichlet 2v - s[], neumann Delta*v + s[] (common.h:957,959), composed
+   dimension by dimension for edges and corners */
+template <int DIM>
+__device__ void ghosts_inhomog (double * f, const bmg_geom & g, int i, int j, int k,
+                                double v, const bmg_bcdesc & bc)
+{
+  const int n = g.n;
+  if (!on_boundary<DIM> (n, i, j, k)) return;
+  const int c[3] = {i, j, k};
+  int pos[3][3], side[3][3], cnt[3];
+  const bool l0p = (n == 1) && (bc.periodic[0] || bc.periodic[1] || bc.periodic[2]);
+#pragma unroll
+  for (int e = 0; e < 3; e++) {
+    pos[e][0] = c[e]; side[e][0] = -1; cnt[e] = 1;
+    if (e < DIM) {
+      if (c[e] == 0) {
+        pos[e][cnt[e]] = bc.periodic[e] ? n : -1;
+        side[e][cnt[e]] = bc.periodic[e] ? -1 : 2*e + 1;
+        cnt[e]++;
+      }
+      if (c[e] == n - 1) {
+        pos[e][cnt[e]] = bc.periodic[e] ? -1 : n;
+        side[e][cnt[e]] = bc.periodic[e] ? -1 : 2*e;
+        cnt[e]++;
+      }
+    }
+  }
+  for (int a = 0; a < cnt[0]; a++)
+    for (int b = 0; b < cnt[1]; b++)
+      for (int d = 0; d < cnt[2]; d++) {
+        if (a == 0 && b == 0 && d == 0) continue;
+        double r = v;
+        if (!l0p) {
+          const int sd[3] = {side[0][a], side[1][b], side[2][d]};
+          for (int e = 0; e < DIM; e++)
+            if (sd[e] >= 0) {
+              double w = bc_data<DIM> (bc, sd[e], n, i, j, k);
+              if (bc.type[sd[e]] == 1 /* BMG_DIRICHLET */)
+                r = 2.*(w) - r;
+              else
+                r = bc.Delta*(w) + r;
+            }
+        }
+        f[cidx<DIM> (g, pos[0][a], pos[1][b], pos[2][d])] = r;
+      }
+}
+
+/* ---------------------------------------------------------------- */
+/* relax                                                             */
+/* ---------------------------------------------------------------- */
+
+/* one cell of relax (poisson.h:303-319) */
+template <int DIM, typename T>
+__device__ __forceinline__ T relax_value (const bmg_geom & g, long long id, const T * in,
+                                          const T * rhs, const Coef<T> & ax,
+                                          const Coef<T> & ay, const Coef<T> & az,
+                                          const Coef<T> & lam, T D2)
+{
+  T nn = (-D2)*rhs[id], d = (-lam.at (id))*D2;
+  {
+    long long s = cstride<DIM> (g, 0);
+    T a1 = ax.at (id + s), a0 = ax.at (id);
+    nn += a1*in[id + s] + a0*in[id - s];
+    d += a1 + a0;
+  }
+  if (DIM > 1) {
+    long long s = cstride<DIM> (g, 1);
+    T a1 = ay.at (id + s), a0 = ay.at (id);
+    nn += a1*in[id + s] + a0*in[id - s];
+    d += a1 + a0;
+  }
+  if (DIM > 2) {
+    long long s = cstride<DIM> (g, 2);
+    T a1 = az.at (id + s), a0 = az.at (id);
+    nn += a1*in[id + s] + a0*in[id - s];
+    d += a1 + a0;
+  }
+  return nn/d;
+}
+
+template <int DIM, typename T, int MODE>
+__global__ void k_relax (bmg_geom g, T * out, const T * in, const T * __restrict__ rhs,
+                         Coef<T> ax, Coef<T> ay, Coef<T> az, Coef<T> lam, T Delta, BCH bc)
+{
+  int i, j, k;
+  if (!cell_of_thread<DIM> (g.n, i, j, k)) return;
+  if (MODE != BMG_SWEEP_JACOBI && ((i + j + k) & 1) != MODE) return;
+  const long long id = cidx<DIM> (g, i, j, k);
+  const T D2 = Delta*Delta;
+  T c = relax_value<DIM, T> (g, id, in, rhs, ax, ay, az, lam, D2);
+  T v;
+  if (MODE == BMG_SWEEP_JACOBI)
+    v = (in[id] + T(2)*c)/T(3);
+  else
+    v = c;
+  out[id] = v;
+  ghosts_homog<DIM, T> (out, g, i, j, k, v, bc);
+}
+
+/* ---------------------------------------------------------------- */
+/* prolongation / restriction                                        */
+/* ---------------------------------------------------------------- */
+
+template <int DIM, typename TC, typename TF>
+__global__ void k_prolong (bmg_geom gc, bmg_geom gf, const TC * __restrict__ s,
+                           TF * __restrict__ f, BCH bc, int zero)
+{
+  int i, j, k;
+  if (!cell_of_thread<DIM> (gf.n, i, j, k)) return;
+  TC v = TC(0);
+  if (!zero) {
+    const int pi = i >> 1, cx = (i & 1) ? 1 : -1;
+    if (DIM == 1)
+      v = (TC(3)*s[cidx<1> (gc, pi, 0, 0)] + s[cidx<1> (gc, pi + cx, 0, 0)])/TC(4);
+    else if (DIM == 2) {
+      const int pj = j >> 1, cy = (j & 1) ? 1 : -1;
+      v = (TC(9)*s[cidx<2> (gc, pi, pj, 0)] +
+           TC(3)*(s[cidx<2> (gc, pi + cx, pj, 0)] + s[cidx<2> (gc, pi, pj + cy, 0)]) +
+           s[cidx<2> (gc, pi + cx, pj + cy, 0)])/TC(16);
+    }
+    else {
+      const int pj = j >> 1, cy = (j & 1) ? 1 : -1;
+      const int pk = k >> 1, cz = (k & 1) ? 1 : -1;
+      v = (TC(27)*s[cidx<3> (gc, pi, pj, pk)] +
+           TC(9)*(s[cidx<3> (gc, pi + cx, pj, pk)] + s[cidx<3> (gc, pi, pj + cy, pk)] +
+                  s[cidx<3> (gc, pi, pj, pk + cz)]) +
+           TC(3)*(s[cidx<3> (gc, pi + cx, pj + cy, pk)] + s[cidx<3> (gc, pi + cx, pj, pk + cz)] +
+                  s[cidx<3> (gc, pi, pj + cy, pk + cz)]) +
+           s[cidx<3> (gc, pi + cx, pj + cy, pk + cz)])/TC(64);
+    }
+  }
+  const TF w = (TF) v;
+  f[cidx<DIM> (gf, i, j, k)] = w;
+  ghosts_homog<DIM, TF> (f, gf, i, j, k, w, bc);
+}
+
+/* coarse = mean of the children, summed in foreach_child order */
+template <int DIM, typename TF, typename TC>
+__global__ void k_restrict (bmg_geom gf, bmg_geom gc, const TF * __restrict__ f,
+                            TC * __restrict__ c)
+{
+  int i, j, k;
+  if (!cell_of_thread<DIM> (gc.n, i, j, k)) return;
+  TC sum = TC(0);
+  const int fi = 2*i, fj = 2*j, fk = 2*k;
+  if (DIM == 1) {
+    for (int a = 0; a < 2; a++) sum += (TC) f[cidx<1> (gf, fi + a, 0, 0)];
+  }
+  else if (DIM == 2) {
+    for (int a = 0; a < 2; a++)
+      for (int b = 0; b < 2; b++)
+        sum += (TC) f[cidx<2> (gf, fi + a, fj + b, 0)];
+  }
+  else {
+    for (int a = 0; a < 2; a++)
+      for (int b = 0; b < 2; b++)
+        for (int d = 0; d < 2; d++)
+          sum += (TC) f[cidx<3> (gf, fi + a, fj + b, fk + d)];
+  }
+  c[cidx<DIM> (gc, i, j, k)] = sum/TC(1 << DIM);
+}
+
+struct FacePtrs {
+  const double * f[3];
+  double * c[3];
+};
+
+/* face_average (multigrid-common.h:42-58) with the foreach_dimension
+   rotation of the fine() offsets; every coarse cell writes its lower face,
+   the last cell along each axis also its upper face. */
+template <int DIM>
+__global__ void k_restrict_face (bmg_geom gf, bmg_geom gc, FacePtrs p)
+{
+  int i, j, k;
+  if (!cell_of_thread<DIM> (gc.n, i, j, k)) return;
+  const int n = gc.n;
+#define FV(o0, o1, o2) f[cidx<DIM> (gf, 2*i + (o0), DIM > 1 ? 2*j + (o1) : 0, DIM > 2 ? 2*k + (o2) : 0)]
+  for (int e = 0; e < DIM; e++) {
+    const double * f = p.f[e];
+    double * c = p.c[e];
+    const int ce = e == 0 ? i : e == 1 ? j : k;
+    for (int side = 0; side < 2; side++) {
+      if (side == 1 && ce != n - 1) break;
+      const int o = 2*side;
+      double v;
+      if (DIM == 1)
+        v = FV (o, 0, 0);
+      else if (DIM == 2)
+        v = e == 0 ? (FV (o, 0, 0) + FV (o, 1, 0))/2. : (FV (0, o, 0) + FV (1, o, 0))/2.;
+      else {
+        if (e == 0)
+          v = (FV (o, 0, 0) + FV (o, 1, 0) + FV (o, 0, 1) + FV (o, 1, 1))/4.;
+        else if (e == 1)
+          v = (FV (0, o, 0) + FV (0, o, 1) + FV (1, o, 0) + FV (1, o, 1))/4.;
+        else
+          v = (FV (0, 0, o) + FV (1, 0, o) + FV (0, 1, o) + FV (1, 1, o))/4.;
+      }
+      const int ii = e == 0 ? i + side : i, jj = e == 1 ? j + side : j, kk = e == 2 ? k + side : k;
+      c[cidx<DIM> (gc, ii, jj, kk)] = v;
+    }
+  }
+#undef FV
+}
+
+/* ---------------------------------------------------------------- */
+/* residual + max reduction                                          */
+/* ---------------------------------------------------------------- */
+
+/* max that keeps NaN */
+__device__ __forceinline__ double nanmax (double a, double b)
+{
+  return (a > b || a != a) ? a : b;
+}
+
+__device__ __forceinline__ void block_max_atomic (double m, unsigned long long * out)
+{
+  __shared__ double sm[32];
+  const int tid = threadIdx.x + blockDim.x*(threadIdx.y + blockDim.y*threadIdx.z);
+  const int lane = tid & 31;
+  const int nth = blockDim.x*blockDim.y*blockDim.z;
+  for (int o = 16; o > 0; o >>= 1)
+    m = nanmax (m, __shfl_xor_sync (0xffffffffu, m, o));
+  const int warp = tid >> 5;
+  if ((tid & 31) == 0) sm[warp] = m;
+  __syncthreads ();
+  if (warp == 0) {
+    const int nw = (nth + 31) >> 5;
+    double v = lane < nw ? sm[lane] : 0.;
+    for (int o = 16; o > 0; o >>= 1)
+      v = nanmax (v, __shfl_xor_sync (0xffffffffu, v, o));
+    if (lane == 0)
+      atomicMax (out, (unsigned long long) __double_as_longlong (v));
+  }
+}
+
+template <int DIM, typename TR>
+__global__ void k_residual (bmg_geom g, bmg_geom gr, const double * __restrict__ a,
+                            const double * __restrict__ b, Coef<double> ax,
+                            Coef<double> ay, Coef<double> az, Coef<double> lam,
+                            double Delta, TR * __restrict__ res,
+                            unsigned long long * maxres)
+{
+  int i, j, k;
+  double m = 0.;
+  if (cell_of_thread<DIM> (g.n, i, j, k)) {
+    const long long id = cidx<DIM> (g, i, j, k);
+    const double ac = a[id];
+    double r = b[id] - lam.at (id)*ac;
+    {
+      long long s = cstride<DIM> (g, 0);
+      r += (ax.at (id)*((ac - a[id - s])/Delta) - ax.at (id + s)*((a[id + s] - ac)/Delta))/Delta;
+    }
+    if (DIM > 1) {
+      long long s = cstride<DIM> (g, 1);
+      r += (ay.at (id)*((ac - a[id - s])/Delta) - ay.at (id + s)*((a[id + s] - ac)/Delta))/Delta;
+    }
+    if (DIM > 2) {
+      long long s = cstride<DIM> (g, 2);
+      r += (az.at (id)*((ac - a[id - s])/Delta) - az.at (id + s)*((a[id + s] - ac)/Delta))/Delta;
+    }
+    res[cidx<DIM> (gr, i, j, k)] = (TR) r;
+    m = fabs (r);
+  }
+  block_max_atomic (m, maxres);
+}
+
+/* ---------------------------------------------------------------- */
+/* correction a += da, boundary conditions                           */
+/* ---------------------------------------------------------------- */
+
+template <int DIM, typename TD>
+__global__ void k_correct (bmg_geom g, bmg_geom gd, double * a, const TD * __restrict__ da,
+                           bmg_bcdesc bc)
+{
+  int i, j, k;
+  if (!cell_of_thread<DIM> (g.n, i, j, k)) return;
+  const long long id = cidx<DIM> (g, i, j, k);
+  const double v = a[id] + (double) da[cidx<DIM> (gd, i, j, k)];
+  a[id] = v;
+  ghosts_inhomog<DIM> (a, g, i, j, k, v, bc);
+}
+
+template <int DIM, typename T>
+__global__ void k_apply_bc (bmg_geom g, T * f, bmg_bcdesc bc, BCH h, int homogeneous)
+{
+  int i, j, k;
+  if (!cell_of_thread<DIM> (g.n, i, j, k)) return;
+  if (!on_boundary<DIM> (g.n, i, j, k)) return;
+  const long long id = cidx<DIM> (g, i, j, k);
+  if (homogeneous)
+    ghosts_homog<DIM, T> (f, g, i, j, k, f[id], h);
+  else
+    ghosts_inhomog<DIM> ((double *) f, g, i, j, k, (double) f[id], bc);
+}
+
+/* ---------------------------------------------------------------- */
+/* sums, packing, conversion                                         */
+/* ---------------------------------------------------------------- */
+
+template <int DIM>
+__device__ __forceinline__ void decode (long long q, int ni, int nj, int nk, int & i, int & j, int & k)
+{
+  if (DIM == 1) { i = (int) q; j = k = 0; return; }
+  if (DIM == 2) { i = (int) (q/nj); j = (int) (q - (long long) i*nj); k = 0; return; }
+  long long ij = q/nk;
+  k = (int) (q - ij*nk);
+  i = (int) (ij/nj);
+  j = (int) (ij - (long long) i*nj);
+}
+
+__device__ __forceinline__ double block_sum (double v, double * sm)
+{
+  const int tid = threadIdx.x;
+  for (int o = 16; o > 0; o >>= 1)
+    v += __shfl_down_sync (0xffffffffu, v, o);
+  if ((tid & 31) == 0) sm[tid >> 5] = v;
+  __syncthreads ();
+  double r = 0.;
+  if (tid < 32) {
+    const int nw = blockDim.x >> 5;
+    r = tid < nw ? sm[tid] : 0.;
+    for (int o = 16; o > 0; o >>= 1)
+      r += __shfl_down_sync (0xffffffffu, r, o);
+  }
+  return r;
+}
+
+/* deterministic two-stage sum of the interior (fixed partition, fixed order) */
+template <int DIM>
+__global__ void k_sum_partial (bmg_geom g, const double * __restrict__ b, double * partials)
+{
+  __shared__ double sm[32];
+  const int n = g.n;
+  const long long total = DIM == 1 ? n : DIM == 2 ? (long long) n*n : (long long) n*n*n;
+  double s = 0.;
+  for (long long q = (long long) blockIdx.x*blockDim.x + threadIdx.x; q < total;
+       q += (long long) gridDim.x*blockDim.x) {
+    int i, j, k;
+    decode<DIM> (q, n, n, n, i, j, k);
+    s += b[cidx<DIM> (g, i, j, k)];
+  }
+  s = block_sum (s, sm);
+  if (threadIdx.x == 0) partials[blockIdx.x] = s;
+}
+
+__global__ void k_sum_final (const double * partials, int np, double * out)
+{
+  __shared__ double sm[32];
+  double s = 0.;
+  for (int q = threadIdx.x; q < np; q += blockDim.x) s += partials[q];
+  s = block_sum (s, sm);
+  if (threadIdx.x == 0) *out = s;
+}
+
+template <int DIM, typename T>
+__global__ void k_pack (bmg_geom g, int ni, int nj, int nk, const double * __restrict__ src,
+                        T * __restrict__ dst)
+{
+  const long long total = (long long) ni*nj*nk;
+  for (long long q = (long long) blockIdx.x*blockDim.x + threadIdx.x; q < total;
+       q += (long long) gridDim.x*blockDim.x) {
+    int i, j, k;
+    decode<DIM> (q, ni, nj, nk, i, j, k);
+    dst[cidx<DIM> (g, i, j, k)] = (T) src[q];
+  }
+}
+
+template <int DIM>
+__global__ void k_unpack (bmg_geom g, int ni, int nj, int nk, const double * __restrict__ src,
+                          double * __restrict__ dst)
+{
+  const long long total = (long long) ni*nj*nk;
+  for (long long q = (long long) blockIdx.x*blockDim.x + threadIdx.x; q < total;
+       q += (long long) gridDim.x*blockDim.x) {
+    int i, j, k;
+    decode<DIM> (q, ni, nj, nk, i, j, k);
+    dst[q] = src[cidx<DIM> (g, i, j, k)];
+  }
+}
+
+template <int DIM>
+__global__ void k_convert (bmg_geom g64, bmg_geom g32, int ni, int nj, int nk,
+                           const double * __restrict__ src, float * __restrict__ dst)
+{
+  const long long total = (long long) ni*nj*nk;
+  for (long long q = (long long) blockIdx.x*blockDim.x + threadIdx.x; q < total;
+       q += (long long) gridDim.x*blockDim.x) {
+    int i, j, k;
+    decode<DIM> (q, ni, nj, nk, i, j, k);
+    dst[cidx<DIM> (g32, i, j, k)] = (float) src[cidx<DIM> (g64, i, j, k)];
+  }
+}
+
+template <typename T>
+__global__ void k_fill (T * f, long long n, T v)
+{
+  for (long long q = (long long) blockIdx.x*blockDim.x + threadIdx.x; q < n;
+       q += (long long) gridDim.x*blockDim.x)
+    f[q] = v;
+}
+
+template <int DIM>
+__global__ void k_shift (bmg_geom g, double * f, const double * sum, double scale)
+{
+  int i, j, k;
+  if (!cell_of_thread<DIM> (g.n, i, j, k)) return;
+  f[cidx<DIM> (g, i, j, k)] -= (*sum)*scale;
+}
+
+/* face n along a periodic direction = face 0 */
+template <int DIM>
+__global__ void k_face_wrap (bmg_geom g, int e, double * f)
+{
+  const int n = g.n;
+  const long long total = DIM == 1 ? 1 : DIM == 2 ? n : (long long) n*n;
+  const long long q = (long long) blockIdx.x*blockDim.x + threadIdx.x;
+  if (q >= total) return;
+  int t1 = DIM > 1 ? (int) (DIM == 2 ? q : q/n) : 0, t2 = DIM > 2 ? (int) (q % n) : 0;
+  int c0[3], c1[3], m = 0;
+  const int tt[2] = {t1, t2};
+  for (int d = 0; d < 3; d++) {
+    if (d == e) { c0[d] = 0; c1[d] = n; }
+    else if (d < DIM) { c0[d] = c1[d] = tt[m++]; }
+    else c0[d] = c1[d] = 0;
+  }
+  f[cidx<DIM> (g, c1[0], c1[1], c1[2])] = f[cidx<DIM> (g, c0[0], c0[1], c0[2])];
+}
+
+int lin_blocks (long long total)
+{
+  long long b = (total + 255)/256;
+  if (b > 148*16) b = 148*16;
+  if (b < 1) b = 1;
+  return (int) b;
+}
+
+int status_of_launch ()
+{
+  cudaError_t e = cudaGetLastError ();
+  return e == cudaSuccess ? 0 : (int) e;
+}
+
+/* ---------------------------------------------------------------- */
+/* dimension dispatch                                                */
+/* ---------------------------------------------------------------- */
+
+template <int DIM, typename T>
+void relax_dim (int mode, bmg_geom g, void * out, const void * in, const void * rhs,
+                const bmg_coef * alpha, bmg_coef lambda, double Delta, BCH h,
+                cudaStream_t s)
+{
+  Coef<T> ax = coef_of<T> (alpha[0]), ay = coef_of<T> (alpha[1]),
+    az = coef_of<T> (alpha[2]), lam = coef_of<T> (lambda);
+  dim3 gb = grid_shape<DIM> (g.n), bb = block_shape<DIM> ();
+  if (mode == BMG_SWEEP_JACOBI)
+    k_relax<DIM, T, BMG_SWEEP_JACOBI><<<gb, bb, 0, s>>> (g, (T *) out, (const T *) in,
+                                                          (const T *) rhs, ax, ay, az, lam, (T) Delta, h);
+  else if (mode == BMG_SWEEP_RED)
+    k_relax<DIM, T, BMG_SWEEP_RED><<<gb, bb, 0, s>>> (g, (T *) out, (const T *) in,
+                                                       (const T *) rhs, ax, ay, az, lam, (T) Delta, h);
+  else
+    k_relax<DIM, T, BMG_SWEEP_BLACK><<<gb, bb, 0, s>>> (g, (T *) out, (const T *) in,
+                                                         (const T *) rhs, ax, ay, az, lam, (T) Delta, h);
+}
+
+#define DISPATCH_DIM(dim, F, ...)                         \
+  do {                                                    \
+    if ((dim) == 1) F<1> (__VA_ARGS__);                   \
+    else if ((dim) == 2) F<2> (__VA_ARGS__);              \
+    else F<3> (__VA_ARGS__);                              \
+  } while (0)
+
+template <int DIM>
+void relax_st (int st, int mode, bmg_geom g, void * out, const void * in, const void * rhs,
+               const bmg_coef * alpha, bmg_coef lambda, double Delta, BCH h, cudaStream_t s)
+{
+  if (st == BMG_ST_F64) relax_dim<DIM, double> (mode, g, out, in, rhs, alpha, lambda, Delta, h, s);
+  else relax_dim<DIM, float> (mode, g, out, in, rhs, alpha, lambda, Delta, h, s);
+}
+
+template <int DIM>
+void prolong_dim (int stc, int stf, bmg_geom gc, bmg_geom gf, const void * c, void * f,
+                  BCH h, int zero, cudaStream_t s)
+{
+  dim3 gb = grid_shape<DIM> (gf.n), bb = block_shape<DIM> ();
+  if (stc == BMG_ST_F64 && stf == BMG_ST_F64)
+    k_prolong<DIM, double, double><<<gb, bb, 0, s>>> (gc, gf, (const double *) c, (double *) f, h, zero);
+  else if (stc == BMG_ST_F32 && stf == BMG_ST_F32)
+    k_prolong<DIM, float, float><<<gb, bb, 0, s>>> (gc, gf, (const float *) c, (float *) f, h, zero);
+  else if (stc == BMG_ST_F64 && stf == BMG_ST_F32)
+    k_prolong<DIM, double, float><<<gb, bb, 0, s>>> (gc, gf, (const double *) c, (float *) f, h, zero);
+  else
+    k_prolong<DIM, float, double><<<gb, bb, 0, s>>> (gc, gf, (const float *) c, (double *) f, h, zero);
+}
+
+template <int DIM>
+void restrict_dim (int stf, int stc, bmg_geom gf, bmg_geom gc, const void * f, void * c,
+                   cudaStream_t s)
+{
+  dim3 gb = grid_shape<DIM> (gc.n), bb = block_shape<DIM> ();
+  if (stf == BMG_ST_F64 && stc == BMG_ST_F64)
+    k_restrict<DIM, double, double><<<gb, bb, 0, s>>> (gf, gc, (const double *) f, (double *) c);
+  else if (stf == BMG_ST_F32 && stc == BMG_ST_F32)
+    k_restrict<DIM, float, float><<<gb, bb, 0, s>>> (gf, gc, (const float *) f, (float *) c);
+  else if (stf == BMG_ST_F32 && stc == BMG_ST_F64)
+    k_restrict<DIM, float, double><<<gb, bb, 0, s>>> (gf, gc, (const float *) f, (double *) c);
+  else
+    k_restrict<DIM, double, float><<<gb, bb, 0, s>>> (gf, gc, (const double *) f, (float *) c);
+}
+
+template <int DIM>
+void restrict_face_dim (bmg_geom gf, bmg_geom gc, FacePtrs p, cudaStream_t s)
+{
+  k_restrict_face<DIM><<<grid_shape<DIM> (gc.n), block_shape<DIM> (), 0, s>>> (gf, gc, p);
+}
+
+template <int DIM>
+void residual_dim (int st, bmg_geom g, bmg_geom gr, const double * a, const double * b,
+                   const bmg_coef * alpha, bmg_coef lambda, double Delta, void * res,
+                   unsigned long long * maxres, cudaStream_t s)
+{
+  Coef<double> ax = coef_of<double> (alpha[0]), ay = coef_of<double> (alpha[1]),
+    az = coef_of<double> (alpha[2]), lam = coef_of<double> (lambda);
+  dim3 gb = grid_shape<DIM> (g.n), bb = block_shape<DIM> ();
+  if (st == BMG_ST_F64)
+    k_residual<DIM, double><<<gb, bb, 0, s>>> (g, gr, a, b, ax, ay, az, lam, Delta, (double *) res, maxres);
+  else
+    k_residual<DIM, float><<<gb, bb, 0, s>>> (g, gr, a, b, ax, ay, az, lam, Delta, (float *) res, maxres);
+}
+
+template <int DIM>
+void correct_dim (int st, bmg_geom g, bmg_geom gd, double * a, const void * da,
+                  bmg_bcdesc bc, cudaStream_t s)
+{
+  dim3 gb = grid_shape<DIM> (g.n), bb = block_shape<DIM> ();
+  if (st == BMG_ST_F64)
+    k_correct<DIM, double><<<gb, bb, 0, s>>> (g, gd, a, (const double *) da, bc);
+  else
+    k_correct<DIM, float><<<gb, bb, 0, s>>> (g, gd, a, (const float *) da, bc);
+}
+
+template <int DIM>
+void apply_bc_dim (int st, bmg_geom g, void * f, bmg_bcdesc bc, BCH h, int homogeneous,
+                   cudaStream_t s)
+{
+  dim3 gb = grid_shape<DIM> (g.n), bb = block_shape<DIM> ();
+  if (st == BMG_ST_F64)
+    k_apply_bc<DIM, double><<<gb, bb, 0, s>>> (g, (double *) f, bc, h, homogeneous);
+  else
+    k_apply_bc<DIM, float><<<gb, bb, 0, s>>> (g, (float *) f, bc, h, homogeneous);
+}
+
+template <int DIM>
+void extents (int n, int face_dim, int & ni, int & nj, int & nk)
+{
+  ni = n + (face_dim == 0);
+  nj = DIM > 1 ? n + (face_dim == 1) : 1;
+  nk = DIM > 2 ? n + (face_dim == 2) : 1;
+}
+
+template <int DIM>
+void pack_dim (int st, bmg_geom g, int face_dim, const double * c, void * p, cudaStream_t s)
+{
+  int ni, nj, nk;
+  extents<DIM> (g.n, face_dim, ni, nj, nk);
+  int nb = lin_blocks ((long long) ni*nj*nk);
+  if (st == BMG_ST_F64)
+    k_pack<DIM, double><<<nb, 256, 0, s>>> (g, ni, nj, nk, c, (double *) p);
+  else
+    k_pack<DIM, float><<<nb, 256, 0, s>>> (g, ni, nj, nk, c, (float *) p);
+}
+
+template <int DIM>
+void unpack_dim (bmg_geom g, int face_dim, const double * p, double * c, cudaStream_t s)
+{
+  int ni, nj, nk;
+  extents<DIM> (g.n, face_dim, ni, nj, nk);
+  k_unpack<DIM><<<lin_blocks ((long long) ni*nj*nk), 256, 0, s>>> (g, ni, nj, nk, p, c);
+}
+
+template <int DIM>
+void convert_dim (bmg_geom g64, bmg_geom g32, int face_dim, const double * src, float * dst,
+                  cudaStream_t s)
+{
+  int ni, nj, nk;
+  extents<DIM> (g64.n, face_dim, ni, nj, nk);
+  k_convert<DIM><<<lin_blocks ((long long) ni*nj*nk), 256, 0, s>>> (g64, g32, ni, nj, nk, src, dst);
+}
+
+template <int DIM>
+void sum_dim (bmg_geom g, const double * b, double * partials, int np, double * out,
+              cudaStream_t s)
+{
+  k_sum_partial<DIM><<<np, 256, 0, s>>> (g, b, partials);
+  k_sum_final<<<1, 1024, 0, s>>> (partials, np, out);
+}
+
+template <int DIM>
+void shift_dim (bmg_geom g, double * f, const double * sum, double scale, cudaStream_t s)
+{
+  k_shift<DIM><<<grid_shape<DIM> (g.n), block_shape<DIM> (), 0, s>>> (g, f, sum, scale);
+}
+
+} // namespace
+
+/* ---------------------------------------------------------------- */
+/* C launchers                                                       */
+/* ---------------------------------------------------------------- */
+
+extern "C" {
+
+int bmg_launch_relax (int dim, int st, int mode, bmg_geom g, void * out, const void * in,
+                      const void * rhs, const bmg_coef * alpha, bmg_coef lambda,
+                      double Delta, const bmg_bcdesc * bc, cudaStream_t s)
+{
+  BCH h = bch_of (bc);
+  DISPATCH_DIM (dim, relax_st, st, mode, g, out, in, rhs, alpha, lambda, Delta, h, s);
+  return status_of_launch ();
+}
+
+int bmg_launch_prolong (int dim, int st_coarse, int st_fine, bmg_geom gc, bmg_geom gf,
+                        const void * coarse, void * fine, const bmg_bcdesc * bc, int zero,
+                        cudaStream_t s)
+{
+  BCH h = bch_of (bc);
+  DISPATCH_DIM (dim, prolong_dim, st_coarse, st_fine, gc, gf, coarse, fine, h, zero, s);
+  return status_of_launch ();
+}
+
+int bmg_launch_restrict (int dim, int st_fine, int st_coarse, bmg_geom gf, bmg_geom gc,
+                         const void * fine, void * coarse, cudaStream_t s)
+{
+  DISPATCH_DIM (dim, restrict_dim, st_fine, st_coarse, gf, gc, fine, coarse, s);
+  return status_of_launch ();
+}
+
+int bmg_launch_restrict_face (int dim, bmg_geom gf, bmg_geom gc, const double * const * fine,
+                              double * const * coarse, cudaStream_t s)
+{
+  FacePtrs p;
+  for (int e = 0; e < 3; e++) {
+    p.f[e] = e < dim ? fine[e] : 0;
+    p.c[e] = e < dim ? coarse[e] : 0;
+  }
+  DISPATCH_DIM (dim, restrict_face_dim, gf, gc, p, s);
+  return status_of_launch ();
+}
+
+int bmg_launch_residual (int dim, int st_res, bmg_geom g, bmg_geom gres, const double * a,
+                         const double * b, const bmg_coef * alpha, bmg_coef lambda,
+                         double Delta, void * res, unsigned long long * maxres,
+                         cudaStream_t s)
+{
+  DISPATCH_DIM (dim, residual_dim, st_res, g, gres, a, b, alpha, lambda, Delta, res, maxres, s);
+  return status_of_launch ();
+}
+
+int bmg_launch_correct (int dim, int st_da, bmg_geom g, bmg_geom gda, double * a,
+                        const void * da, const bmg_bcdesc * bc, cudaStream_t s)
+{
+  DISPATCH_DIM (dim, correct_dim, st_da, g, gda, a, da, *bc, s);
+  return status_of_launch ();
+}
+
+int bmg_launch_apply_bc (int dim, int st, bmg_geom g, void * f, const bmg_bcdesc * bc,
+                         int homogeneous, cudaStream_t s)
+{
+  BCH h = bch_of (bc);
+  DISPATCH_DIM (dim, apply_bc_dim, st, g, f, *bc, h, homogeneous, s);
+  return status_of_launch ();
+}
+
+int bmg_sum_partials (int dim, bmg_geom g)
+{
+  long long total = dim == 1 ? g.n : dim == 2 ? (long long) g.n*g.n : (long long) g.n*g.n*g.n;
+  long long nb = (total + 255)/256;
+  if (nb > 1024) nb = 1024;
+  if (nb < 1) nb = 1;
+  return (int) nb;
+}
+
+int bmg_launch_sum (int dim, bmg_geom g, const double * b, double * partials, int npartials,
+                    double * out, cudaStream_t s)
+{
+  DISPATCH_DIM (dim, sum_dim, g, b, partials, npartials, out, s);
+  return status_of_launch ();
+}
+
+int bmg_launch_pack (int dim, int st, bmg_geom g, int face_dim, const double * compact,
+                     void * padded, cudaStream_t s)
+{
+  DISPATCH_DIM (dim, pack_dim, st, g, face_dim, compact, padded, s);
+  return status_of_launch ();
+}
+
+int bmg_launch_unpack (int dim, bmg_geom g, int face_dim, const double * padded,
+                       double * compact, cudaStream_t s)
+{
+  DISPATCH_DIM (dim, unpack_dim, g, face_dim, padded, compact, s);
+  return status_of_launch ();
+}
+
+int bmg_launch_convert (int dim, bmg_geom g64, bmg_geom g32, int face_dim, const double * src,
+                        float * dst, cudaStream_t s)
+{
+  DISPATCH_DIM (dim, convert_dim, g64, g32, face_dim, src, dst, s);
+  return status_of_launch ();
+}
+
+int bmg_launch_fill (int dim, int st, bmg_geom g, void * f, double v, cudaStream_t s)
+{
+  (void) dim;
+  int nb = lin_blocks (g.size);
+  if (st == BMG_ST_F64) k_fill<double><<<nb, 256, 0, s>>> ((double *) f, g.size, v);
+  else k_fill<float><<<nb, 256, 0, s>>> ((float *) f, g.size, (float) v);
+  return status_of_launch ();
+}
+
+int bmg_launch_face_wrap (int dim, bmg_geom g, int face_dim, double * f, cudaStream_t s)
+{
+  long long total = dim == 1 ? 1 : dim == 2 ? g.n : (long long) g.n*g.n;
+  int nb = (int) ((total + 255)/256);
+  if (dim == 1) k_face_wrap<1><<<nb, 256, 0, s>>> (g, face_dim, f);
+  else if (dim == 2) k_face_wrap<2><<<nb, 256, 0, s>>> (g, face_dim, f);
+  else k_face_wrap<3><<<nb, 256, 0, s>>> (g, face_dim, f);
+  return status_of_launch ();
+}
+
+int bmg_launch_shift (int dim, bmg_geom g, double * f, const double * sum, double scale,
+                      cudaStream_t s)
+{
+  DISPATCH_DIM (dim, shift_dim, g, f, sum, scale, s);
+  return status_of_launch ();
+}
+
+} // extern "C"

@@ -1,0 +1,112 @@
+/*
+ * mg_launch.h -- internal interface between the C host layer (mg_host.c)
+ * and the CUDA kernels (mg_kernels.cu).  Plain C types only.
+ *
+ * Device level layout (one array per field per level, structure of arrays):
+ *   interior cell (i, j, k), 0 <= i, j, k < n, of a level lives at
+ *     1D:  xo + i
+ *     2D:  (i + 1)*P + xo + j
+ *     3D:  (i + 1)*plane + (j + 1)*P + xo + k
+ *   with one ghost layer on every side (the reference keeps GHOSTS = 2 but
+ *   its box conditions fill only BGHOSTS = 1, grid/multigrid.h:2-9, and no
+ *   operator of this path reads the second layer).  xo puts interior index 0
+ *   of the contiguous axis on a 32-byte boundary; P is padded to 128 bytes.
+ *   Face component d uses the same array shape: face f along d sits at the
+ *   slot of cell f, so face n is the ghost slot (as alpha.x[1] of the last
+ *   cell in the reference).
+ */
+#ifndef MG_LAUNCH_H
+#define MG_LAUNCH_H
+
+#include <cuda_runtime_api.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BMG_MAXLEVEL 15
+
+typedef struct {
+  int n;             /* interior cells per side */
+  int P;             /* elements per row of the contiguous axis */
+  int xo;            /* element offset of interior index 0 on that axis */
+  int pad_;
+  long long plane;   /* elements per slab of the first axis (3D) */
+  long long size;    /* elements of the level array */
+} bmg_geom;
+
+/* boundary conditions of one field (finest level for inhomogeneous data) */
+typedef struct {
+  int periodic[3];
+  int type[6];             /* BMG_NEUMANN / BMG_DIRICHLET / BMG_PERIODIC */
+  const double * val[6];   /* device boundary values, NULL = cval */
+  double cval[6];
+  double Delta;            /* finest-level cell size, for Neumann data */
+} bmg_bcdesc;
+
+/* a coefficient on one level: array of the storage type, or a constant */
+typedef struct {
+  const void * p;
+  double c;
+} bmg_coef;
+
+/* storage types */
+enum { BMG_ST_F64 = 0, BMG_ST_F32 = 1 };
+/* relax modes */
+enum { BMG_SWEEP_RED = 0, BMG_SWEEP_BLACK = 1, BMG_SWEEP_JACOBI = 2 };
+
+int bmg_launch_relax (int dim, int st, int mode, bmg_geom g, void * out,
+                      const void * in, const void * rhs, const bmg_coef * alpha,
+                      bmg_coef lambda, double Delta, const bmg_bcdesc * bc,
+                      cudaStream_t s);
+
+int bmg_launch_prolong (int dim, int st_coarse, int st_fine, bmg_geom gc,
+                        bmg_geom gf, const void * coarse, void * fine,
+                        const bmg_bcdesc * bc, int zero, cudaStream_t s);
+
+int bmg_launch_restrict (int dim, int st_fine, int st_coarse, bmg_geom gf,
+                         bmg_geom gc, const void * fine, void * coarse,
+                         cudaStream_t s);
+
+int bmg_launch_restrict_face (int dim, bmg_geom gf, bmg_geom gc,
+                              const double * const * fine, double * const * coarse,
+                              cudaStream_t s);
+
+int bmg_launch_residual (int dim, int st_res, bmg_geom g, bmg_geom gres,
+                         const double * a, const double * b,
+                         const bmg_coef * alpha, bmg_coef lambda, double Delta,
+                         void * res, unsigned long long * maxres,
+                         cudaStream_t s);
+
+int bmg_launch_correct (int dim, int st_da, bmg_geom g, bmg_geom gda, double * a,
+                        const void * da, const bmg_bcdesc * bc, cudaStream_t s);
+
+int bmg_launch_apply_bc (int dim, int st, bmg_geom g, void * f,
+                         const bmg_bcdesc * bc, int homogeneous, cudaStream_t s);
+
+int bmg_launch_sum (int dim, bmg_geom g, const double * b, double * partials,
+                    int npartials, double * out, cudaStream_t s);
+
+int bmg_launch_pack (int dim, int st, bmg_geom g, int face_dim,
+                     const double * compact, void * padded, cudaStream_t s);
+
+int bmg_launch_unpack (int dim, bmg_geom g, int face_dim, const double * padded,
+                       double * compact, cudaStream_t s);
+
+int bmg_launch_convert (int dim, bmg_geom g64, bmg_geom g32, int face_dim,
+                        const double * src, float * dst, cudaStream_t s);
+
+int bmg_launch_fill (int dim, int st, bmg_geom g, void * f, double v, cudaStream_t s);
+
+int bmg_launch_shift (int dim, bmg_geom g, double * f, const double * sum,
+                      double scale, cudaStream_t s);
+
+int bmg_launch_face_wrap (int dim, bmg_geom g, int face_dim, double * f, cudaStream_t s);
+
+/* number of partial sums bmg_launch_sum needs for a level */
+int bmg_sum_partials (int dim, bmg_geom g);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

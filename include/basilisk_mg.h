@@ -1,0 +1,210 @@
+/*
+ * basilisk_mg.h -- C-ABI of the B200 multigrid Poisson--Helmholtz solver.
+ *
+ * A device-resident replacement for Basilisk's multigrid Poisson solver
+ * (poisson.h: mg_cycle, mg_solve, poisson; grid/multigrid.h levels).  The
+ * reference-facing entry points keep the reference's names, argument
+ * meaning and result struct; the grid/field functions are the device
+ * counterpart of what grid/multigrid.h and grid/cartesian-common.h give a
+ * Basilisk program (init_grid, new scalar fields, boundary conditions,
+ * origin/size/periodic).
+ *
+ * Conventions
+ *   - Fields live on the device, on every level 0..depth of one grid, as
+ *     padded, level-contiguous structure-of-arrays buffers.  Host code moves
+ *     finest-level values in and out with bmg_field_set / bmg_field_get, from
+ *     host or device memory, in the compact layout: n^dimension values in C
+ *     order with the last index contiguous (the reference's index order,
+ *     grid/multigrid.h:59-73).  Face component d has n+1 values along d; face
+ *     f is the left/bottom/back face of cell f (alpha.x[] / alpha.x[1],
+ *     poisson.h:306).
+ *   - Handles are small integers, 0 meaning "unset" (poisson.h:410-413 tests
+ *     alpha.x.i and lambda.i against 0).
+ *   - Every call is on one host thread per grid; the grid owns one CUDA
+ *     stream; calls are not re-entrant on one grid.
+ *   - The library never aborts the process and never traps on the device:
+ *     failures are status codes (bmg_* functions) or bmg_last_error() (the
+ *     reference-named functions, which return mgstats by value).
+ */
+#ifndef BASILISK_MG_H
+#define BASILISK_MG_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- result and globals: poisson.h:102-114 ---------------------------- */
+
+/* byte-identical to the reference's mgstats (poisson.h:108-114) */
+typedef struct {
+  int i;              /* number of iterations */
+  double resb, resa;  /* maximum residual before and after the iterations */
+  double sum;         /* sum of r.h.s. */
+  int nrelax;         /* number of relaxations */
+  int minlevel;       /* minimum level of the multigrid hierarchy */
+} mgstats;
+
+/* poisson.h:102-103: same names, same defaults (100, 1, 1e-3) */
+extern int NITERMAX, NITERMIN;
+extern double TOLERANCE;
+
+/* ---- status codes --------------------------------------------------- */
+enum {
+  BMG_OK = 0,
+  BMG_EINVAL = 1,        /* invalid argument or handle */
+  BMG_ECUDA = 2,         /* a CUDA runtime call failed */
+  BMG_ENOMEM = 3,        /* device allocation failed */
+  BMG_ENAN = 4,          /* the residual became NaN or Inf */
+  BMG_ENOTCONV = 5,      /* tolerance not reached after NITERMAX cycles */
+  BMG_EUNSUPPORTED = 6,  /* callbacks other than the Poisson ones */
+  BMG_ENODEV = 7         /* no CUDA device */
+};
+const char * bmg_error_string (int status);
+int bmg_last_error (void);           /* status of the last call on this thread */
+
+/* ---- grid: grid/multigrid.h init_grid, common.h origin/size/periodic -- */
+
+/* sides in the reference's order (common.h:949) */
+enum { BMG_RIGHT = 0, BMG_LEFT, BMG_TOP, BMG_BOTTOM, BMG_FRONT, BMG_BACK };
+
+/* boundary-condition kinds (common.h:957-960; periodic: cartesian-common.h:898) */
+enum { BMG_NEUMANN = 0, BMG_DIRICHLET = 1, BMG_PERIODIC = 2 };
+
+/* smoother: red-black Gauss-Seidel, or the reference's -DJACOBI weighted
+   Jacobi (poisson.h:293-328), which gives results independent of the
+   traversal order and therefore bit-comparable with the reference. */
+enum { BMG_RELAX_RBGS = 0, BMG_RELAX_JACOBI = 1 };
+
+/* arithmetic of the solve: FP64 throughout, or FP32 cycles inside an FP64
+   iterative-refinement loop (outer residual, accumulation, compatibility
+   projection and coarsest level in FP64). */
+enum { BMG_FP64 = 0, BMG_MIXED = 1 };
+
+/* where the pointers given to bmg_field_set / get / bmg_bc point */
+enum { BMG_HOST = 0, BMG_DEVICE = 1 };
+
+typedef struct bmg_grid bmg_grid;
+
+/* init_grid (grid/multigrid.h:723-759): levels 0..depth of a 2^depth per
+   side box, dimension 1, 2 or 3, on the current CUDA device.  The new grid
+   becomes the current grid used by poisson(), mg_solve() and mg_cycle(). */
+int bmg_grid_new (bmg_grid ** grid, int dimension, int depth);
+void bmg_grid_free (bmg_grid * grid);
+int bmg_grid_select (bmg_grid * grid);      /* make it the current grid */
+bmg_grid * bmg_grid_current (void);
+int bmg_grid_info (const bmg_grid * grid, int * dimension, int * depth);
+/* origin (common.h:935) and size (common.h:939) */
+int bmg_origin (bmg_grid * grid, double x, double y, double z);
+int bmg_size (bmg_grid * grid, double L0);
+/* periodic (cartesian-common.h:920-933): dir is a side (BMG_RIGHT, BMG_TOP,
+   BMG_FRONT or their opposite); applies to every field of the grid */
+int bmg_periodic (bmg_grid * grid, int dir);
+int bmg_set_relax (bmg_grid * grid, int relax);
+int bmg_set_precision (bmg_grid * grid, int precision);
+/* optional: run on a caller's stream (cudaStream_t); NULL = the grid's own */
+int bmg_set_stream (bmg_grid * grid, void * stream);
+int bmg_synchronize (bmg_grid * grid);
+
+/* ---- fields: scalar / face vector handles ---------------------------- */
+
+/* layout-compatible with Basilisk's scalar {int i;} and vector {scalar x, y, z;} */
+typedef struct { int i; } bmg_scalar;
+typedef struct { bmg_scalar x, y, z; } bmg_vector;
+
+/* a new cell-centred field, zero on every level (cartesian-common.h:62-106) */
+int bmg_scalar_new (bmg_grid * grid, bmg_scalar * s);
+/* a new face vector; its components have no box BCs (cartesian-common.h:566) */
+int bmg_face_vector_new (bmg_grid * grid, bmg_vector * v);
+/* constant fields (common.h:1275-1277): stored as one value, never as arrays */
+int bmg_const_scalar (bmg_grid * grid, double value, bmg_scalar * s);
+int bmg_const_face_vector (bmg_grid * grid, double value, bmg_vector * v);
+int bmg_field_delete (bmg_grid * grid, bmg_scalar s);
+/* finest-level values in the compact layout; count = number of doubles */
+int bmg_field_set (bmg_grid * grid, bmg_scalar s, const double * values, size_t count, int memory);
+int bmg_field_get (bmg_grid * grid, bmg_scalar s, double * values, size_t count, int memory);
+/* values of any level (tests, diagnostics) */
+int bmg_field_get_level (bmg_grid * grid, bmg_scalar s, int level, double * values, size_t count, int memory);
+int bmg_field_set_level (bmg_grid * grid, bmg_scalar s, int level, const double * values, size_t count, int memory);
+
+/* s[side] = dirichlet(v) / neumann(v) (common.h:957-960): a constant v, or,
+   when values != NULL, one value per boundary face of the finest level
+   (n^(dimension-1) values over the tangential indices in increasing
+   dimension order).  The homogeneous twin (-s[] / s[]) is used for the
+   correction field of mg_solve (poisson.h:155-157). */
+int bmg_bc (bmg_grid * grid, bmg_scalar s, int side, int type, double value,
+            const double * values, int memory);
+
+/* ---- the solver: poisson.h ----------------------------------------- */
+
+/* struct Poisson (poisson.h:258-265), same members and order */
+struct Poisson {
+  bmg_scalar a, b;
+  bmg_vector alpha;      /* 0 = unityf */
+  bmg_scalar lambda;     /* 0 = zeroc */
+  double tolerance;      /* 0 = TOLERANCE */
+  int nrelax, minlevel;
+  bmg_scalar * res;      /* optional: receives the final residual */
+};
+
+/* poisson (poisson.h:402-441) on the current grid.  Status: bmg_last_error(). */
+mgstats poisson (struct Poisson p);
+/* the same on a given grid, returning a status */
+int bmg_poisson (bmg_grid * grid, struct Poisson p, mgstats * stats);
+
+/* the Poisson--Helmholtz callbacks (poisson.h:271-391); data is a
+   struct Poisson *.  These are the only callbacks mg_solve/mg_cycle accept:
+   they run on the device, host callbacks cannot. */
+void bmg_relax (bmg_scalar * da, bmg_scalar * res, int level, void * data);
+double bmg_residual (bmg_scalar * a, bmg_scalar * b, bmg_scalar * res, void * data);
+
+/* struct MGSolve (poisson.h:125-137), same members and order */
+struct MGSolve {
+  bmg_scalar * a, * b;
+  double (* residual) (bmg_scalar * a, bmg_scalar * b, bmg_scalar * res, void * data);
+  void (* relax) (bmg_scalar * da, bmg_scalar * res, int depth, void * data);
+  void * data;
+  int nrelax;
+  bmg_scalar * res;
+  int minlevel;
+  double tolerance;
+};
+
+/* mg_solve (poisson.h:139-235).  Status: bmg_last_error(). */
+mgstats mg_solve (struct MGSolve p);
+
+/* mg_cycle (poisson.h:32-90): restriction of res, coarse-to-fine
+   correction of da with nrelax relaxations per level, then a += da.  da
+   takes the homogeneous BCs of a. */
+void mg_cycle (bmg_scalar * a, bmg_scalar * res, bmg_scalar * da,
+               void (* relax) (bmg_scalar * da, bmg_scalar * res, int depth, void * data),
+               void * data, int nrelax, int minlevel, int maxlevel);
+
+/* restriction of a list of fields to all levels (multigrid-common.h:368-404),
+   as test/variable.c calls it for its face coefficients; list ends with .i=0 */
+int bmg_restriction (bmg_grid * grid, const bmg_scalar * list);
+
+/* ---- measurement ---------------------------------------------------- */
+
+/* totals since the grid was created: V-cycles, relaxation sweeps per level
+   (summed), algorithmic bytes moved by the cycle kernels (each array pass
+   counted once at its storage precision, ghosts excluded) and the device
+   time of the cycles in milliseconds (CUDA events), when timing is on. */
+typedef struct {
+  long long cycles;
+  long long sweeps;
+  double bytes;
+  double cycle_ms;
+  long long launches;
+} bmg_counters;
+int bmg_get_counters (bmg_grid * grid, bmg_counters * c);
+int bmg_reset_counters (bmg_grid * grid);
+int bmg_set_timing (bmg_grid * grid, int on);
+/* use CUDA graphs for the V-cycles (default on) */
+int bmg_set_graphs (bmg_grid * grid, int on);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
