@@ -72,7 +72,8 @@ class MGSolve(ctypes.Structure):
 class bmg_counters(ctypes.Structure):
     _fields_ = [("cycles", ctypes.c_longlong), ("sweeps", ctypes.c_longlong),
                 ("bytes", ctypes.c_double), ("cycle_ms", ctypes.c_double),
-                ("launches", ctypes.c_longlong)]
+                ("launches", ctypes.c_longlong), ("relax_ms", ctypes.c_double),
+                ("relax_bytes", ctypes.c_double), ("relax_sweeps", ctypes.c_longlong)]
 
 
 # every function the header declares, with its signature

@@ -60,7 +60,7 @@ struct bmg_grid {
   int npartials;
   double * h_pinned;
   bmg_counters counters;
-  cudaEvent_t ev0, ev1;
+  cudaEvent_t ev0, ev1, evr0, evr1;
   struct graph_entry * graphs;     /* captured V-cycles, see run_cycle() */
   unsigned long long clock;
 };
@@ -97,7 +97,7 @@ static int fail (int s) { last_error = s; return s; }
    pure function of its parameters (cycle_key), so each distinct key is
    captured once into a CUDA graph and replayed afterwards */
 #define NGRAPH 16
-typedef struct { double bytes; long long launches, sweeps; } work_t;
+typedef struct { double bytes; long long launches, sweeps; double relax_bytes; long long relax_sweeps; } work_t;
 struct graph_entry {
   int valid;
   unsigned long long stamp;
@@ -198,6 +198,8 @@ int bmg_grid_new (bmg_grid ** out, int dim, int depth)
   CK (cudaMallocHost ((void **) &g->h_pinned, 4*sizeof (double)));
   CK (cudaEventCreate (&g->ev0));
   CK (cudaEventCreate (&g->ev1));
+  CK (cudaEventCreate (&g->evr0));
+  CK (cudaEventCreate (&g->evr1));
   g->graphs = calloc (NGRAPH, sizeof (struct graph_entry));
   *out = g;
   current_grid = g;
@@ -221,6 +223,7 @@ void bmg_grid_free (bmg_grid * g)
   cudaFree (g->d_maxres); cudaFree (g->d_partials); cudaFree (g->d_sum);
   cudaFreeHost (g->h_pinned);
   cudaEventDestroy (g->ev0); cudaEventDestroy (g->ev1);
+  cudaEventDestroy (g->evr0); cudaEventDestroy (g->evr1);
   if (g->own_stream) cudaStreamDestroy (g->stream);
   if (current_grid == g) current_grid = NULL;
   free (g);
@@ -734,6 +737,8 @@ static int cycle_launches (bmg_grid * g, field_t * a, const levels_t * lv, const
     launches++;
     const bmg_coef * al = st == BMG_ST_F64 ? c->alpha64[l] : c->alpha32[l];
     const bmg_coef la = st == BMG_ST_F64 ? c->lambda64[l] : c->lambda32[l];
+    const int timed = g->timing && l == L && maxlevel == L;
+    if (timed) CK (cudaEventRecord (g->evr0, s));
     for (int i = 0; i < nrelax; i++) {
       if (g->relax == BMG_RELAX_JACOBI) {
         CL (bmg_launch_relax (dim, st, BMG_SWEEP_JACOBI, gl, oth[l], cur[l], lv->res[l], al, la,
@@ -750,6 +755,11 @@ static int cycle_launches (bmg_grid * g, field_t * a, const levels_t * lv, const
       }
       bytes += narr*ncells (g, l)*es_of (st);
       sweeps++;
+    }
+    if (timed) {
+      CK (cudaEventRecord (g->evr1, s));
+      w->relax_bytes += nrelax*narr*ncells (g, l)*es_of (st);
+      w->relax_sweeps += nrelax;
     }
   }
   /* a += da on the finest level, with the BCs of a (poisson.h:84-89) */
@@ -771,7 +781,7 @@ static int cycle_launches (bmg_grid * g, field_t * a, const levels_t * lv, const
 
 /* everything that determines the launches of one solver iteration */
 typedef struct {
-  int nrelax, minlevel, relax, precision, dim, depth;
+  int nrelax, minlevel, relax, precision, dim, depth, timing;
   cudaStream_t stream;
   const void * a, * b;
   levels_t lv;
@@ -790,13 +800,13 @@ static int run_cycle (bmg_grid * g, field_t * a, const double * bdata, const lev
   cycle_key key;
   memset (&key, 0, sizeof key);
   key.nrelax = nrelax; key.minlevel = minlevel; key.relax = g->relax;
-  key.precision = g->precision; key.dim = g->dim; key.depth = L;
+  key.precision = g->precision; key.dim = g->dim; key.depth = L; key.timing = g->timing;
   key.stream = g->stream; key.a = a->lv[L]; key.b = bdata;
   key.lv = *lv; key.c = *c; key.dabc = *dabc;
   bcdesc_of (g, a, &key.abc);
   key.maxres = g->d_maxres; key.pinned = g->h_pinned;
 
-  work_t w = {0., 0, 0};
+  work_t w = {0., 0, 0, 0., 0};
   void * fin[BMG_MAXLEVEL + 1];
   if (g->use_graphs) {
     struct graph_entry * e = NULL, * victim = &g->graphs[0];
@@ -847,6 +857,10 @@ static int run_cycle (bmg_grid * g, field_t * a, const double * bdata, const lev
   g->counters.bytes += w.bytes;
   g->counters.launches += w.launches;
   g->counters.sweeps += w.sweeps;
+  if (g->timing) {
+    g->counters.relax_bytes += w.relax_bytes;
+    g->counters.relax_sweeps += w.relax_sweeps;
+  }
   return BMG_OK;
 }
 
@@ -904,7 +918,7 @@ static int solve (bmg_grid * g, field_t * a, field_t * b, coefs_t * c, int nrela
   }
 
   double resb;
-  work_t w0 = {0., 0, 0};
+  work_t w0 = {0., 0, 0, 0., 0};
   r = residual_max (g, a, bdata, c, lv.res[L], lv.st[L], &s.resb, 1, &w0);
   if (r) return r;
   resb = s.resa = s.resb;
@@ -920,9 +934,11 @@ static int solve (bmg_grid * g, field_t * a, field_t * b, coefs_t * c, int nrela
     s.resa = g->h_pinned[0];
     g->counters.cycles++;
     if (g->timing) {
-      float ms = 0.f;
+      float ms = 0.f, rms = 0.f;
       CK (cudaEventElapsedTime (&ms, g->ev0, g->ev1));
+      CK (cudaEventElapsedTime (&rms, g->evr0, g->evr1));
       g->counters.cycle_ms += ms;
+      g->counters.relax_ms += rms;
     }
     if (!isfinite (s.resa)) { status = BMG_ENAN; s.i++; break; }
     /* nrelax adaptation (poisson.h:198-204) */
@@ -949,7 +965,7 @@ static int solve (bmg_grid * g, field_t * a, field_t * b, coefs_t * c, int nrela
     else {
       /* widen the FP32 residual: recompute it in FP64 into the caller's field */
       double dummy;
-      work_t wr = {0., 0, 0};
+      work_t wr = {0., 0, 0, 0., 0};
       r = residual_max (g, a, bdata, c, resout->lv[L], BMG_ST_F64, &dummy, 0, &wr);
       if (r) return r;
     }
@@ -1045,7 +1061,7 @@ double bmg_residual (bmg_scalar * al, bmg_scalar * bl, bmg_scalar * resl, void *
   coefs_t c;
   if (resolve_coefs (g, p->alpha, p->lambda, &c)) return NAN;
   double m = NAN;
-  work_t w = {0., 0, 0};
+  work_t w = {0., 0, 0, 0., 0};
   if (residual_max (g, a, b->lv[g->depth], &c, res->lv[g->depth], BMG_ST_F64, &m, 1, &w)) return NAN;
   fail (BMG_OK);
   return m;
@@ -1102,7 +1118,7 @@ void mg_cycle (bmg_scalar * al, bmg_scalar * resl, bmg_scalar * dal,
   bmg_bcdesc dabc;
   bcdesc_of (g, da, &dabc);
   void * fin[BMG_MAXLEVEL + 1];
-  work_t w = {0., 0, 0};
+  work_t w = {0., 0, 0, 0., 0};
   if (cycle_launches (g, a, &lv, &c, &dabc, nrelax, minlevel, maxlevel, fin, &w)) return;
   /* Jacobi may leave a level's final iterate in the workspace partner */
   for (int l = minlevel; l <= maxlevel; l++)

@@ -1,0 +1,387 @@
+"""Benchmark: 2048^2 variable-coefficient Poisson solve to max residual 1e-6.
+
+Workload (seeded synthetic input, the reference publishes no data set): the
+two-phase projection problem on a 2048x2048 uniform grid (depth 11) --
+face alpha = 1/rho with rho = 1 inside a circle of radius 0.25 and 1000
+outside, blended by tanh over 2 cells; b ~ N(0, 1) per cell; Dirichlet a = 0
+on the four walls (basilisk_b200.problems.two_phase_2d).  One step = one
+poisson() solve from a = 0 to max|residual| <= 1e-6, as the reference's
+mg_solve does it (V-cycles, nrelax adaptation).
+
+Headline: the mixed form (FP32 cycles, FP64 iterative refinement), in
+solves/s; the plain FP64 form is measured beside it on the same input.
+Inputs live in HBM and exceed L2 (a, b, alpha_x, alpha_y and the hierarchy:
+~400 MB), and L2 is also flushed (a 256 MB write) before every timed step,
+outside the step's event pair.
+
+Under torchrun (N > 1) every rank solves its own instance (replicas: the
+solve does not shard); value = N * solves / max-over-ranks
+time.
+
+--impl reference times the reference algorithm's CPU implementation (the
+plain-C restatement in oracle/, OpenMP on all host threads, lexicographic
+Gauss-Seidel as the reference's default relax): full solves of the same
+workload (about 20 s each on 8 cores).
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = ("time-to-residual 1e-6 & V-cycle HBM GB/s, 2048²: mixed vs FP64 mg_solve, 1 B200")
+DEPTH = 11
+TOL = 1e-6
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.device_index = device_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device_index), "--query-gpu=" + self.Q,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        busy = [s for s in sm if smax and s > 0.3 * smax] or sm
+        return {"sm_mhz": statistics.median(busy) if busy else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_init():
+    import torch
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    elif torch.cuda.is_available():
+        torch.cuda.set_device(local)
+    return ws, rank, local
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(ws, v):
+    if ws == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+class Solver:
+    """The workload on one grid: fields created once, reset every step."""
+
+    def __init__(self, prob, precision, relax="rbgs"):
+        import torch
+        import basilisk_b200 as bmg
+        from basilisk_b200 import problems
+        self.torch = torch
+        self.g = bmg.Grid(2, prob["depth"], relax=relax, precision=precision)
+        self.g.set_stream(torch.cuda.current_stream().cuda_stream)
+        self.a, self.b, self.alpha, self.lam = problems.setup(self.g, prob)
+        n = 1 << prob["depth"]
+        self.zero = torch.zeros((n, n), dtype=torch.float64, device="cuda")
+        self.g.set_timing(True)
+
+    def step(self):
+        self.a.set(self.zero)
+        return self.g.poisson(self.a, self.b, alpha=self.alpha, lambda_=self.lam, tolerance=TOL)
+
+
+def flush_l2(buf):
+    buf.zero_()
+
+
+def time_steps(solver, steps, warmup, ws, flush):
+    import torch
+    for _ in range(warmup):
+        solver.step()
+    torch.cuda.synchronize()
+    barrier(ws)
+    solver.g.reset_counters()
+    times, stats = [], None
+    for _ in range(steps):
+        flush_l2(flush)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        stats = solver.step()
+        e1.record()
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+    barrier(ws)
+    return times, stats, solver.g.counters()
+
+
+def e2e_steps(prob, steps, warmup, precision):
+    """The public API with host buffers: every step copies the inputs
+    (a = 0, b, alpha_x, alpha_y) from pinned host memory to the device, solves,
+    and reads the solution back to pinned host memory."""
+    import torch
+    import basilisk_b200 as bmg
+    g = bmg.Grid(2, prob["depth"], relax="rbgs", precision=precision)
+    g.set_stream(torch.cuda.current_stream().cuda_stream)
+    a = g.scalar()
+    for side, (kind, val) in prob["bc"].items():
+        a.bc(side, kind, val)
+    b = g.scalar()
+    alpha = g.face_vector()
+    pin = lambda x: torch.from_numpy(np.ascontiguousarray(x)).pin_memory()
+    h_b = pin(prob["b"])
+    h_ax, h_ay = pin(prob["alpha"][0]), pin(prob["alpha"][1])
+    h_a0 = pin(np.zeros_like(prob["b"]))
+    h_out = torch.empty_like(h_b).pin_memory()
+    L = bmg._lib.load()
+
+    def put(f, h):
+        bmg._lib.check(L.bmg_field_set(g.ptr, f.scalar, h.data_ptr(), h.numel(), bmg._lib.HOST))
+
+    def one():
+        put(a, h_a0); put(b, h_b)
+        put(alpha.components[0], h_ax); put(alpha.components[1], h_ay)
+        st = g.poisson(a, b, alpha=alpha, tolerance=TOL)
+        bmg._lib.check(L.bmg_field_get(g.ptr, a.scalar, h_out.data_ptr(), h_out.numel(),
+                                       bmg._lib.HOST))
+        return st
+
+    for _ in range(warmup):
+        one()
+    torch.cuda.synchronize()
+    times = []
+    for _ in range(steps):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        one()
+        e1.record()
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+    h2d = sum(x.numel() * 8 for x in (h_a0, h_b, h_ax, h_ay))
+    d2h = h_out.numel() * 8
+    g.close()
+    return times, h2d, d2h
+
+
+def cpu_solve(prob, threads=None):
+    """One full solve of the workload by the oracle (plain-C restatement of
+    the reference's mg_solve, OpenMP on all host threads, the reference's
+    default lexicographic Gauss-Seidel relax).  Returns (seconds, mgstats)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from oracle import oracle
+    from helpers import oracle_grid
+    threads = threads or os.cpu_count()
+    g = oracle_grid(prob, relax=oracle.RELAX_GS, threads=threads)
+    t0 = time.perf_counter()
+    st = g.poisson(tolerance=TOL)
+    return time.perf_counter() - t0, st, threads
+
+
+def run_reference(args, ws, rank):
+    """The reference arm: the CPU implementation, full solves of the same
+    workload, on rank 0 only."""
+    from basilisk_b200 import problems
+    if rank != 0:
+        return
+    prob = problems.two_phase_2d(depth=DEPTH, seed=1)
+    budget = float(os.environ.get("BMG_CPU_BUDGET", "90"))
+    times, st, threads = [], None, None
+    for _ in range(max(1, args.steps)):
+        t, st, threads = cpu_solve(prob)
+        times.append(t)
+        if sum(times) > budget:
+            break
+    ms = 1e3 * sum(times) / len(times)
+    val = 1e3 / ms
+    line = {"impl": "reference", "metric": METRIC, "value": val, "unit": "solves/s",
+            "n_gpus": args.gpus, "steps": len(times), "warmup": 0, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": "two_phase_2d 2048^2 variable-coefficient Poisson, density "
+                                   "ratio 1000, b ~ N(0,1), Dirichlet 0, tolerance 1e-6",
+                       "grid": "2048x2048 (depth 11)", "parallelism": "cpu-openmp"},
+            "mgstats": {k: st[k] for k in ("i", "resb", "resa", "nrelax")},
+            "cpu_baseline": {"value": val, "unit": "solves/s", "cores": threads, "kind": "port",
+                             "sample": "%d full solve(s) of the same workload, lexicographic GS, "
+                                       "%d OpenMP threads" % (len(times), threads)},
+            "e2e": {"value": val, "unit": "solves/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="bmg", choices=["bmg", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline solve")
+    ap.add_argument("--profile", choices=["fp64", "mixed"], default=None,
+                    help="profiling run: only this form, no e2e, no CPU baseline, no JSON")
+    ap.add_argument("--depth", type=int, default=DEPTH, help="grid depth (profiling runs)")
+    args = ap.parse_args()
+    ws, rank, local = dist_init()
+    if args.impl == "reference":
+        run_reference(args, ws, rank)
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+
+    import torch
+    from basilisk_b200 import problems
+    peak, peak_kind = load_peaks()
+    prob = problems.two_phase_2d(depth=args.depth if args.profile else DEPTH, seed=1 + rank)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    if args.profile:
+        s = Solver(prob, args.profile)
+        t, st, c = time_steps(s, args.steps, args.warmup, ws, flush)
+        print("profile run: %s depth %d: %.3f ms/solve, %d cycles, nrelax %d, %d launches"
+              % (args.profile, prob["depth"], sum(t) / len(t), st["i"], st["nrelax"],
+                 c["launches"]), flush=True)
+        return
+
+    # plain FP64 form
+    s64 = Solver(prob, "fp64")
+    t64, st64, c64 = time_steps(s64, args.steps, args.warmup, ws, flush)
+    a64 = s64.a.get()
+    # mixed form (headline), with clocks sampled during its timed region
+    smx = Solver(prob, "mixed")
+    clocks = ClockSampler(local)
+    clocks.start()
+    tmx, stmx, cmx = time_steps(smx, args.steps, args.warmup, ws, flush)
+    clk = clocks.stop()
+    amx = smx.a.get()
+
+    ms_mx = max_over_ranks(ws, sum(tmx) / len(tmx))
+    ms_64 = max_over_ranks(ws, sum(t64) / len(t64))
+    err = float(np.abs(amx - a64).max() / np.abs(a64).max())
+
+    # e2e through the public API with host buffers (mixed form)
+    te2e, h2d, d2h = e2e_steps(prob, args.steps, max(1, args.warmup // 2), "mixed")
+    ms_e2e = max_over_ranks(ws, sum(te2e) / len(te2e))
+
+    if rank != 0:
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+
+    def cyc(c):
+        return {"cycles": c["cycles"], "sweeps": c["sweeps"],
+                "vcycle_gbs": c["bytes"] / (c["cycle_ms"] * 1e-3) / 1e9 if c["cycle_ms"] else None,
+                "relax_gbs": c["relax_bytes"] / (c["relax_ms"] * 1e-3) / 1e9 if c["relax_ms"] else None,
+                "bytes_per_cycle": c["bytes"] / max(1, c["cycles"]),
+                "ms_per_cycle": c["cycle_ms"] / max(1, c["cycles"])}
+
+    f64, fmx = cyc(c64), cyc(cmx)
+    relax_avg_ms = cmx["relax_ms"] / max(1, cmx["relax_sweeps"])
+    relax_bytes = cmx["relax_bytes"] / max(1, cmx["relax_sweeps"])
+    achieved = relax_bytes / (relax_avg_ms * 1e-3) / 1e9 if relax_avg_ms else None
+    line = {
+        "metric": METRIC, "value": ws * 1e3 / ms_mx, "unit": "solves/s", "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_mx,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
+        "data": "synthetic",
+        "config": {"workload": "two_phase_2d 2048^2 variable-coefficient Poisson, density ratio "
+                               "1000, b ~ N(0,1), Dirichlet 0, tolerance 1e-6",
+                   "grid": "2048x2048 (depth 11)", "form": "mixed FP32 cycles + FP64 refinement",
+                   "relax": "red-black Gauss-Seidel", "parallelism": "replicas" if ws > 1 else "1 gpu",
+                   "l2": "flushed (256 MB write) before every timed step; inputs > L2"},
+        "time_to_residual_ms": {"mixed": ms_mx, "fp64": ms_64, "speedup_mixed_vs_fp64": ms_64 / ms_mx},
+        "mgstats": {"mixed": {k: stmx[k] for k in ("i", "resb", "resa", "nrelax")},
+                    "fp64": {k: st64[k] for k in ("i", "resb", "resa", "nrelax")}},
+        "mixed_vs_fp64_rel_error": err,
+        "vcycle": {"mixed": fmx, "fp64": f64},
+        "roofline": {"bound": "hbm", "kernel": "k_relax (finest level, red+black sweep)",
+                     "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak if achieved else None,
+                     "traffic": None, "peak_kind": peak_kind},
+        "clocks": clk,
+        "gpu_launches": int(cmx["launches"]),
+        "e2e": {"value": ws * 1e3 / ms_e2e, "unit": "solves/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+    }
+    if not args.no_cpu:
+        try:
+            t, st, threads = cpu_solve(prob)
+            line["cpu_baseline"] = {
+                "value": 1.0 / t, "unit": "solves/s", "cores": threads, "kind": "port",
+                "sample": "1 full solve of the same workload (%d V-cycles, final nrelax %d), "
+                          "lexicographic GS, %d OpenMP threads" % (st["i"], st["nrelax"], threads)}
+        except Exception as e:  # the baseline is reported, never required
+            line["cpu_baseline"] = {"value": None, "unit": "solves/s", "cores": 0, "kind": "port",
+                                    "sample": "failed: %s" % e}
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -197,6 +197,11 @@ typedef struct {
   double bytes;
   double cycle_ms;
   long long launches;
+  /* the finest level's relaxation sweeps of each timed cycle, bracketed by
+     CUDA events: their device time and algorithmic bytes */
+  double relax_ms;
+  double relax_bytes;
+  long long relax_sweeps;
 } bmg_counters;
 int bmg_get_counters (bmg_grid * grid, bmg_counters * c);
 int bmg_reset_counters (bmg_grid * grid);
