@@ -161,6 +161,13 @@ static long long ncells (const bmg_grid * g, int l)
   return n;
 }
 
+/* level 0 of a grid with a periodic direction: the reference's periodic
+   boundary makes every neighbour of the single cell a copy of it */
+static int level0_periodic (const bmg_grid * g, int l)
+{
+  return l == 0 && (g->periodic[0] || g->periodic[1] || g->periodic[2]);
+}
+
 static double delta_of (const bmg_grid * g, int l)
 {
   return g->L0*(1./(1 << l));    /* cartesian-common.h:11, multigrid.h:14 */
@@ -445,9 +452,11 @@ int bmg_field_set_level (bmg_grid * g, bmg_scalar s, int level, const double * v
   int st = stage_in (g, values, count, memory, &d, &tmp);
   if (st) return st;
   CL (bmg_launch_pack (g->dim, BMG_ST_F64, g->g64[level], f->face_dim, d, f->lv[level], g->stream));
-  if (f->face_dim >= 0 && g->periodic[f->face_dim])
+  if (f->face_dim >= 0 && (g->periodic[f->face_dim] || level0_periodic (g, level)))
     /* periodic face vectors: the last face is the image of the first
-       (periodic_boundary_level_x copies face vectors, multigrid.h:644-647) */
+       (periodic_boundary_level_x copies face vectors, multigrid.h:644-647);
+       on a periodic level 0 every neighbour slot takes the cell's value,
+       the upper face of every component included (multigrid.h:655-664) */
     CL (bmg_launch_face_wrap (g->dim, g->g64[level], f->face_dim, f->lv[level], g->stream));
   if (tmp) CK (cudaFreeAsync (tmp, g->stream));
   if (f->face_dim < 0 && level == g->depth) {
@@ -645,7 +654,8 @@ static int restrict_coefs (bmg_grid * g, const coefs_t * c)
         fine[d] = (const double *) c->alpha64[l + 1][d].p;
         coarse[d] = (double *) c->alpha64[l][d].p;
       }
-      CL (bmg_launch_restrict_face (g->dim, g->g64[l + 1], g->g64[l], fine, coarse, g->stream));
+      CL (bmg_launch_restrict_face (g->dim, g->g64[l + 1], g->g64[l], fine, coarse,
+                                    level0_periodic (g, l), g->stream));
     }
     if (c->lambda_stored)
       CL (bmg_launch_restrict (g->dim, BMG_ST_F64, BMG_ST_F64, g->g64[l + 1], g->g64[l],
@@ -738,7 +748,7 @@ static int cycle_launches (bmg_grid * g, field_t * a, const levels_t * lv, const
     const bmg_coef * al = st == BMG_ST_F64 ? c->alpha64[l] : c->alpha32[l];
     const bmg_coef la = st == BMG_ST_F64 ? c->lambda64[l] : c->lambda32[l];
     const int timed = g->timing && l == L && maxlevel == L;
-    if (timed) CK (cudaEventRecord (g->evr0, s));
+    if (timed) CK (cudaEventRecordWithFlags (g->evr0, s, cudaEventRecordExternal));
     for (int i = 0; i < nrelax; i++) {
       if (g->relax == BMG_RELAX_JACOBI) {
         CL (bmg_launch_relax (dim, st, BMG_SWEEP_JACOBI, gl, oth[l], cur[l], lv->res[l], al, la,
@@ -757,7 +767,7 @@ static int cycle_launches (bmg_grid * g, field_t * a, const levels_t * lv, const
       sweeps++;
     }
     if (timed) {
-      CK (cudaEventRecord (g->evr1, s));
+      CK (cudaEventRecordWithFlags (g->evr1, s, cudaEventRecordExternal));
       w->relax_bytes += nrelax*narr*ncells (g, l)*es_of (st);
       w->relax_sweeps += nrelax;
     }
@@ -822,6 +832,7 @@ static int run_cycle (bmg_grid * g, field_t * a, const double * bdata, const lev
         victim->valid = 0;
       }
       cudaGraph_t graph;
+      memset (&victim->w, 0, sizeof victim->w);
       CK (cudaStreamBeginCapture (g->stream, cudaStreamCaptureModeThreadLocal));
       int r = cycle_launches (g, a, lv, c, dabc, nrelax, minlevel, L, fin, &victim->w);
       double dummy;
@@ -1153,7 +1164,8 @@ int bmg_restriction (bmg_grid * g, const bmg_scalar * list)
           if (!fd || fd->face_dim != d) return fail (BMG_EINVAL);
           fine[d] = fd->lv[l + 1]; coarse[d] = fd->lv[l];
         }
-        CL (bmg_launch_restrict_face (g->dim, g->g64[l + 1], g->g64[l], fine, coarse, g->stream));
+        CL (bmg_launch_restrict_face (g->dim, g->g64[l + 1], g->g64[l], fine, coarse,
+                                      level0_periodic (g, l), g->stream));
       }
     }
     else

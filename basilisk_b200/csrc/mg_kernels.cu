@@ -355,7 +355,7 @@ struct FacePtrs {
    rotation of the fine() offsets; every coarse cell writes its lower face,
    the last cell along each axis also its upper face. */
 template <int DIM>
-__global__ void k_restrict_face (bmg_geom gf, bmg_geom gc, FacePtrs p)
+__global__ void k_restrict_face (bmg_geom gf, bmg_geom gc, FacePtrs p, int level0p)
 {
   int i, j, k;
   if (!cell_of_thread<DIM> (gc.n, i, j, k)) return;
@@ -383,6 +383,11 @@ __global__ void k_restrict_face (bmg_geom gf, bmg_geom gc, FacePtrs p)
       }
       const int ii = e == 0 ? i + side : i, jj = e == 1 ? j + side : j, kk = e == 2 ? k + side : k;
       c[cidx<DIM> (gc, ii, jj, kk)] = v;
+      if (level0p) {
+        /* periodic level 0: the upper face is a copy of the lower one */
+        c[cidx<DIM> (gc, e == 0 ? 1 : 0, e == 1 ? 1 : 0, e == 2 ? 1 : 0)] = v;
+        break;
+      }
     }
   }
 #undef FV
@@ -695,9 +700,9 @@ void restrict_dim (int stf, int stc, bmg_geom gf, bmg_geom gc, const void * f, v
 }
 
 template <int DIM>
-void restrict_face_dim (bmg_geom gf, bmg_geom gc, FacePtrs p, cudaStream_t s)
+void restrict_face_dim (bmg_geom gf, bmg_geom gc, FacePtrs p, int level0p, cudaStream_t s)
 {
-  k_restrict_face<DIM><<<grid_shape<DIM> (gc.n), block_shape<DIM> (), 0, s>>> (gf, gc, p);
+  k_restrict_face<DIM><<<grid_shape<DIM> (gc.n), block_shape<DIM> (), 0, s>>> (gf, gc, p, level0p);
 }
 
 template <int DIM>
@@ -821,14 +826,14 @@ int bmg_launch_restrict (int dim, int st_fine, int st_coarse, bmg_geom gf, bmg_g
 }
 
 int bmg_launch_restrict_face (int dim, bmg_geom gf, bmg_geom gc, const double * const * fine,
-                              double * const * coarse, cudaStream_t s)
+                              double * const * coarse, int level0p, cudaStream_t s)
 {
   FacePtrs p;
   for (int e = 0; e < 3; e++) {
     p.f[e] = e < dim ? fine[e] : 0;
     p.c[e] = e < dim ? coarse[e] : 0;
   }
-  DISPATCH_DIM (dim, restrict_face_dim, gf, gc, p, s);
+  DISPATCH_DIM (dim, restrict_face_dim, gf, gc, p, level0p, s);
   return status_of_launch ();
 }
 

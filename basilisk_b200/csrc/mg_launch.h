@@ -68,9 +68,11 @@ int bmg_launch_restrict (int dim, int st_fine, int st_coarse, bmg_geom gf,
                          bmg_geom gc, const void * fine, void * coarse,
                          cudaStream_t s);
 
+/* level0p: the coarse level is a periodic level 0, whose upper faces are
+   copies of the lower ones */
 int bmg_launch_restrict_face (int dim, bmg_geom gf, bmg_geom gc,
                               const double * const * fine, double * const * coarse,
-                              cudaStream_t s);
+                              int level0p, cudaStream_t s);
 
 int bmg_launch_residual (int dim, int st_res, bmg_geom g, bmg_geom gres,
                          const double * a, const double * b,
