@@ -120,6 +120,7 @@ SIGNATURES = {
     "bmg_reset_counters": (I, [P]),
     "bmg_set_timing": (I, [P, I]),
     "bmg_set_graphs": (I, [P, I]),
+    "bmg_sum_noalloc": (I, [P, SZ, P, P]),
 }
 GLOBALS = {"NITERMAX": ctypes.c_int, "NITERMIN": ctypes.c_int, "TOLERANCE": ctypes.c_double}
 

@@ -33,6 +33,7 @@
  */
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <stdio.h>
 #include "mg_launch.h"
 
 namespace {
@@ -793,6 +794,92 @@ void shift_dim (bmg_geom g, double * f, const double * sum, double scale, cudaSt
 }
 
 } // namespace
+
+
+/* ---------------------------------------------------------------- */
+/* allocation-free sum                                               */
+/* ---------------------------------------------------------------- */
+
+/* Scratch of bmg_sum_noalloc: one partial sum per tile of BMG_NOALLOC_TILE
+   values.  A file-scope device array, so every GPU that loads the library
+   holds these 32 KB until the process exits, and every call shares them. */
+#define BMG_NOALLOC_THREADS 256
+#define BMG_NOALLOC_TILE (BMG_NOALLOC_THREADS*16)
+#define BMG_NOALLOC_PARTIALS 4096
+static __device__ __align__(256) double bmg_noalloc_scratch[BMG_NOALLOC_PARTIALS];
+
+namespace {
+
+/* stage 1: block b sums values [b*TILE, (b+1)*TILE) in a fixed order */
+__global__ void k_sum_noalloc_partial (const double * __restrict__ v, long long count,
+                                       double * partials)
+{
+  __shared__ double sm[32];
+  const long long base = (long long) blockIdx.x*BMG_NOALLOC_TILE;
+  double s = 0.;
+  for (int r = 0; r < BMG_NOALLOC_TILE/BMG_NOALLOC_THREADS; r++) {
+    const long long q = base + (long long) r*BMG_NOALLOC_THREADS + threadIdx.x;
+    if (q < count) s += v[q];
+  }
+  s = block_sum (s, sm);
+  if (threadIdx.x == 0) partials[blockIdx.x] = s;
+}
+
+/* stage 2: one block sums the partials written by this call's stage 1 */
+__global__ void k_sum_noalloc_final (const double * partials, int np, double * out)
+{
+  __shared__ double sm[32];
+  double s = 0.;
+  for (int q = threadIdx.x; q < np; q += blockDim.x) s += partials[q];
+  s = block_sum (s, sm);
+  if (threadIdx.x == 0) *out = s;
+}
+
+} // namespace
+
+#define BMG_NOALLOC_MAXDEV 64
+static double * noalloc_scratch_ptr[BMG_NOALLOC_MAXDEV];
+
+extern "C" int bmg_sum_noalloc (const double * values, size_t count, double * result,
+                                void * stream)
+{
+  const size_t maxcount = (size_t) BMG_NOALLOC_PARTIALS*BMG_NOALLOC_TILE;
+  if (!result || (count > 0 && !values))
+    return 1; /* BMG_EINVAL */
+  if (count > maxcount) {
+    fprintf (stderr, "bmg_sum_noalloc: %zu values exceed the maximum of %zu "
+             "(%d partial sums of %d values in the static scratch)\n",
+             count, maxcount, BMG_NOALLOC_PARTIALS, BMG_NOALLOC_TILE);
+    return 1; /* BMG_EINVAL */
+  }
+  int dev = 0;
+  if (cudaGetDevice (&dev) != cudaSuccess || dev < 0 || dev >= BMG_NOALLOC_MAXDEV) {
+    cudaGetLastError ();
+    return 7; /* BMG_ENODEV */
+  }
+  /* once per device, with that device current: the device address of the
+     scratch array (its name in host code is only a stand-in) */
+  if (!noalloc_scratch_ptr[dev]) {
+    void * p = NULL;
+    cudaError_t e = cudaGetSymbolAddress (&p, bmg_noalloc_scratch);
+    if (e != cudaSuccess || !p) {
+      fprintf (stderr, "bmg_sum_noalloc: cudaGetSymbolAddress failed: %s\n",
+               cudaGetErrorString (e));
+      return 2; /* BMG_ECUDA */
+    }
+    noalloc_scratch_ptr[dev] = (double *) p;
+  }
+  cudaStream_t s = (cudaStream_t) stream;
+  const int np = (int) ((count + BMG_NOALLOC_TILE - 1)/BMG_NOALLOC_TILE);
+  /* nothing accumulates across calls: stage 1 overwrites the np partials
+     that stage 2 reads, and stage 2 overwrites *result (count 0: one empty
+     partial, a sum of 0) */
+  const int nb = np > 0 ? np : 1;
+  k_sum_noalloc_partial<<<nb, BMG_NOALLOC_THREADS, 0, s>>> (values, (long long) count,
+                                                             noalloc_scratch_ptr[dev]);
+  k_sum_noalloc_final<<<1, 1024, 0, s>>> (noalloc_scratch_ptr[dev], nb, result);
+  return cudaGetLastError () == cudaSuccess ? 0 : 2;
+}
 
 /* ---------------------------------------------------------------- */
 /* C launchers                                                       */

@@ -185,6 +185,24 @@ void mg_cycle (bmg_scalar * a, bmg_scalar * res, bmg_scalar * da,
    as test/variable.c calls it for its face coefficients; list ends with .i=0 */
 int bmg_restriction (bmg_grid * grid, const bmg_scalar * list);
 
+/* ---- allocation-free sum ------------------------------------------- */
+
+/* The sum of count doubles at values (device memory), written to *result
+   (device memory) on stream (a cudaStream_t, NULL = the default stream):
+   the Sigma b that mg_solve reports in mgstats.sum, for callers that cannot
+   allocate device memory -- code running while a stream is captured into a
+   CUDA graph in global capture mode, where cudaMalloc is refused, or
+   programs that hand all device memory to their own pool at start-up and
+   let nothing else allocate.  It allocates nothing: its scratch is a static
+   32 KB device array inside the library (4096 partial sums), so count is at
+   most 16,777,216 (4096^2 in 2D, 256^3 in 3D); larger counts are rejected
+   with BMG_EINVAL and a message on stderr.  The first call on a device looks
+   up the scratch's device address with that device current; make that
+   first call before any stream capture.  All calls share the scratch: calls
+   that overlap on the GPU (different streams, no ordering) race.  The
+   result is asynchronous on stream.  No counterpart in the reference. */
+int bmg_sum_noalloc (const double * values, size_t count, double * result, void * stream);
+
 /* ---- measurement ---------------------------------------------------- */
 
 /* totals since the grid was created: V-cycles, relaxation sweeps per level
