@@ -1,0 +1,780 @@
+/*
+ * mg_fused.cu -- fused relaxation kernels of the multigrid solver.
+ *
+ * The reference's V-cycle (poisson.h:32-90) relaxes every level nrelax times,
+ * and mg_solve raises nrelax while a cycle reduces the residual by less than
+ * 1.2 (poisson.h:198-204): on stiff problems nrelax reaches 30-50, so the
+ * solve is a long chain of small relaxation sweeps.  Two kernels replace the
+ * one-launch-per-colour sweeps of mg_kernels.cu on the red-black path:
+ *
+ *   k_relax_tile2d  S complete red-black sweeps of a 2D level in one launch.
+ *                   Each CTA stages a TS x TS tile plus a 2S-cell halo of
+ *                   da, res, alpha_x, alpha_y (and lambda) in shared memory,
+ *                   updates red then black cells on a region that shrinks by
+ *                   one cell per colour pass, and writes the TS x TS interior
+ *                   back to the partner buffer (CTAs read halos that other
+ *                   CTAs own, so a launch never writes what it reads).  The
+ *                   halo is recomputed redundantly, so each array is read
+ *                   about once per S sweeps instead of twice per sweep.
+ *   k_bottom        the coarse end of the cycle in one single-CTA launch:
+ *                   restriction of res down to minlevel, the coarsest zero,
+ *                   then for each level up to a small one the bilinear
+ *                   prolongation and all nrelax sweeps, with __syncthreads
+ *                   between colour passes.  Those levels are pure latency
+ *                   when each pass is a launch.
+ *
+ * Both compute every cell update with relax_value's expression and order and
+ * write the same ghost images as the unfused kernels, so their results are
+ * bit-identical to the red / boundary / black sequence of the oracle.
+ */
+#include <cuda_runtime.h>
+#include <stdio.h>
+#include <string.h>
+#include "mg_device.cuh"
+
+using namespace bmgd;
+
+namespace {
+
+/* ---------------------------------------------------------------- */
+/* tile-fused red-black sweeps, 2D                                    */
+/* ---------------------------------------------------------------- */
+
+/* a global index along one axis: its periodic image, or -1 when it is a
+   box ghost or outside the domain (never updated) */
+__device__ __forceinline__ int real_index (int gi, int n, int periodic)
+{
+  if (gi >= 0 && gi < n) return gi;
+  if (!periodic) return -1;
+  int r = gi % n;
+  return r < 0 ? r + n : r;
+}
+
+/* a face index along its own axis (faces 0..n; face n of a periodic
+   direction is face 0) */
+__device__ __forceinline__ int real_face (int f, int n, int periodic)
+{
+  if (f >= 0 && f <= n) return (periodic && f == n) ? 0 : f;
+  if (!periodic) return -1;
+  int r = f % n;
+  return r < 0 ? r + n : r;
+}
+
+/* Shared-memory tile of TS x TS cells plus a 2S halo, stored split by
+   colour: colour c = (i + j) & 1 of cell (i, j) (global indices); cell
+   (p, q) of the staged region lives in the colour-c arrays at [p][q >> 1].
+   A colour pass then reads its neighbours (all of the other colour) with
+   unit stride: up/down at [p -+ 1][m], left/right at [p][m - 1 + o] and
+   [p][m + o], o the column offset of colour c in row p. */
+/* asynchronous global -> shared copy of one element (cp.async, sm_80+), with
+   zero fill when the source is not a real cell: all staging loads of a
+   thread are in flight at once instead of one dependent load per step */
+template <typename T>
+__device__ __forceinline__ void cp_async_elem (T * smem, const T * gmem, bool valid)
+{
+  const unsigned s = (unsigned) __cvta_generic_to_shared (smem);
+  const int sz = valid ? (int) sizeof (T) : 0;
+  if (sizeof (T) == 8)
+    asm volatile ("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" :: "r"(s), "l"(gmem), "r"(sz) : "memory");
+  else
+    asm volatile ("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" :: "r"(s), "l"(gmem), "r"(sz) : "memory");
+}
+
+__device__ __forceinline__ void cp_async_wait_all ()
+{
+  asm volatile ("cp.async.commit_group;\n" ::: "memory");
+  asm volatile ("cp.async.wait_group 0;\n" ::: "memory");
+}
+
+template <typename T, int TS, int S>
+struct TileShape {
+  static constexpr int H = 2*S;        /* halo: one cell per colour pass */
+  static constexpr int W = TS + 2*H;   /* staged cells per side (even) */
+  static constexpr int M = W/2;        /* cells of one colour per row */
+  static_assert (W % 2 == 0, "staged width must be even");
+  static constexpr int MY = M + 2;     /* y-face row pitch (even: aligned pairs) */
+  /* da, res, (lambda): 2 colours x W x M; alpha_x faces: 2 x (W+1) x M;
+     alpha_y faces: 2 x W x MY */
+  static constexpr size_t elems (bool lam)
+  {
+    return (size_t) 2*W*M*(lam ? 3 : 2) + (size_t) 2*(W + 1)*M + (size_t) 2*W*MY;
+  }
+  static constexpr size_t bytes (bool lam) { return sizeof (T)*elems (lam); }
+};
+
+/* the cell update's division: IEEE for FP64 (the plain form is
+   bit-compared with the oracle), the fast reciprocal-multiply for the FP32
+   smoothing of the mixed form, whose rounding the FP64 outer residual
+   corrects anyway */
+__device__ __forceinline__ double relax_div (double n, double d) { return n/d; }
+__device__ __forceinline__ float relax_div (float n, float d) { return __fdividef (n, d); }
+
+template <typename T> struct Pair;
+template <> struct Pair<float> { typedef float2 type; };
+template <> struct Pair<double> { typedef double2 type; };
+
+/* BX x BY threads: thread (tx, ty) updates the cell pair 2 tx, 2 tx + 1 of
+   row ty + lo in every colour pass */
+template <typename T, int TS, int S, bool LAM, int BX, int BY>
+__global__ void __launch_bounds__ (BX*BY)
+k_relax_tile2d (bmg_geom g, T * __restrict__ out, const T * __restrict__ in,
+                const T * __restrict__ res, Coef<T> ax, Coef<T> ay, Coef<T> lam, T Delta, BCH bc,
+                int nsweeps)
+{
+  typedef TileShape<T, TS, S> Sh;
+  constexpr int H = Sh::H, W = Sh::W, M = Sh::M, MY = Sh::MY;
+  static_assert (M % 2 == 0 && M <= 2*BX && W - 2 <= BY, "one pair of cells per thread per row");
+  typedef typename Pair<T>::type T2;
+  extern __shared__ __align__ (16) unsigned char smem_raw[];
+  T * sa[2], * sr[2], * sx[2], * sy[2], * sl[2];
+  {
+    T * p = (T *) smem_raw;
+    for (int c = 0; c < 2; c++) { sa[c] = p; p += W*M; }
+    for (int c = 0; c < 2; c++) { sr[c] = p; p += W*M; }
+    for (int c = 0; c < 2; c++) { sx[c] = p; p += (W + 1)*M; }
+    for (int c = 0; c < 2; c++) { sy[c] = p; p += W*MY; }
+    for (int c = 0; c < 2; c++) { sl[c] = p; p += LAM ? W*M : 0; }
+  }
+  const int n = g.n, tx = threadIdx.x, ty = threadIdx.y;
+  const int tid = ty*BX + tx, nth = BX*BY;
+  const int i0 = blockIdx.y*TS - H, j0 = blockIdx.x*TS - H;   /* global index of (0,0) */
+  const int px = bc.periodic[0], py = bc.periodic[1];
+  const int base = (i0 + j0) & 1;                             /* colour of (0,0) */
+  /* the whole staged region inside the domain: no cell checks needed */
+  const bool inner = i0 >= 0 && i0 + W <= n && j0 >= 0 && j0 + W <= n;
+
+  /* stage cells and faces with asynchronous copies (zero fill outside) */
+  for (int idx = tid; idx < W*W; idx += nth) {
+    const int p = idx/W, q = idx - p*W;
+    const int c = (base + p + q) & 1, m = q >> 1;
+    const int ri = real_index (i0 + p, n, px), rj = real_index (j0 + q, n, py);
+    const bool ok = ri >= 0 && rj >= 0;
+    const long long id = ok ? cidx<2> (g, ri, rj, 0) : 0;
+    cp_async_elem (&sa[c][p*M + m], in + id, ok);
+    cp_async_elem (&sr[c][p*M + m], res + id, ok);
+    if (LAM) cp_async_elem (&sl[c][p*M + m], lam.p + id, ok);
+  }
+  /* x faces: W+1 rows of W (face (p, q): lower face of cell (p, q)) */
+  for (int idx = tid; idx < (W + 1)*W; idx += nth) {
+    const int p = idx/W, q = idx - p*W;
+    const int c = (base + p + q) & 1;
+    const int fi = real_face (i0 + p, n, px), rj = real_index (j0 + q, n, py);
+    const bool ok = fi >= 0 && rj >= 0;
+    if (ax.p) cp_async_elem (&sx[c][p*M + (q >> 1)], ax.p + (ok ? cidx<2> (g, fi, rj, 0) : 0), ok);
+    else sx[c][p*M + (q >> 1)] = ok ? ax.c : T(0);
+  }
+  /* y faces: W rows of W+1 (face (p, q): left face of cell (p, q)) */
+  for (int idx = tid; idx < W*(W + 1); idx += nth) {
+    const int p = idx/(W + 1), q = idx - p*(W + 1);
+    const int c = (base + p + q) & 1;
+    const int ri = real_index (i0 + p, n, px), fj = real_face (j0 + q, n, py);
+    const bool ok = ri >= 0 && fj >= 0;
+    if (ay.p) cp_async_elem (&sy[c][p*MY + (q >> 1)], ay.p + (ok ? cidx<2> (g, ri, fj, 0) : 0), ok);
+    else sy[c][p*MY + (q >> 1)] = ok ? ay.c : T(0);
+  }
+  cp_async_wait_all ();
+  __syncthreads ();
+
+  /* box ghosts (global -1 and n) of the staged region: ghost = factor x
+     mirror, both of opposite colours at the same or adjacent column index */
+  const int glo_i = px ? -1 : -1 - i0, ghi_i = px ? -1 : n - i0;
+  const int glo_j = py ? -1 : -1 - j0, ghi_j = py ? -1 : n - j0;
+  const bool has_ghosts = !inner &&
+    ((glo_i >= 0 && glo_i < W) || (ghi_i >= 0 && ghi_i < W) ||
+     (glo_j >= 0 && glo_j < W) || (ghi_j >= 0 && ghi_j < W));
+  auto refresh = [&] () {
+    for (int t = tid; t < 4*W; t += nth) {
+      const int line = t/W, u = t - line*W;
+      int p, q, pm, qm, f;
+      if (line == 0) { p = glo_i; q = u; pm = p + 1; qm = q; f = bc.fac[1]; }
+      else if (line == 1) { p = ghi_i; q = u; pm = p - 1; qm = q; f = bc.fac[0]; }
+      else if (line == 2) { p = u; q = glo_j; pm = p; qm = q + 1; f = bc.fac[3]; }
+      else { p = u; q = ghi_j; pm = p; qm = q - 1; f = bc.fac[2]; }
+      if (p < 0 || p >= W || q < 0 || q >= W || pm < 0 || pm >= W || qm < 0 || qm >= W)
+        continue;
+      if (line < 2 ? real_index (j0 + q, n, py) < 0 : real_index (i0 + p, n, px) < 0)
+        continue;
+      const int c = (base + p + q) & 1;
+      sa[c][p*M + (q >> 1)] = sa[c ^ 1][pm*M + (qm >> 1)]*T(f);
+    }
+  };
+  if (has_ghosts) refresh ();
+  __syncthreads ();
+
+  const T D2 = Delta*Delta;
+  for (int sw = 0; sw < nsweeps; sw++)
+    for (int c = 0; c < 2; c++) {
+      const int k = 2*sw + c;
+      const int lo = k + 1, hi = W - k - 1;      /* valid update region [lo, hi)^2 */
+      const T * __restrict__ o_a = sa[c ^ 1];
+      const T * __restrict__ xr = sx[c], * __restrict__ xo = sx[c ^ 1];
+      const T * __restrict__ yr = sy[c], * __restrict__ yo = sy[c ^ 1];
+      T * __restrict__ a = sa[c];
+      const T * __restrict__ r = sr[c];
+      const T * __restrict__ l = sl[c];
+      /* thread (tx, ty): cells m0 = 2 tx and m0 + 1 of colour c in row lo + ty */
+      const int p = lo + ty;
+      if (p < hi) {
+        const int o = (c - base - p) & 1;        /* column offset of colour c */
+        const int mlo = (lo - o + 1) >> 1, mhi = (hi - o + 1) >> 1;
+        const int m0 = 2*tx;
+        bool ok0 = m0 >= mlo && m0 < mhi, ok1 = m0 + 1 >= mlo && m0 + 1 < mhi;
+        if (!inner) {
+          const int gi = i0 + p, gj = j0 + 2*m0 + o;
+          const bool rowok = px || (unsigned) gi < (unsigned) n;
+          ok0 = ok0 && rowok && (py || (unsigned) gj < (unsigned) n);
+          ok1 = ok1 && rowok && (py || (unsigned) (gj + 2) < (unsigned) n);
+        }
+        if (ok0 || ok1) {
+          const int ci = p*M + m0;
+          const T2 up = *(const T2 *) &o_a[ci - M], dn = *(const T2 *) &o_a[ci + M];
+          /* the other colour's cells left and right: [m0-1+o], [m0+o], [m0+1+o] */
+          T vl, vm, vr;
+          if (o == 0) {
+            const T2 v = *(const T2 *) &o_a[ci];
+            vl = o_a[ci - 1]; vm = v.x; vr = v.y;
+          }
+          else {
+            const T2 v = *(const T2 *) &o_a[ci];
+            vl = v.x; vm = v.y; vr = o_a[ci + 2];
+          }
+          const T2 rr = *(const T2 *) &r[ci];
+          const T2 xl = *(const T2 *) &xr[ci], xu = *(const T2 *) &xo[ci + M];
+          const T2 yl = *(const T2 *) &yr[p*MY + m0];
+          T yr0, yr1;
+          if (o == 0) { const T2 v = *(const T2 *) &yo[p*MY + m0]; yr0 = v.x; yr1 = v.y; }
+          else { yr0 = yo[p*MY + m0 + 1]; yr1 = yo[p*MY + m0 + 2]; }
+          T2 lv;
+          if (LAM) lv = *(const T2 *) &l[ci];
+          else { lv.x = lam.c; lv.y = lam.c; }
+          /* relax_value's expression and order (poisson.h:303-319), two cells */
+          T n0 = (-D2)*rr.x, d0 = (-lv.x)*D2;
+          T n1 = (-D2)*rr.y, d1 = (-lv.y)*D2;
+          n0 += xu.x*dn.x + xl.x*up.x; d0 += xu.x + xl.x;
+          n1 += xu.y*dn.y + xl.y*up.y; d1 += xu.y + xl.y;
+          n0 += yr0*vm + yl.x*vl;      d0 += yr0 + yl.x;
+          n1 += yr1*vr + yl.y*vm;      d1 += yr1 + yl.y;
+          const T a0 = relax_div (n0, d0), a1 = relax_div (n1, d1);
+          if (ok0 && ok1) { T2 w; w.x = a0; w.y = a1; *(T2 *) &a[ci] = w; }
+          else if (ok0) a[ci] = a0;
+          else a[ci + 1] = a1;
+        }
+      }
+      __syncthreads ();
+      if (has_ghosts) {
+        refresh ();
+        __syncthreads ();
+      }
+    }
+
+  /* write the tile interior back, with its ghost images */
+  for (int idx = tid; idx < TS*TS; idx += nth) {
+    const int rr = idx/TS, s = idx - rr*TS;
+    const int gi = blockIdx.y*TS + rr, gj = blockIdx.x*TS + s;
+    if (gi >= n || gj >= n) continue;
+    const int p = rr + H, q = s + H;
+    const T v = sa[(base + p + q) & 1][p*M + (q >> 1)];
+    out[cidx<2> (g, gi, gj, 0)] = v;
+    ghosts_homog<2, T> (out, g, gi, gj, 0, v, bc);
+  }
+}
+
+/* ---------------------------------------------------------------- */
+/* single-CTA bottom of the cycle                                    */
+/* ---------------------------------------------------------------- */
+
+typedef bmg_bottom_level BotLevel;
+
+#define BOT_MAXLEVELS 14
+/* levels up to this size use the small relaxation tiles */
+#define BMG_SMALL_TILE_N 256
+/* staged levels up to this many padded cells are relaxed by one warp */
+#define BOT_WARP_CELLS 400
+
+/* a staged level: its global arrays and their shared-memory copies, which
+   use a compact padded layout described by a bmg_geom of its own (pitch
+   n+2, offset 1), so relax_value and ghosts_homog apply unchanged */
+struct BotStage {
+  bmg_geom gs;                  /* shared-memory geometry */
+  unsigned off_da, off_res, off_alpha[3], off_lambda;   /* byte offsets, ~0u = absent */
+};
+
+struct BotParams {
+  BotLevel lv[BOT_MAXLEVELS];   /* levels lo..hi at indices 0..hi-lo */
+  BotStage sm[BOT_MAXLEVELS];
+  bmg_geom g_src;               /* level hi+1: the restricted res comes from it */
+  const void * res_src;
+  int st_src;
+  int nlev, nrelax, restrict_src;
+  BCH bc;
+};
+
+__device__ __forceinline__ void * sm_at (unsigned char * base, unsigned off)
+{
+  return off == ~0u ? NULL : (void *) (base + off);
+}
+
+template <int DIM>
+__device__ __forceinline__ void decode_padded (long long q, int e, int & i, int & j, int & k)
+{
+  /* q over (n+2)^DIM positions -> (i, j, k) in [-1, n]^DIM, e = n + 2 */
+  if (DIM == 1) { i = (int) q - 1; j = k = 0; }
+  else if (DIM == 2) { i = (int) (q/e) - 1; j = (int) (q % e) - 1; k = 0; }
+  else { i = (int) (q/((long long) e*e)) - 1; long long r = q % ((long long) e*e); j = (int) (r/e) - 1; k = (int) (r % e) - 1; }
+}
+
+/* copy every position [-1, n]^DIM of a level array between global and shared
+   memory: one warp per row of the contiguous axis, no index divisions */
+template <int DIM, typename T>
+__device__ __forceinline__ void bot_copy (const bmg_geom & gg, T * gp, const bmg_geom & gs, T * sp,
+                                          int to_shared)
+{
+  const int e = gs.n + 2;
+  const int rows = DIM == 1 ? 1 : DIM == 2 ? e : e*e;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  for (int r = warp; r < rows; r += nw) {
+    int i, j;
+    if (DIM == 1) { i = 0; j = 0; }
+    else if (DIM == 2) { i = r - 1; j = 0; }
+    else { i = r/e - 1; j = r - (i + 1)*e - 1; }
+    for (int k = lane - 1; k < e - 1; k += 32) {
+      long long gi, si;
+      if (DIM == 1) { gi = cidx<1> (gg, k, 0, 0); si = cidx<1> (gs, k, 0, 0); }
+      else if (DIM == 2) { gi = cidx<2> (gg, i, k, 0); si = cidx<2> (gs, i, k, 0); }
+      else { gi = cidx<3> (gg, i, j, k); si = cidx<3> (gs, i, j, k); }
+      if (to_shared) sp[si] = gp[gi];
+      else gp[gi] = sp[si];
+    }
+  }
+}
+
+template <int DIM>
+__device__ __forceinline__ void bot_copy_st (int st, const bmg_geom & gg, const void * gp, const bmg_geom & gs,
+                             void * sp, int to_shared)
+{
+  if (st == BMG_ST_F64) bot_copy<DIM, double> (gg, (double *) gp, gs, (double *) sp, to_shared);
+  else bot_copy<DIM, float> (gg, (float *) gp, gs, (float *) sp, to_shared);
+}
+
+template <typename T>
+__device__ __forceinline__ T ld (const void * p, long long i) { return ((const T *) p)[i]; }
+
+template <int DIM, typename TF, typename TC>
+__device__ __forceinline__ void bot_restrict (const bmg_geom & gf, const void * f, const bmg_geom & gc, void * c)
+{
+  const int n = gc.n;
+  const long long total = DIM == 1 ? n : DIM == 2 ? (long long) n*n : (long long) n*n*n;
+  for (long long q = threadIdx.x; q < total; q += blockDim.x) {
+    int i, j = 0, k = 0;
+    const int ln = 31 - __clz (n), qq = (int) q;
+    if (DIM == 1) i = qq;
+    else if (DIM == 2) { i = qq >> ln; j = qq & (n - 1); }
+    else { i = qq >> (2*ln); j = (qq >> ln) & (n - 1); k = qq & (n - 1); }
+    TC sum = TC(0);
+    if (DIM == 1) {
+      for (int a = 0; a < 2; a++) sum += (TC) ld<TF> (f, cidx<1> (gf, 2*i + a, 0, 0));
+    }
+    else if (DIM == 2) {
+      for (int a = 0; a < 2; a++)
+        for (int b = 0; b < 2; b++)
+          sum += (TC) ld<TF> (f, cidx<2> (gf, 2*i + a, 2*j + b, 0));
+    }
+    else {
+      for (int a = 0; a < 2; a++)
+        for (int b = 0; b < 2; b++)
+          for (int d = 0; d < 2; d++)
+            sum += (TC) ld<TF> (f, cidx<3> (gf, 2*i + a, 2*j + b, 2*k + d));
+    }
+    ((TC *) c)[cidx<DIM> (gc, i, j, k)] = sum/TC(1 << DIM);
+  }
+}
+
+template <int DIM, typename TC, typename TF>
+__device__ __forceinline__ void bot_prolong (const bmg_geom & gc, const void * cv, const bmg_geom & gf, void * fv,
+                             const BCH & bc, int zero)
+{
+  const TC * s = (const TC *) cv;
+  TF * f = (TF *) fv;
+  const int n = gf.n;
+  const long long total = DIM == 1 ? n : DIM == 2 ? (long long) n*n : (long long) n*n*n;
+  for (long long q = threadIdx.x; q < total; q += blockDim.x) {
+    int i, j = 0, k = 0;
+    const int ln = 31 - __clz (n), qq = (int) q;
+    if (DIM == 1) i = qq;
+    else if (DIM == 2) { i = qq >> ln; j = qq & (n - 1); }
+    else { i = qq >> (2*ln); j = (qq >> ln) & (n - 1); k = qq & (n - 1); }
+    TC v = TC(0);
+    if (!zero) {
+      const int pi = i >> 1, cx = (i & 1) ? 1 : -1;
+      if (DIM == 1)
+        v = (TC(3)*s[cidx<1> (gc, pi, 0, 0)] + s[cidx<1> (gc, pi + cx, 0, 0)])/TC(4);
+      else if (DIM == 2) {
+        const int pj = j >> 1, cy = (j & 1) ? 1 : -1;
+        v = (TC(9)*s[cidx<2> (gc, pi, pj, 0)] +
+             TC(3)*(s[cidx<2> (gc, pi + cx, pj, 0)] + s[cidx<2> (gc, pi, pj + cy, 0)]) +
+             s[cidx<2> (gc, pi + cx, pj + cy, 0)])/TC(16);
+      }
+      else {
+        const int pj = j >> 1, cy = (j & 1) ? 1 : -1;
+        const int pk = k >> 1, cz = (k & 1) ? 1 : -1;
+        v = (TC(27)*s[cidx<3> (gc, pi, pj, pk)] +
+             TC(9)*(s[cidx<3> (gc, pi + cx, pj, pk)] + s[cidx<3> (gc, pi, pj + cy, pk)] +
+                    s[cidx<3> (gc, pi, pj, pk + cz)]) +
+             TC(3)*(s[cidx<3> (gc, pi + cx, pj + cy, pk)] + s[cidx<3> (gc, pi + cx, pj, pk + cz)] +
+                    s[cidx<3> (gc, pi, pj + cy, pk + cz)]) +
+             s[cidx<3> (gc, pi + cx, pj + cy, pk + cz)])/TC(64);
+      }
+    }
+    const TF w = (TF) v;
+    f[cidx<DIM> (gf, i, j, k)] = w;
+    ghosts_homog<DIM, TF> (f, gf, i, j, k, w, bc);
+  }
+}
+
+/* ghost images of a 2D cell (homogeneous BCs) without local arrays: the
+   edge images and the corner image, composed as in ghosts_homog */
+template <typename T>
+__device__ __forceinline__ void ghosts_homog_2d (T * f, const bmg_geom & g, int i, int j, T v,
+                                                 const BCH & bc)
+{
+  const int n = g.n;
+  if (i != 0 && i != n - 1 && j != 0 && j != n - 1) return;
+  if (n == 1) { ghosts_homog<2, T> (f, g, i, j, 0, v, bc); return; }
+  int gi = i, gj = j;
+  T fi = T(1), fj = T(1);
+  if (i == 0) { gi = bc.periodic[0] ? n : -1; fi = bc.periodic[0] ? T(1) : T(bc.fac[1]); }
+  else if (i == n - 1) { gi = bc.periodic[0] ? -1 : n; fi = bc.periodic[0] ? T(1) : T(bc.fac[0]); }
+  if (j == 0) { gj = bc.periodic[1] ? n : -1; fj = bc.periodic[1] ? T(1) : T(bc.fac[3]); }
+  else if (j == n - 1) { gj = bc.periodic[1] ? -1 : n; fj = bc.periodic[1] ? T(1) : T(bc.fac[2]); }
+  if (gi != i) f[cidx<2> (g, gi, j, 0)] = v*fi;
+  if (gj != j) f[cidx<2> (g, i, gj, 0)] = v*fj;
+  if (gi != i && gj != j) f[cidx<2> (g, gi, gj, 0)] = v*fi*fj;
+}
+
+/* one colour pass of red-black relaxation over a whole staged level, by
+   threads [t0, t0 + nt) of the block */
+template <int DIM, typename T>
+__device__ __forceinline__ void bot_pass (const bmg_geom & g, void * dav, const void * resv, const void * const * al,
+                          const BotLevel & L, const void * lamp, const BCH & bc, int color,
+                          int t0, int nt)
+{
+  T * a = (T *) dav;
+  const T * b = (const T *) resv;
+  Coef<T> ax, ay, az, lam;
+  ax.p = (const T *) al[0]; ax.c = (T) L.alpha[0].c;
+  ay.p = (const T *) al[1]; ay.c = (T) L.alpha[1].c;
+  az.p = (const T *) al[2]; az.c = (T) L.alpha[2].c;
+  lam.p = (const T *) lamp; lam.c = (T) L.lambda.c;
+  const T D2 = (T) L.Delta*(T) L.Delta;
+  const int n = g.n;
+  /* cells of one colour: the contiguous index runs over half the row
+     (n is a power of two: shifts, no divisions) */
+  const int ln = 31 - __clz (n), nh = n > 1 ? n >> 1 : 1, lh = n > 1 ? ln - 1 : 0;
+  const int rows = DIM == 1 ? 1 : DIM == 2 ? n : n*n;
+  const int total = rows*nh;
+  for (int q = threadIdx.x - t0; q < total; q += nt) {
+    const int row = q >> lh, h = q & (nh - 1);
+    int i, j, k;
+    if (DIM == 1) { i = 2*h + color; j = k = 0; if (i >= n) continue; }
+    else if (DIM == 2) { i = row; j = 2*h + ((color + i) & 1); k = 0; if (j >= n) continue; }
+    else { i = row >> ln; j = row & (n - 1); k = 2*h + ((color + i + j) & 1); if (k >= n) continue; }
+    const long long id = cidx<DIM> (g, i, j, k);
+    const T v = relax_value<DIM, T> (g, id, a, b, ax, ay, az, lam, D2);
+    a[id] = v;
+    if (DIM == 2) ghosts_homog_2d<T> (a, g, i, j, v, bc);
+    else ghosts_homog<DIM, T> (a, g, i, j, k, v, bc);
+  }
+}
+
+/* the 2D pass of the bottom solve with instruction-level parallelism: each
+   thread first gathers the operands of up to K cells (independent loads,
+   no stores in between), then divides and stores */
+template <typename T, bool AST, bool LST, int K>
+__device__ __forceinline__ void bot_pass2d (const bmg_geom & g, T * a, const T * b, const T * ax, const T * ay,
+                            T axc, T ayc, const T * lam, T lamc, T D2, const BCH & bc,
+                            int color, int nt)
+{
+  const int n = g.n, P = g.P;
+  if (n == 1) {   /* level 0: the generic path handles its single cell */
+    if (threadIdx.x == 0 && color == 0) {
+      Coef<T> cx, cy, cz, cl;
+      cx.p = AST ? ax : NULL; cx.c = axc; cy.p = AST ? ay : NULL; cy.c = ayc;
+      cz.p = NULL; cz.c = T(0); cl.p = LST ? lam : NULL; cl.c = lamc;
+      const long long id = cidx<2> (g, 0, 0, 0);
+      const T v = relax_value<2, T> (g, id, a, b, cx, cy, cz, cl, D2);
+      a[id] = v;
+      ghosts_homog<2, T> (a, g, 0, 0, 0, v, bc);
+    }
+    return;
+  }
+  const int ln = 31 - __clz (n), lh = ln - 1, nh = n >> 1;
+  const int total = n*nh;
+  for (int q0 = threadIdx.x; q0 < total; q0 += nt*K) {
+    T nn[K], dd[K];
+    int ids[K], is[K], js[K];
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+      const int q = q0 + k*nt;
+      const int i = q >> lh, j = 2*(q & (nh - 1)) + ((color + i) & 1);
+      is[k] = i; js[k] = j;
+      const int id = (i + 1)*P + 1 + j;
+      ids[k] = q < total ? id : -1;
+      if (q < total) {
+        const T ax0 = AST ? ax[id] : axc, ax1 = AST ? ax[id + P] : axc;
+        const T ay0 = AST ? ay[id] : ayc, ay1 = AST ? ay[id + 1] : ayc;
+        T m = (-D2)*b[id], d = (-(LST ? lam[id] : lamc))*D2;
+        m += ax1*a[id + P] + ax0*a[id - P];
+        d += ax1 + ax0;
+        m += ay1*a[id + 1] + ay0*a[id - 1];
+        d += ay1 + ay0;
+        nn[k] = m; dd[k] = d;
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < K; k++)
+      if (ids[k] >= 0) {
+        const T v = nn[k]/dd[k];
+        a[ids[k]] = v;
+        ghosts_homog_2d<T> (a, g, is[k], js[k], v, bc);
+      }
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ void bot_pass2d_any (const bmg_geom & g, void * dav, const void * resv,
+                                const void * const * al, const BotLevel & L, const void * lamp,
+                                const BCH & bc, int color, int nt)
+{
+  T * a = (T *) dav;
+  const T * b = (const T *) resv;
+  const T * ax = (const T *) al[0], * ay = (const T *) al[1], * lam = (const T *) lamp;
+  const T axc = (T) L.alpha[0].c, ayc = (T) L.alpha[1].c, lamc = (T) L.lambda.c;
+  const T D2 = (T) L.Delta*(T) L.Delta;
+  if ((ax == NULL) != (ay == NULL))   /* one component stored, one constant */
+    bot_pass<2, T> (g, dav, resv, al, L, lamp, bc, color, 0, nt);
+  else if (ax && lam) bot_pass2d<T, true, true, 1> (g, a, b, ax, ay, axc, ayc, lam, lamc, D2, bc, color, nt);
+  else if (ax) bot_pass2d<T, true, false, 1> (g, a, b, ax, ay, axc, ayc, lam, lamc, D2, bc, color, nt);
+  else if (lam) bot_pass2d<T, false, true, 1> (g, a, b, ax, ay, axc, ayc, lam, lamc, D2, bc, color, nt);
+  else bot_pass2d<T, false, false, 1> (g, a, b, ax, ay, axc, ayc, lam, lamc, D2, bc, color, nt);
+}
+
+template <int DIM>
+__device__ __forceinline__ void bot_restrict_st (int stf, const bmg_geom & gf, const void * f, int stc,
+                                 const bmg_geom & gc, void * c)
+{
+  if (stf == BMG_ST_F64 && stc == BMG_ST_F64) bot_restrict<DIM, double, double> (gf, f, gc, c);
+  else if (stf == BMG_ST_F32 && stc == BMG_ST_F32) bot_restrict<DIM, float, float> (gf, f, gc, c);
+  else if (stf == BMG_ST_F32 && stc == BMG_ST_F64) bot_restrict<DIM, float, double> (gf, f, gc, c);
+  else bot_restrict<DIM, double, float> (gf, f, gc, c);
+}
+
+template <int DIM>
+__device__ __forceinline__ void bot_prolong_st (int stc, const bmg_geom & gc, const void * c, int stf,
+                                const bmg_geom & gf, void * f, const BCH & bc, int zero)
+{
+  if (stc == BMG_ST_F64 && stf == BMG_ST_F64) bot_prolong<DIM, double, double> (gc, c, gf, f, bc, zero);
+  else if (stc == BMG_ST_F32 && stf == BMG_ST_F32) bot_prolong<DIM, float, float> (gc, c, gf, f, bc, zero);
+  else if (stc == BMG_ST_F64 && stf == BMG_ST_F32) bot_prolong<DIM, double, float> (gc, c, gf, f, bc, zero);
+  else bot_prolong<DIM, float, double> (gc, c, gf, f, bc, zero);
+}
+
+template <int DIM>
+__global__ void __launch_bounds__ (1024, 1) k_bottom (const __grid_constant__ BotParams P)
+{
+  extern __shared__ __align__ (16) unsigned char bsm[];
+  /* stage the coefficients of every level */
+  for (int m = 0; m < P.nlev; m++) {
+    const BotLevel & L = P.lv[m];
+    const BotStage & S = P.sm[m];
+    for (int d = 0; d < DIM; d++)
+      if (S.off_alpha[d] != ~0u)
+        bot_copy_st<DIM> (L.st, L.g, L.alpha[d].p, S.gs, sm_at (bsm, S.off_alpha[d]), 1);
+    if (S.off_lambda != ~0u)
+      bot_copy_st<DIM> (L.st, L.g, L.lambda.p, S.gs, sm_at (bsm, S.off_lambda), 1);
+  }
+  /* res of the top staged level: restricted from level hi+1, or as given */
+  const int top = P.nlev - 1;
+  if (P.restrict_src)
+    bot_restrict_st<DIM> (P.st_src, P.g_src, P.res_src, P.lv[top].st, P.sm[top].gs,
+                          sm_at (bsm, P.sm[top].off_res));
+  else
+    bot_copy_st<DIM> (P.lv[top].st, P.lv[top].g, P.lv[top].res, P.sm[top].gs,
+                      sm_at (bsm, P.sm[top].off_res), 1);
+  __syncthreads ();
+  /* restriction down to the coarsest level (multigrid-common.h:368-404) */
+  for (int m = top - 1; m >= 0; m--) {
+    bot_restrict_st<DIM> (P.lv[m + 1].st, P.sm[m + 1].gs, sm_at (bsm, P.sm[m + 1].off_res),
+                          P.lv[m].st, P.sm[m].gs, sm_at (bsm, P.sm[m].off_res));
+    __syncthreads ();
+  }
+  /* coarse to fine: zero / bilinear, then nrelax red-black sweeps */
+  for (int m = 0; m < P.nlev; m++) {
+    const BotLevel & L = P.lv[m];
+    const BotStage & S = P.sm[m];
+    void * da = sm_at (bsm, S.off_da);
+    if (m == 0)
+      bot_prolong_st<DIM> (L.st, S.gs, NULL, L.st, S.gs, da, P.bc, 1);
+    else
+      bot_prolong_st<DIM> (P.lv[m - 1].st, P.sm[m - 1].gs, sm_at (bsm, P.sm[m - 1].off_da),
+                           L.st, S.gs, da, P.bc, 0);
+    __syncthreads ();
+    const void * al[3];
+    for (int d = 0; d < 3; d++) al[d] = d < DIM ? sm_at (bsm, S.off_alpha[d]) : NULL;
+    const void * res = sm_at (bsm, S.off_res);
+    const void * lam = sm_at (bsm, S.off_lambda);
+    /* levels of at most BOT_WARP_CELLS cells are relaxed by warp 0 alone,
+       with warp barriers; the other warps wait at the level's end */
+    const bool small = S.gs.size <= BOT_WARP_CELLS;
+    if (!small || threadIdx.x < 32)
+      for (int sw = 0; sw < P.nrelax; sw++)
+        for (int color = 0; color < 2; color++) {
+          const int nt = small ? 32 : blockDim.x;
+          if (DIM == 2) {
+            /* x and y coefficients are both stored or both constant */
+            if (L.st == BMG_ST_F64) bot_pass2d_any<double> (S.gs, da, res, al, L, lam, P.bc, color, nt);
+            else bot_pass2d_any<float> (S.gs, da, res, al, L, lam, P.bc, color, nt);
+          }
+          else if (L.st == BMG_ST_F64)
+            bot_pass<DIM, double> (S.gs, da, res, al, L, lam, P.bc, color, 0, nt);
+          else
+            bot_pass<DIM, float> (S.gs, da, res, al, L, lam, P.bc, color, 0, nt);
+          if (small) __syncwarp ();
+          else __syncthreads ();
+        }
+    if (small) __syncthreads ();
+  }
+  /* da of every staged level, ghosts included, back to global memory (the
+     next level's prolongation reads it) */
+  for (int m = 0; m < P.nlev; m++)
+    bot_copy_st<DIM> (P.lv[m].st, P.lv[m].g, P.lv[m].da, P.sm[m].gs, sm_at (bsm, P.sm[m].off_da), 0);
+}
+
+template <typename T, int TS, int S, bool LAM, int BX, int BY>
+int launch_tile_v (bmg_geom g, void * out, const void * in, const void * res,
+                   const bmg_coef * alpha, bmg_coef lambda, double Delta, BCH h, int nsweeps,
+                   cudaStream_t s)
+{
+  typedef TileShape<T, TS, S> Sh;
+  const size_t bytes = Sh::bytes (LAM);
+  /* the shared-memory opt-in, once per device */
+  static unsigned char configured[64];
+  int dev = 0;
+  cudaGetDevice (&dev);
+  if (dev < 0 || dev >= 64) return (int) cudaErrorInvalidDevice;
+  if (!configured[dev]) {
+    cudaError_t e = cudaFuncSetAttribute (k_relax_tile2d<T, TS, S, LAM, BX, BY>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int) bytes);
+    if (e != cudaSuccess) return (int) e;
+    configured[dev] = 1;
+  }
+  dim3 grid ((g.n + TS - 1)/TS, (g.n + TS - 1)/TS, 1);
+  k_relax_tile2d<T, TS, S, LAM, BX, BY><<<grid, dim3 (BX, BY, 1), bytes, s>>>
+    (g, (T *) out, (const T *) in, (const T *) res, coef_of<T> (alpha[0]), coef_of<T> (alpha[1]),
+     coef_of<T> (lambda), (T) Delta, h, nsweeps);
+  return 0;
+}
+
+template <typename T, int TS, int S, int BX, int BY>
+int launch_tile (bmg_geom g, void * out, const void * in, const void * res,
+                 const bmg_coef * alpha, bmg_coef lambda, double Delta, BCH h, int nsweeps,
+                 cudaStream_t s)
+{
+  if (lambda.p)
+    return launch_tile_v<T, TS, S, true, BX, BY> (g, out, in, res, alpha, lambda, Delta, h, nsweeps, s);
+  return launch_tile_v<T, TS, S, false, BX, BY> (g, out, in, res, alpha, lambda, Delta, h, nsweeps, s);
+}
+
+} // namespace
+
+extern "C" {
+
+int bmg_tile_sweeps (int st)
+{
+  return st == BMG_ST_F64 ? 4 : 4;
+}
+
+int bmg_launch_relax_tile (int dim, int st, bmg_geom g, void * out, const void * in,
+                           const void * res, const bmg_coef * alpha, bmg_coef lambda,
+                           double Delta, const bmg_bcdesc * bc, int nsweeps, cudaStream_t s)
+{
+  if (dim != 2 || nsweeps < 1 || nsweeps > bmg_tile_sweeps (st)) return (int) cudaErrorInvalidValue;
+  BCH h = bch_of (bc);
+  int e;
+  /* small levels: 16 x 16 tiles (more CTAs, a shorter critical path per
+     CTA); large levels: big tiles (less halo recomputation) */
+  const bool small = g.n <= BMG_SMALL_TILE_N;
+  if (st == BMG_ST_F64)
+    e = small ? launch_tile<double, 16, 4, 8, 32> (g, out, in, res, alpha, lambda, Delta, h, nsweeps, s)
+      : launch_tile<double, 40, 4, 16, 64> (g, out, in, res, alpha, lambda, Delta, h, nsweeps, s);
+  else
+    e = small ? launch_tile<float, 16, 4, 8, 32> (g, out, in, res, alpha, lambda, Delta, h, nsweeps, s)
+      : launch_tile<float, 48, 4, 16, 64> (g, out, in, res, alpha, lambda, Delta, h, nsweeps, s);
+  if (e) return e;
+  cudaError_t r = cudaGetLastError ();
+  return r == cudaSuccess ? 0 : (int) r;
+}
+
+size_t bmg_bottom_smem (int dim, const bmg_bottom_level * lv, int nlev)
+{
+  size_t off = 0;
+  for (int m = 0; m < nlev; m++) {
+    size_t cells = 1;
+    for (int d = 0; d < dim; d++) cells *= (size_t) lv[m].g.n + 2;
+    const size_t arr = (cells*(lv[m].st == BMG_ST_F64 ? 8 : 4) + 15)/16*16;
+    int narr = 2 + (lv[m].lambda.p ? 1 : 0);
+    for (int d = 0; d < dim; d++) narr += lv[m].alpha[d].p ? 1 : 0;
+    off += narr*arr;
+  }
+  return off;
+}
+
+int bmg_launch_bottom (int dim, const bmg_bottom_level * lv, int nlev, bmg_geom g_src,
+                       const void * res_src, int st_src, int restrict_src, int nrelax,
+                       const bmg_bcdesc * bc, cudaStream_t s)
+{
+  if (nlev < 1 || nlev > BOT_MAXLEVELS) return (int) cudaErrorInvalidValue;
+  const size_t bytes = bmg_bottom_smem (dim, lv, nlev);
+  if (bytes > BMG_BOTTOM_SMEM) return (int) cudaErrorInvalidValue;
+  BotParams P;
+  memset (&P, 0, sizeof P);
+  size_t off = 0;
+  for (int m = 0; m < nlev; m++) {
+    P.lv[m] = lv[m];
+    BotStage & S = P.sm[m];
+    const int n = lv[m].g.n;
+    S.gs.n = n; S.gs.P = n + 2; S.gs.xo = 1;
+    S.gs.plane = dim == 3 ? (long long) (n + 2)*(n + 2) : dim == 2 ? n + 2 : 1;
+    size_t cells = 1;
+    for (int d = 0; d < dim; d++) cells *= (size_t) n + 2;
+    S.gs.size = (long long) cells;
+    const size_t arr = (cells*(lv[m].st == BMG_ST_F64 ? 8 : 4) + 15)/16*16;
+    S.off_da = (unsigned) off; off += arr;
+    S.off_res = (unsigned) off; off += arr;
+    for (int d = 0; d < 3; d++)
+      if (d < dim && lv[m].alpha[d].p) { S.off_alpha[d] = (unsigned) off; off += arr; }
+      else S.off_alpha[d] = ~0u;
+    if (lv[m].lambda.p) { S.off_lambda = (unsigned) off; off += arr; }
+    else S.off_lambda = ~0u;
+  }
+  P.g_src = g_src; P.res_src = res_src; P.st_src = st_src;
+  P.nlev = nlev; P.nrelax = nrelax; P.restrict_src = restrict_src;
+  P.bc = bch_of (bc);
+  static unsigned char configured[64][3];
+  int dev = 0;
+  cudaGetDevice (&dev);
+  if (dev < 0 || dev >= 64) return (int) cudaErrorInvalidDevice;
+  if (!configured[dev][dim - 1]) {
+    cudaError_t e = dim == 1 ? cudaFuncSetAttribute (k_bottom<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, BMG_BOTTOM_SMEM)
+      : dim == 2 ? cudaFuncSetAttribute (k_bottom<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, BMG_BOTTOM_SMEM)
+      : cudaFuncSetAttribute (k_bottom<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, BMG_BOTTOM_SMEM);
+    if (e != cudaSuccess) return (int) e;
+    configured[dev][dim - 1] = 1;
+  }
+  if (dim == 1) k_bottom<1><<<1, 1024, bytes, s>>> (P);
+  else if (dim == 2) k_bottom<2><<<1, 1024, bytes, s>>> (P);
+  else k_bottom<3><<<1, 1024, bytes, s>>> (P);
+  cudaError_t r = cudaGetLastError ();
+  return r == cudaSuccess ? 0 : (int) r;
+}
+
+} // extern "C"

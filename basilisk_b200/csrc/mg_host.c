@@ -27,6 +27,9 @@ static bmg_grid * current_grid = NULL;
 
 #define XO64 4
 #define XO32 8
+/* levels with at most this many cells are solved by the single-CTA bottom
+   kernel on the red-black path */
+#define BMG_BOTTOM_CELLS 4096
 
 typedef struct {
   int used;
@@ -96,7 +99,8 @@ static int fail (int s) { last_error = s; return s; }
 /* captured V-cycles: the launch sequence of one mg_solve iteration is a
    pure function of its parameters (cycle_key), so each distinct key is
    captured once into a CUDA graph and replayed afterwards */
-#define NGRAPH 16
+#define NGRAPH_MAX 256
+#define NGRAPH_DEFAULT 64
 typedef struct { double bytes; long long launches, sweeps; double relax_bytes; long long relax_sweeps; } work_t;
 struct graph_entry {
   int valid;
@@ -110,7 +114,7 @@ struct graph_entry {
 static void graphs_clear (struct bmg_grid * g)
 {
   if (!g->graphs) return;
-  for (int i = 0; i < NGRAPH; i++)
+  for (int i = 0; i < NGRAPH_MAX; i++)
     if (g->graphs[i].valid) {
       cudaGraphExecDestroy (g->graphs[i].exec);
       free (g->graphs[i].key);
@@ -190,7 +194,7 @@ int bmg_grid_new (bmg_grid ** out, int dim, int depth)
   bmg_grid * g = calloc (1, sizeof (bmg_grid));
   if (!g) return fail (BMG_ENOMEM);
   g->dim = dim; g->depth = depth; g->L0 = 1.;
-  g->relax = BMG_RELAX_RBGS; g->precision = BMG_FP64; g->use_graphs = 1;
+  g->relax = BMG_RELAX_RBGS; g->precision = BMG_FP64; g->use_graphs = NGRAPH_DEFAULT;
   CK (cudaGetDevice (&g->device));
   CK (cudaStreamCreateWithFlags (&g->stream, cudaStreamNonBlocking));
   g->own_stream = 1;
@@ -207,7 +211,7 @@ int bmg_grid_new (bmg_grid ** out, int dim, int depth)
   CK (cudaEventCreate (&g->ev1));
   CK (cudaEventCreate (&g->evr0));
   CK (cudaEventCreate (&g->evr1));
-  g->graphs = calloc (NGRAPH, sizeof (struct graph_entry));
+  g->graphs = calloc (NGRAPH_MAX, sizeof (struct graph_entry));
   *out = g;
   current_grid = g;
   return fail (BMG_OK);
@@ -318,7 +322,13 @@ int bmg_synchronize (bmg_grid * g)
   return BMG_OK;
 }
 
-int bmg_set_graphs (bmg_grid * g, int on) { if (!g) return fail (BMG_EINVAL); g->use_graphs = on; return BMG_OK; }
+int bmg_set_graphs (bmg_grid * g, int n)
+{
+  if (!g || n < 0) return fail (BMG_EINVAL);
+  graphs_clear (g);
+  g->use_graphs = n == 1 ? NGRAPH_DEFAULT : n > NGRAPH_MAX ? NGRAPH_MAX : n;
+  return BMG_OK;
+}
 int bmg_set_timing (bmg_grid * g, int on) { if (!g) return fail (BMG_EINVAL); g->timing = on; return BMG_OK; }
 
 int bmg_get_counters (bmg_grid * g, bmg_counters * c)
@@ -709,6 +719,31 @@ static int residual_max (bmg_grid * g, field_t * a, const double * b, const coef
   return BMG_OK;
 }
 
+/* the levels of the single-CTA bottom solve: minlevel up to the largest
+   level with at most BMG_BOTTOM_CELLS cells whose staged arrays fit the
+   bottom kernel's shared memory; fills bl[0..top-minlevel] */
+static int bottom_top (const bmg_grid * g, const levels_t * lv, const coefs_t * c,
+                       int minlevel, int maxlevel, bmg_bottom_level * bl)
+{
+  int top = minlevel - 1;
+  for (int l = minlevel; l <= maxlevel; l++) {
+    if (l > minlevel && ncells (g, l) > BMG_BOTTOM_CELLS) break;
+    bmg_bottom_level * b = &bl[l - minlevel];
+    memset (b, 0, sizeof *b);
+    b->st = lv->st[l];
+    b->g = geom_st (g, l, b->st);
+    b->da = lv->da[l];
+    b->res = lv->res[l];
+    for (int d = 0; d < 3; d++)
+      b->alpha[d] = b->st == BMG_ST_F64 ? c->alpha64[l][d] : c->alpha32[l][d];
+    b->lambda = b->st == BMG_ST_F64 ? c->lambda64[l] : c->lambda32[l];
+    b->Delta = delta_of (g, l);
+    if (l > minlevel && bmg_bottom_smem (g->dim, bl, l - minlevel + 1) > BMG_BOTTOM_SMEM) break;
+    top = l;
+  }
+  return top < minlevel ? minlevel : top;
+}
+
 /* the launches of one mg_cycle (poisson.h:32-90).  Each level's final
    iterate of da is returned in fin[] (the Jacobi sweeps alternate between
    the da and da2 buffers). */
@@ -720,8 +755,14 @@ static int cycle_launches (bmg_grid * g, field_t * a, const levels_t * lv, const
   cudaStream_t s = g->stream;
   double bytes = 0.;
   long long launches = 0, sweeps = 0;
-  /* restriction (res) down to minlevel (multigrid-common.h:368-404) */
-  for (int l = L - 1; l >= minlevel; l--) {
+  /* restriction (res) down to minlevel (multigrid-common.h:368-404); on the
+     red-black path the levels of the bottom solve are restricted inside it */
+  int rlow = minlevel;
+  if (g->relax == BMG_RELAX_RBGS) {
+    bmg_bottom_level bl[BMG_MAXLEVEL + 1];
+    rlow = bottom_top (g, lv, c, minlevel, maxlevel, bl) + 1;
+  }
+  for (int l = L - 1; l >= rlow; l--) {
     CL (bmg_launch_restrict (dim, lv->st[l + 1], lv->st[l], geom_st (g, l + 1, lv->st[l + 1]),
                              geom_st (g, l, lv->st[l]), lv->res[l + 1], lv->res[l], s));
     bytes += ncells (g, l + 1)*es_of (lv->st[l + 1]) + ncells (g, l)*es_of (lv->st[l]);
@@ -729,7 +770,31 @@ static int cycle_launches (bmg_grid * g, field_t * a, const levels_t * lv, const
   }
   void * cur[BMG_MAXLEVEL + 1], * oth[BMG_MAXLEVEL + 1];
   const double narr = relax_arrays (g, c);
-  for (int l = minlevel; l <= maxlevel; l++) {
+  int first = minlevel;
+  if (g->relax == BMG_RELAX_RBGS) {
+    /* the coarse end in one single-CTA launch: levels minlevel..top */
+    bmg_bottom_level bl[BMG_MAXLEVEL + 1];
+    const int top = bottom_top (g, lv, c, minlevel, maxlevel, bl);
+    for (int l = minlevel; l <= top; l++) {
+      const int st = lv->st[l];
+      cur[l] = lv->da[l]; oth[l] = lv->da2[l];
+      if (l < L)   /* restriction of res into this level */
+        bytes += ncells (g, l + 1)*es_of (lv->st[l + 1]) + ncells (g, l)*es_of (st);
+      bytes += ncells (g, l)*es_of (st);            /* zero or prolongation */
+      if (l > minlevel)
+        bytes += ncells (g, l - 1)*es_of (lv->st[l - 1]);
+      bytes += nrelax*narr*ncells (g, l)*es_of (st);
+      sweeps += nrelax;
+    }
+    const int src = top < L;
+    CL (bmg_launch_bottom (dim, bl, top - minlevel + 1,
+                           src ? geom_st (g, top + 1, lv->st[top + 1]) : g->g64[L],
+                           src ? lv->res[top + 1] : NULL, src ? lv->st[top + 1] : 0, src,
+                           nrelax, dabc, s));
+    launches++;
+    first = top + 1;
+  }
+  for (int l = first; l <= maxlevel; l++) {
     const int st = lv->st[l];
     const bmg_geom gl = geom_st (g, l, st);
     cur[l] = lv->da[l]; oth[l] = lv->da2[l];
@@ -749,23 +814,36 @@ static int cycle_launches (bmg_grid * g, field_t * a, const levels_t * lv, const
     const bmg_coef la = st == BMG_ST_F64 ? c->lambda64[l] : c->lambda32[l];
     const int timed = g->timing && l == L && maxlevel == L;
     if (timed) CK (cudaEventRecordWithFlags (g->evr0, s, cudaEventRecordExternal));
-    for (int i = 0; i < nrelax; i++) {
-      if (g->relax == BMG_RELAX_JACOBI) {
-        CL (bmg_launch_relax (dim, st, BMG_SWEEP_JACOBI, gl, oth[l], cur[l], lv->res[l], al, la,
-                              delta_of (g, l), dabc, s));
+    if (g->relax == BMG_RELAX_RBGS && dim == 2) {
+      /* several complete red-black sweeps per launch, ping-pong buffers */
+      const int S = bmg_tile_sweeps (st);
+      for (int done = 0; done < nrelax; ) {
+        const int k = nrelax - done < S ? nrelax - done : S;
+        CL (bmg_launch_relax_tile (dim, st, gl, oth[l], cur[l], lv->res[l], al, la,
+                                   delta_of (g, l), dabc, k, s));
         void * t = cur[l]; cur[l] = oth[l]; oth[l] = t;
         launches++;
+        done += k;
       }
-      else {
-        CL (bmg_launch_relax (dim, st, BMG_SWEEP_RED, gl, cur[l], cur[l], lv->res[l], al, la,
-                              delta_of (g, l), dabc, s));
-        CL (bmg_launch_relax (dim, st, BMG_SWEEP_BLACK, gl, cur[l], cur[l], lv->res[l], al, la,
-                              delta_of (g, l), dabc, s));
-        launches += 2;
-      }
-      bytes += narr*ncells (g, l)*es_of (st);
-      sweeps++;
     }
+    else
+      for (int i = 0; i < nrelax; i++) {
+        if (g->relax == BMG_RELAX_JACOBI) {
+          CL (bmg_launch_relax (dim, st, BMG_SWEEP_JACOBI, gl, oth[l], cur[l], lv->res[l], al, la,
+                                delta_of (g, l), dabc, s));
+          void * t = cur[l]; cur[l] = oth[l]; oth[l] = t;
+          launches++;
+        }
+        else {
+          CL (bmg_launch_relax (dim, st, BMG_SWEEP_RED, gl, cur[l], cur[l], lv->res[l], al, la,
+                                delta_of (g, l), dabc, s));
+          CL (bmg_launch_relax (dim, st, BMG_SWEEP_BLACK, gl, cur[l], cur[l], lv->res[l], al, la,
+                                delta_of (g, l), dabc, s));
+          launches += 2;
+        }
+      }
+    bytes += nrelax*narr*ncells (g, l)*es_of (st);
+    sweeps += nrelax;
     if (timed) {
       CK (cudaEventRecordWithFlags (g->evr1, s, cudaEventRecordExternal));
       w->relax_bytes += nrelax*narr*ncells (g, l)*es_of (st);
@@ -820,7 +898,7 @@ static int run_cycle (bmg_grid * g, field_t * a, const double * bdata, const lev
   void * fin[BMG_MAXLEVEL + 1];
   if (g->use_graphs) {
     struct graph_entry * e = NULL, * victim = &g->graphs[0];
-    for (int i = 0; i < NGRAPH; i++) {
+    for (int i = 0; i < g->use_graphs; i++) {
       struct graph_entry * q = &g->graphs[i];
       if (q->valid && q->keylen == sizeof key && !memcmp (q->key, &key, sizeof key)) { e = q; break; }
       if (!q->valid || q->stamp < victim->stamp) victim = q;

@@ -105,6 +105,35 @@ int bmg_launch_shift (int dim, bmg_geom g, double * f, const double * sum,
 
 int bmg_launch_face_wrap (int dim, bmg_geom g, int face_dim, double * f, cudaStream_t s);
 
+/* fused red-black relaxation (mg_fused.cu) */
+int bmg_tile_sweeps (int st);   /* sweeps one tile launch can do */
+int bmg_launch_relax_tile (int dim, int st, bmg_geom g, void * out, const void * in,
+                           const void * res, const bmg_coef * alpha, bmg_coef lambda,
+                           double Delta, const bmg_bcdesc * bc, int nsweeps, cudaStream_t s);
+
+/* one level of the single-CTA bottom solve */
+typedef struct {
+  bmg_geom g;
+  void * da;
+  void * res;
+  bmg_coef alpha[3];
+  bmg_coef lambda;
+  double Delta;
+  int st;
+  int pad_;
+} bmg_bottom_level;
+
+/* levels lv[0..nlev-1] (coarse to fine): restriction of res (from the level
+   above, g_src/res_src, when restrict_src), zero, prolongations and nrelax
+   red-black sweeps per level, in one launch of one CTA, with every level
+   staged in shared memory (at most BMG_BOTTOM_SMEM bytes, see
+   bmg_bottom_smem) */
+#define BMG_BOTTOM_SMEM (200*1024)
+size_t bmg_bottom_smem (int dim, const bmg_bottom_level * lv, int nlev);
+int bmg_launch_bottom (int dim, const bmg_bottom_level * lv, int nlev, bmg_geom g_src,
+                       const void * res_src, int st_src, int restrict_src, int nrelax,
+                       const bmg_bcdesc * bc, cudaStream_t s);
+
 /* number of partial sums bmg_launch_sum needs for a level */
 int bmg_sum_partials (int dim, bmg_geom g);
 

@@ -180,8 +180,10 @@ class Grid:
         p = {"fp64": _lib.FP64, "mixed": _lib.MIXED}.get(precision, precision)
         check(_lib.load().bmg_set_precision(self.ptr, p), "bmg_set_precision")
 
-    def set_graphs(self, on):
-        check(_lib.load().bmg_set_graphs(self.ptr, 1 if on else 0), "bmg_set_graphs")
+    def set_graphs(self, n):
+        """0/False: plain launches; 1/True: graphs with the default cache;
+        n > 1: a cache of n captured V-cycles."""
+        check(_lib.load().bmg_set_graphs(self.ptr, int(n)), "bmg_set_graphs")
 
     def set_timing(self, on):
         check(_lib.load().bmg_set_timing(self.ptr, 1 if on else 0), "bmg_set_timing")

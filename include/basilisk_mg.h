@@ -224,8 +224,9 @@ typedef struct {
 int bmg_get_counters (bmg_grid * grid, bmg_counters * c);
 int bmg_reset_counters (bmg_grid * grid);
 int bmg_set_timing (bmg_grid * grid, int on);
-/* use CUDA graphs for the V-cycles (default on) */
-int bmg_set_graphs (bmg_grid * grid, int on);
+/* CUDA graphs for the V-cycles: 0 = off, 1 = on with the default cache
+   (64 captured cycles, one per distinct nrelax), n > 1 = a cache of n (<= 256) */
+int bmg_set_graphs (bmg_grid * grid, int n);
 
 #ifdef __cplusplus
 }

@@ -68,6 +68,45 @@ def test_poisson_bit_exact(case, relax):
     assert_same(ost, gst, og.get_a(), a.get(), prob["b"])
 
 
+LARGE = [
+    # larger 2D levels: several shared-memory tiles per level, tile edges,
+    # lambda staged in shared memory, periodic halos wrapping across tiles
+    (2, 9, (), {s: ("dirichlet", 0.0) for s in range(4)}, "field", None),
+    (2, 9, (0, 1), {}, "field", -2.0),
+    (2, 8, (1,), {0: ("dirichlet", 1.0), 1: ("neumann", -0.5)}, "field", "field"),
+    (2, 10, (0,), {2: ("neumann", 0.0), 3: ("dirichlet", 0.0)}, 1.0, None),
+]
+
+
+@pytest.mark.parametrize("case", range(len(LARGE)))
+def test_rbgs_large_levels_bit_exact(case):
+    dim, depth, per, bc, al, lam = LARGE[case]
+    rng = np.random.default_rng(300 + case)
+    prob = random_problem(dim, depth, rng, periodic=per, bc=bc, alpha=al, lam=lam)
+    og, ost, g, a, gst = solve_both(prob, "rbgs", tolerance=1e-7)
+    assert_same(ost, gst, og.get_a(), a.get(), prob["b"])
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_two_phase_rbgs(precision):
+    """The two-phase recipe at 256^2 on the red-black path: bit-identical in
+    FP64; the mixed form within the tolerance-implied bound of the oracle."""
+    from basilisk_b200 import problems
+    prob = problems.two_phase_2d(depth=8, seed=12)
+    og = oracle_grid(prob, relax=oracle.RELAX_RBGS)
+    ost = og.poisson(tolerance=1e-6)
+    g, a, b, alpha, lam = gpu_grid(prob, relax="rbgs", precision=precision)
+    gst = g.poisson(a, b, alpha=alpha, lambda_=lam, tolerance=1e-6)
+    if precision == "fp64":
+        assert_same(ost, gst, og.get_a(), a.get(), prob["b"])
+    else:
+        assert gst["resa"] <= 1e-6
+        # FP32 smoothing changes the trajectory, not the convergence rate
+        assert gst["i"] <= 1.2*ost["i"]
+        ref = og.get_a()
+        assert np.abs(a.get() - ref).max() <= 1e-3 * np.abs(ref).max()
+
+
 @pytest.mark.parametrize("relax", ["jacobi", "rbgs"])
 def test_per_face_boundary_values(relax):
     """Dirichlet / Neumann data given per boundary face (a[left] =
