@@ -121,6 +121,7 @@ SIGNATURES = {
     "bmg_set_timing": (I, [P, I]),
     "bmg_set_graphs": (I, [P, I]),
     "bmg_sum_noalloc": (I, [P, SZ, P, P]),
+    "bmg_adjoint_gradients": (I, [P, bmg_scalar, bmg_scalar, ctypes.POINTER(P), P, I]),
 }
 GLOBALS = {"NITERMAX": ctypes.c_int, "NITERMIN": ctypes.c_int, "TOLERANCE": ctypes.c_double}
 

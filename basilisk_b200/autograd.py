@@ -1,0 +1,172 @@
+"""The differentiable Poisson--Helmholtz solve.
+
+``solve(problem, b, alpha, lam)`` returns ``a`` with ``L(alpha, lambda) a = b``
+(the operator whose residual is Basilisk's poisson.h:373-389) as a
+``torch.autograd.Function`` over the C-ABI of ``libbmg.so``: the forward is
+the GPU multigrid solve, and the hand-written backward is one more solve of
+the same (symmetric) operator for the adjoint ``mu`` from ``dl/da`` with the
+homogeneous boundary conditions, followed by the fused adjoint kernel of the
+library (``bmg_adjoint_gradients``):
+
+    dl/db      = mu
+    dl/dalpha  = grad(mu) . grad(a) on every face (boundary faces: the
+                 interior cell's term only)
+    dl/dlambda = -mu a
+
+The function keeps only the forward solution for the backward pass.
+``chain`` runs time-stepped sequences of solves with a checkpoint every k
+steps (the solutions inside a segment are recomputed in the backward pass).
+
+Tensors are CUDA float64, shape (n,)*dim or (B,)+(n,)*dim for a batch of
+independent instances; face component d has n+1 entries along d.
+"""
+import ctypes
+
+import torch
+
+from . import _lib
+from .grid import Grid
+
+
+class Problem:
+    """The fixed part of a family of solves: grid, boundary conditions of a
+    (``bc = {side: (kind, value)}``, sides in the reference's order right,
+    left, top, bottom, front, back), periodic directions, tolerance,
+    precision ("fp64" or "mixed") and smoother."""
+
+    def __init__(self, dim, depth, periodic=(), bc=None, tolerance=1e-10, precision="fp64",
+                 relax="rbgs", nrelax=4, L0=1.0, origin=(0.0, 0.0, 0.0), alpha=True,
+                 lam=False):
+        self.dim, self.depth, self.n = dim, depth, 1 << depth
+        self.tolerance, self.nrelax = tolerance, nrelax
+        self.periodic = tuple(periodic)
+        self.bc = dict(bc or {})
+        self.grid = Grid(dim, depth, L0=L0, origin=origin, relax=relax, precision=precision)
+        g = self.grid
+        for d in self.periodic:
+            g.periodic(2 * d)
+        self.a, self.b, self.mu, self.rhs = g.scalar(), g.scalar(), g.scalar(), g.scalar()
+        for side, (kind, val) in self.bc.items():
+            self.a.bc(side, kind, val)
+            self.mu.bc(side, kind, 0.0)          # the homogeneous twin
+        self.alpha = g.face_vector() if alpha else None
+        self.lam = g.scalar() if lam else None
+        self.stats = []
+
+    def close(self):
+        self.grid.close()
+
+    # -- one instance --------------------------------------------------
+    def _set_coefficients(self, alpha, lam):
+        if self.alpha is not None:
+            for c, v in zip(self.alpha.components, alpha):
+                c.set(v)
+        if self.lam is not None:
+            self.lam.set(lam)
+
+    def _solve(self, a, b, out):
+        a.set(torch.zeros_like(out))
+        st = self.grid.poisson(a, b, alpha=self.alpha, lambda_=self.lam,
+                               tolerance=self.tolerance, nrelax=self.nrelax)
+        self.stats.append(st)
+        a.get(out=out)
+        return st
+
+    def forward_one(self, b, alpha, lam, out):
+        self._set_coefficients(alpha, lam)
+        self.b.set(b)
+        return self._solve(self.a, self.b, out)
+
+    def backward_one(self, a_sol, grad_a, alpha, lam, grad_b, grad_alpha, grad_lam):
+        """mu from dl/da, then the coefficient gradients; grad_b receives mu."""
+        self._set_coefficients(alpha, lam)
+        self.rhs.set(grad_a)
+        self._solve(self.mu, self.rhs, grad_b)
+        # a with the ghosts of its boundary conditions, for the face kernel
+        self.a.set(a_sol)
+        L = _lib.load()
+        ptrs = (ctypes.c_void_p * 3)()
+        for d in range(3):
+            ptrs[d] = grad_alpha[d].data_ptr() if grad_alpha is not None and d < self.dim else None
+        torch.cuda.current_stream().synchronize()
+        _lib.check(L.bmg_adjoint_gradients(
+            self.grid.ptr, self.mu.scalar, self.a.scalar,
+            ptrs if grad_alpha is not None else None,
+            grad_lam.data_ptr() if grad_lam is not None else None, _lib.DEVICE),
+            "bmg_adjoint_gradients")
+
+
+class _Solve(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, problem, b, lam, *alpha):
+        batched = b.dim() == problem.dim + 1
+        bb = b if batched else b.unsqueeze(0)
+        out = torch.empty_like(bb)
+        for k in range(bb.shape[0]):
+            al = [x[k] if batched else x for x in alpha]
+            lm = None if lam is None else (lam[k] if batched else lam)
+            problem.forward_one(bb[k].contiguous(), al, lm, out[k])
+        a = out if batched else out[0]
+        ctx.problem, ctx.batched = problem, batched
+        ctx.has_lam, ctx.nalpha = lam is not None, len(alpha)
+        ctx.save_for_backward(a, *((lam,) if lam is not None else ()), *alpha)
+        return a
+
+    @staticmethod
+    def backward(ctx, grad_a):
+        problem, batched = ctx.problem, ctx.batched
+        saved = ctx.saved_tensors
+        a = saved[0]
+        lam = saved[1] if ctx.has_lam else None
+        alpha = saved[1 + ctx.has_lam:]
+        A = a if batched else a.unsqueeze(0)
+        G = (grad_a if batched else grad_a.unsqueeze(0)).contiguous()
+        grad_b = torch.empty_like(A)
+        grad_alpha = [torch.empty((A.shape[0],) + tuple(x.shape[-problem.dim:]),
+                                  dtype=torch.float64, device=A.device) for x in alpha]
+        grad_lam = torch.empty_like(A) if lam is not None else None
+        for k in range(A.shape[0]):
+            al = [x[k] if batched else x for x in alpha]
+            lm = None if lam is None else (lam[k] if batched else lam)
+            problem.backward_one(A[k].contiguous(), G[k], al, lm, grad_b[k],
+                                 [ga[k] for ga in grad_alpha] if alpha else None,
+                                 grad_lam[k] if lam is not None else None)
+        if not batched:
+            grad_b = grad_b[0]
+            grad_alpha = [x[0] for x in grad_alpha]
+            grad_lam = grad_lam[0] if grad_lam is not None else None
+        return (None, grad_b, grad_lam, *grad_alpha)
+
+
+def solve(problem, b, alpha=None, lam=None):
+    """a = L(alpha, lam)^{-1} b on ``problem``'s grid (differentiable in b,
+    alpha and lam).  alpha: a list of dim face tensors (None: alpha = 1);
+    lam: a cell tensor (None: lambda = 0)."""
+    if (alpha is None) != (problem.alpha is None):
+        raise ValueError("alpha must match the Problem (alpha=True/False)")
+    if (lam is None) != (problem.lam is None):
+        raise ValueError("lam must match the Problem (lam=True/False)")
+    alpha = tuple(alpha) if alpha is not None else ()
+    return _Solve.apply(problem, b, lam, *alpha)
+
+
+def chain(step, x, nsteps, every=1):
+    """x_{k+1} = step(x_k), nsteps times, with a checkpoint every ``every``
+    steps: only the segment boundaries are kept for the backward pass; the
+    solves inside a segment are run again when the gradient reaches it."""
+    from torch.utils.checkpoint import checkpoint
+
+    def segment(x, m):
+        for _ in range(m):
+            x = step(x)
+        return x
+
+    done = 0
+    while done < nsteps:
+        m = min(every, nsteps - done)
+        if every > 1 and x.requires_grad:
+            x = checkpoint(segment, x, m, use_reentrant=False)
+        else:
+            x = segment(x, m)
+        done += m
+    return x

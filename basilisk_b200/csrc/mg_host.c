@@ -1222,6 +1222,46 @@ void mg_cycle (bmg_scalar * al, bmg_scalar * resl, bmg_scalar * dal,
   fail (BMG_OK);
 }
 
+int bmg_adjoint_gradients (bmg_grid * g, bmg_scalar mu, bmg_scalar a, double * const * grad_alpha,
+                           double * grad_lambda, int memory)
+{
+  field_t * fm, * fa;
+  if (!g || check_cell (g, mu.i, &fm) || check_cell (g, a.i, &fa)) return fail (BMG_EINVAL);
+  if (memory != BMG_DEVICE && memory != BMG_HOST) return fail (BMG_EINVAL);
+  CK (cudaSetDevice (g->device));
+  const int L = g->depth;
+  for (int d = 0; d < g->dim; d++) {
+    if (!grad_alpha || !grad_alpha[d]) continue;
+    const size_t count = field_count (g, L, d);
+    double * dst = grad_alpha[d], * tmp = NULL;
+    if (memory == BMG_HOST) {
+      CK (cudaMallocAsync ((void **) &tmp, count*sizeof (double), g->stream));
+      dst = tmp;
+    }
+    CL (bmg_launch_adjoint_faces (g->dim, g->g64[L], d, g->periodic[d], fm->lv[L], fa->lv[L],
+                                  delta_of (g, L), dst, g->stream));
+    if (tmp) {
+      CK (cudaMemcpyAsync (grad_alpha[d], tmp, count*sizeof (double), cudaMemcpyDeviceToHost, g->stream));
+      CK (cudaFreeAsync (tmp, g->stream));
+    }
+  }
+  if (grad_lambda) {
+    const size_t count = field_count (g, L, -1);
+    double * dst = grad_lambda, * tmp = NULL;
+    if (memory == BMG_HOST) {
+      CK (cudaMallocAsync ((void **) &tmp, count*sizeof (double), g->stream));
+      dst = tmp;
+    }
+    CL (bmg_launch_adjoint_cells (g->dim, g->g64[L], fm->lv[L], fa->lv[L], dst, g->stream));
+    if (tmp) {
+      CK (cudaMemcpyAsync (grad_lambda, tmp, count*sizeof (double), cudaMemcpyDeviceToHost, g->stream));
+      CK (cudaFreeAsync (tmp, g->stream));
+    }
+  }
+  CK (cudaStreamSynchronize (g->stream));
+  return fail (BMG_OK);
+}
+
 int bmg_restriction (bmg_grid * g, const bmg_scalar * list)
 {
   if (!g || !list) return fail (BMG_EINVAL);

@@ -570,6 +570,68 @@ void shift_dim (bmg_geom g, double * f, const double * sum, double scale, cudaSt
   k_shift<DIM><<<grid_shape<DIM> (g.n), block_shape<DIM> (), 0, s>>> (g, f, sum, scale);
 }
 
+
+/* ---------------------------------------------------------------- */
+/* adjoint coefficient gradients (differentiable solve)              */
+/* ---------------------------------------------------------------- */
+
+/* For a = L^{-1} b with (L a)_p = lambda_p a_p + sum over faces f of p of
+   alpha_f (a_neighbour - a_p)/Delta^2 (the operator whose residual
+   poisson.h:373-389 computes), and mu the adjoint (L mu = dl/da, homogeneous
+   conditions; L is symmetric):
+     dl/dalpha_f = -[mu_p (a_q - a_p) + mu_q (a_p - a_q)]/Delta^2
+   over the cells p (lower) and q (upper) of face f that are interior (a
+   boundary face has one; ghosts hold the boundary images of a and mu), and
+     dl/dlambda_c = -mu_c a_c.
+   Face n of a periodic direction is the image of face 0: its gradient is
+   carried by face 0 and its own entry is 0. */
+template <int DIM>
+__global__ void k_adjoint_faces (bmg_geom g, int e, int periodic, const double * __restrict__ mu,
+                                 const double * __restrict__ a, double Delta, double * __restrict__ out)
+{
+  const int n = g.n;
+  const int ne = n + 1;
+  const long long total = DIM == 1 ? ne : DIM == 2 ? (long long) ne*n : (long long) ne*n*n;
+  for (long long q = (long long) blockIdx.x*blockDim.x + threadIdx.x; q < total;
+       q += (long long) gridDim.x*blockDim.x) {
+    /* compact face index, C order with n+1 entries along e */
+    int c[3] = {0, 0, 0};
+    {
+      long long r = q;
+      for (int d = DIM - 1; d >= 0; d--) {
+        const int ext = d == e ? ne : n;
+        c[d] = (int) (r % ext);
+        r /= ext;
+      }
+    }
+    const int f = c[e];
+    double v = 0.;
+    if (!(periodic && f == n)) {
+      int lo[3] = {c[0], c[1], c[2]}, hi[3] = {c[0], c[1], c[2]};
+      lo[e] = f - 1; hi[e] = f;
+      if (periodic && f == 0) lo[e] = n - 1;
+      const bool lin = periodic || f >= 1, hin = periodic || f <= n - 1;
+      const long long il = cidx<DIM> (g, lo[0], lo[1], lo[2]), ih = cidx<DIM> (g, hi[0], hi[1], hi[2]);
+      const double al = a[il], ah = a[ih];
+      if (lin) v -= mu[il]*(ah - al);
+      if (hin) v -= mu[ih]*(al - ah);
+      v /= Delta*Delta;
+    }
+    out[q] = v;
+  }
+}
+
+template <int DIM>
+__global__ void k_adjoint_cells (bmg_geom g, const double * __restrict__ mu,
+                                 const double * __restrict__ a, double * __restrict__ out)
+{
+  int i, j, k;
+  if (!cell_of_thread<DIM> (g.n, i, j, k)) return;
+  const long long id = cidx<DIM> (g, i, j, k);
+  long long q = DIM == 1 ? i : DIM == 2 ? (long long) i*g.n + j : ((long long) i*g.n + j)*g.n + k;
+  out[q] = -mu[id]*a[id];
+}
+
 } // namespace
 
 
@@ -778,6 +840,27 @@ int bmg_launch_face_wrap (int dim, bmg_geom g, int face_dim, double * f, cudaStr
   if (dim == 1) k_face_wrap<1><<<nb, 256, 0, s>>> (g, face_dim, f);
   else if (dim == 2) k_face_wrap<2><<<nb, 256, 0, s>>> (g, face_dim, f);
   else k_face_wrap<3><<<nb, 256, 0, s>>> (g, face_dim, f);
+  return status_of_launch ();
+}
+
+int bmg_launch_adjoint_faces (int dim, bmg_geom g, int e, int periodic, const double * mu,
+                              const double * a, double Delta, double * out, cudaStream_t s)
+{
+  long long total = (long long) (g.n + 1);
+  for (int d = 1; d < dim; d++) total *= g.n;
+  const int nb = lin_blocks (total);
+  if (dim == 1) k_adjoint_faces<1><<<nb, 256, 0, s>>> (g, e, periodic, mu, a, Delta, out);
+  else if (dim == 2) k_adjoint_faces<2><<<nb, 256, 0, s>>> (g, e, periodic, mu, a, Delta, out);
+  else k_adjoint_faces<3><<<nb, 256, 0, s>>> (g, e, periodic, mu, a, Delta, out);
+  return status_of_launch ();
+}
+
+int bmg_launch_adjoint_cells (int dim, bmg_geom g, const double * mu, const double * a,
+                              double * out, cudaStream_t s)
+{
+  if (dim == 1) k_adjoint_cells<1><<<grid_shape<1> (g.n), block_shape<1> (), 0, s>>> (g, mu, a, out);
+  else if (dim == 2) k_adjoint_cells<2><<<grid_shape<2> (g.n), block_shape<2> (), 0, s>>> (g, mu, a, out);
+  else k_adjoint_cells<3><<<grid_shape<3> (g.n), block_shape<3> (), 0, s>>> (g, mu, a, out);
   return status_of_launch ();
 }
 

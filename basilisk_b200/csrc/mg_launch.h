@@ -103,6 +103,13 @@ int bmg_launch_fill (int dim, int st, bmg_geom g, void * f, double v, cudaStream
 int bmg_launch_shift (int dim, bmg_geom g, double * f, const double * sum,
                       double scale, cudaStream_t s);
 
+/* adjoint coefficient gradients: face component e into a compact face
+   array, and -mu*a into a compact cell array */
+int bmg_launch_adjoint_faces (int dim, bmg_geom g, int e, int periodic, const double * mu,
+                              const double * a, double Delta, double * out, cudaStream_t s);
+int bmg_launch_adjoint_cells (int dim, bmg_geom g, const double * mu, const double * a,
+                              double * out, cudaStream_t s);
+
 int bmg_launch_face_wrap (int dim, bmg_geom g, int face_dim, double * f, cudaStream_t s);
 
 /* fused red-black relaxation (mg_fused.cu) */

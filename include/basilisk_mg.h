@@ -185,6 +185,19 @@ void mg_cycle (bmg_scalar * a, bmg_scalar * res, bmg_scalar * da,
    as test/variable.c calls it for its face coefficients; list ends with .i=0 */
 int bmg_restriction (bmg_grid * grid, const bmg_scalar * list);
 
+/* ---- differentiation ----------------------------------------------- */
+
+/* Gradients of a loss l(a) with respect to the coefficients of the solve
+   a = L^{-1} b, given the adjoint mu (solved with poisson() from the
+   right-hand side dl/da on a field with the homogeneous conditions of a;
+   L is symmetric): grad_alpha[d] receives dl/dalpha for face component d
+   (compact face arrays, n+1 along d; NULL skips), grad_lambda receives
+   dl/dlambda = -mu a (compact cell array; NULL skips).  dl/db is mu
+   itself.  No counterpart in the reference (whose solver has no
+   derivatives); it differentiates the discrete operator of poisson.h:373-389. */
+int bmg_adjoint_gradients (bmg_grid * grid, bmg_scalar mu, bmg_scalar a,
+                           double * const * grad_alpha, double * grad_lambda, int memory);
+
 /* ---- allocation-free sum ------------------------------------------- */
 
 /* The sum of count doubles at values (device memory), written to *result
