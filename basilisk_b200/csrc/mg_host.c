@@ -719,6 +719,18 @@ static int residual_max (bmg_grid * g, field_t * a, const double * b, const coef
   return BMG_OK;
 }
 
+/* an event on stream s: a graph node of its own while s is being captured
+   (the external flag), a plain record otherwise (the flag is refused
+   outside a capture) */
+static cudaError_t record_event (cudaEvent_t e, cudaStream_t s)
+{
+  enum cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  cudaError_t r = cudaStreamIsCapturing (s, &cs);
+  if (r != cudaSuccess) return r;
+  return cs == cudaStreamCaptureStatusActive ?
+    cudaEventRecordWithFlags (e, s, cudaEventRecordExternal) : cudaEventRecord (e, s);
+}
+
 /* the levels of the single-CTA bottom solve: minlevel up to the largest
    level with at most BMG_BOTTOM_CELLS cells whose staged arrays fit the
    bottom kernel's shared memory; fills bl[0..top-minlevel] */
@@ -813,7 +825,7 @@ static int cycle_launches (bmg_grid * g, field_t * a, const levels_t * lv, const
     const bmg_coef * al = st == BMG_ST_F64 ? c->alpha64[l] : c->alpha32[l];
     const bmg_coef la = st == BMG_ST_F64 ? c->lambda64[l] : c->lambda32[l];
     const int timed = g->timing && l == L && maxlevel == L;
-    if (timed) CK (cudaEventRecordWithFlags (g->evr0, s, cudaEventRecordExternal));
+    if (timed) CK (record_event (g->evr0, s));
     if (g->relax == BMG_RELAX_RBGS && dim == 2) {
       /* several complete red-black sweeps per launch, ping-pong buffers */
       const int S = bmg_tile_sweeps (st);
@@ -845,7 +857,7 @@ static int cycle_launches (bmg_grid * g, field_t * a, const levels_t * lv, const
     bytes += nrelax*narr*ncells (g, l)*es_of (st);
     sweeps += nrelax;
     if (timed) {
-      CK (cudaEventRecordWithFlags (g->evr1, s, cudaEventRecordExternal));
+      CK (record_event (g->evr1, s));
       w->relax_bytes += nrelax*narr*ncells (g, l)*es_of (st);
       w->relax_sweeps += nrelax;
     }

@@ -126,9 +126,15 @@ def test_two_phase_config_small(graphs):
     adapts upward; trajectories identical."""
     from basilisk_b200 import problems
     prob = problems.two_phase_2d(depth=7, seed=11)
-    og, ost, g, a, gst = solve_both(prob, "jacobi", tolerance=1e-6, graphs=graphs)
+    og = oracle_grid(prob, relax=RELAX["jacobi"])
+    ost = og.poisson(tolerance=1e-6, nrelax=4)
+    g, a, b, alpha, lam = gpu_grid(prob, relax="jacobi", graphs=graphs)
+    g.set_timing(True)       # per-cycle CUDA events, captured or plain
+    gst = g.poisson(a, b, alpha=alpha, lambda_=lam, tolerance=1e-6, nrelax=4)
     assert_same(ost, gst, og.get_a(), a.get(), prob["b"])
     assert ost["nrelax"] > 4
+    c = g.counters()
+    assert c["cycles"] == gst["i"] and c["cycle_ms"] > 0 and c["relax_ms"] > 0
 
 
 def test_periodic_gaussians_128():
