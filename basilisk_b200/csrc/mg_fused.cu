@@ -113,6 +113,47 @@ template <typename T> struct Pair;
 template <> struct Pair<float> { typedef float2 type; };
 template <> struct Pair<double> { typedef double2 type; };
 
+/* four consecutive elements of a row (16-byte aligned in global memory) */
+template <typename T> struct Quad { T x, y, z, w; };
+
+__device__ __forceinline__ Quad<float> load_quad (const float * p)
+{
+  const float4 v = *(const float4 *) p;
+  Quad<float> q = {v.x, v.y, v.z, v.w};
+  return q;
+}
+
+__device__ __forceinline__ Quad<double> load_quad (const double * p)
+{
+  const double2 a = *(const double2 *) p, b = *(const double2 *) (p + 2);
+  Quad<double> q = {a.x, a.y, b.x, b.y};
+  return q;
+}
+
+__device__ __forceinline__ void store_quad (float * p, const Quad<float> & q)
+{
+  *(float4 *) p = make_float4 (q.x, q.y, q.z, q.w);
+}
+
+__device__ __forceinline__ void store_quad (double * p, const Quad<double> & q)
+{
+  *(double2 *) p = make_double2 (q.x, q.y);
+  *(double2 *) (p + 2) = make_double2 (q.z, q.w);
+}
+
+/* a quad starting at an even column q (m = q/2, even): elements q and q + 2
+   belong to colour c0, q + 1 and q + 3 to the other colour, each pair at
+   [m, m + 1] of its colour array */
+template <typename T>
+__device__ __forceinline__ void put_quad (T * a0, T * a1, int off, const Quad<T> & v)
+{
+  typedef typename Pair<T>::type T2;
+  T2 e, o;
+  e.x = v.x; e.y = v.z; o.x = v.y; o.y = v.w;
+  *(T2 *) (a0 + off) = e;
+  *(T2 *) (a1 + off) = o;
+}
+
 /* BX x BY threads: thread (tx, ty) updates the cell pair 2 tx, 2 tx + 1 of
    row ty + lo in every colour pass */
 template <typename T, int TS, int S, bool LAM, int BX, int BY>
@@ -137,12 +178,56 @@ k_relax_tile2d (bmg_geom g, T * __restrict__ out, const T * __restrict__ in,
   }
   const int n = g.n, tx = threadIdx.x, ty = threadIdx.y;
   const int tid = ty*BX + tx, nth = BX*BY;
+  constexpr int RW = 32/BX;     /* rows per warp */
+  static_assert (32 % BX == 0 && BY % (2*RW) == 0, "warps cover whole row pairs");
+  const int pr = 2*RW*(ty/(2*RW)) + 2*(ty % RW) + ((ty/RW) & 1);
   const int i0 = blockIdx.y*TS - H, j0 = blockIdx.x*TS - H;   /* global index of (0,0) */
   const int px = bc.periodic[0], py = bc.periodic[1];
   const int base = (i0 + j0) & 1;                             /* colour of (0,0) */
   /* the whole staged region inside the domain: no cell checks needed */
   const bool inner = i0 >= 0 && i0 + W <= n && j0 >= 0 && j0 + W <= n;
 
+  if (inner) {
+    /* the staged region lies inside the domain: 16-byte loads of four
+       cells, split into the colour arrays with pair stores (all loads of
+       one thread are issued before its stores) */
+    constexpr int QW = W/4;
+    static_assert (W % 4 == 0 && TS % 4 == 0 && H % 4 == 0, "quads of cells");
+    for (int idx = tid; idx < W*QW; idx += nth) {
+      const int p = idx/QW, k = idx - p*QW, q = 4*k;
+      const int c0 = (base + p + q) & 1;
+      const long long id = cidx<2> (g, i0 + p, j0 + q, 0);
+      const Quad<T> va = load_quad (in + id), vr = load_quad (res + id);
+      Quad<T> vl, vx, vy;
+      if (LAM) vl = load_quad (lam.p + id);
+      if (ax.p) vx = load_quad (ax.p + id);
+      else vx.x = vx.y = vx.z = vx.w = ax.c;
+      if (ay.p) vy = load_quad (ay.p + id);
+      else vy.x = vy.y = vy.z = vy.w = ay.c;
+      put_quad (sa[c0], sa[c0 ^ 1], p*M + 2*k, va);
+      put_quad (sr[c0], sr[c0 ^ 1], p*M + 2*k, vr);
+      if (LAM) put_quad (sl[c0], sl[c0 ^ 1], p*M + 2*k, vl);
+      put_quad (sx[c0], sx[c0 ^ 1], p*M + 2*k, vx);
+      put_quad (sy[c0], sy[c0 ^ 1], p*MY + 2*k, vy);
+    }
+    /* the last x-face row (face i0 + W <= n) and y-face column (j0 + W <= n;
+       face n of a periodic direction is face 0) */
+    const int fi = real_face (i0 + W, n, px), fj = real_face (j0 + W, n, py);
+    for (int idx = tid; idx < QW + W; idx += nth) {
+      if (idx < QW) {
+        const int q = 4*idx, c0 = (base + W + q) & 1;
+        Quad<T> vx;
+        if (ax.p) vx = load_quad (ax.p + cidx<2> (g, fi, j0 + q, 0));
+        else vx.x = vx.y = vx.z = vx.w = ax.c;
+        put_quad (sx[c0], sx[c0 ^ 1], W*M + 2*idx, vx);
+      }
+      else {
+        const int p = idx - QW, c = (base + p + W) & 1;
+        sy[c][p*MY + W/2] = ay.p ? ay.p[cidx<2> (g, i0 + p, fj, 0)] : ay.c;
+      }
+    }
+  }
+  else {
   /* stage cells and faces with asynchronous copies (zero fill outside) */
   for (int idx = tid; idx < W*W; idx += nth) {
     const int p = idx/W, q = idx - p*W;
@@ -171,6 +256,7 @@ k_relax_tile2d (bmg_geom g, T * __restrict__ out, const T * __restrict__ in,
     const bool ok = ri >= 0 && fj >= 0;
     if (ay.p) cp_async_elem (&sy[c][p*MY + (q >> 1)], ay.p + (ok ? cidx<2> (g, ri, fj, 0) : 0), ok);
     else sy[c][p*MY + (q >> 1)] = ok ? ay.c : T(0);
+  }
   }
   cp_async_wait_all ();
   __syncthreads ();
@@ -212,8 +298,10 @@ k_relax_tile2d (bmg_geom g, T * __restrict__ out, const T * __restrict__ in,
       T * __restrict__ a = sa[c];
       const T * __restrict__ r = sr[c];
       const T * __restrict__ l = sl[c];
-      /* thread (tx, ty): cells m0 = 2 tx and m0 + 1 of colour c in row lo + ty */
-      const int p = lo + ty;
+      /* thread (tx, ty): cells m0 = 2 tx and m0 + 1 of colour c in row lo + pr;
+         a warp covers RW rows of one parity (pr interleaves them), so the
+         colour offset o, and every branch on it, is uniform per warp */
+      const int p = lo + pr;
       if (p < hi) {
         const int o = (c - base - p) & 1;        /* column offset of colour c */
         const int mlo = (lo - o + 1) >> 1, mhi = (hi - o + 1) >> 1;
@@ -268,6 +356,19 @@ k_relax_tile2d (bmg_geom g, T * __restrict__ out, const T * __restrict__ in,
     }
 
   /* write the tile interior back, with its ghost images */
+  if (inner) {
+    /* no domain-boundary cell in the interior: 16-byte stores, no ghosts */
+    constexpr int QT = TS/4;
+    for (int idx = tid; idx < TS*QT; idx += nth) {
+      const int rr = idx/QT, k = idx - rr*QT;
+      const int p = rr + H, q = H + 4*k, c0 = (base + p + q) & 1, m = q >> 1;
+      Quad<T> v;
+      v.x = sa[c0][p*M + m]; v.z = sa[c0][p*M + m + 1];
+      v.y = sa[c0 ^ 1][p*M + m]; v.w = sa[c0 ^ 1][p*M + m + 1];
+      store_quad (out + cidx<2> (g, blockIdx.y*TS + rr, blockIdx.x*TS + 4*k, 0), v);
+    }
+    return;
+  }
   for (int idx = tid; idx < TS*TS; idx += nth) {
     const int rr = idx/TS, s = idx - rr*TS;
     const int gi = blockIdx.y*TS + rr, gj = blockIdx.x*TS + s;
@@ -342,7 +443,7 @@ __device__ __forceinline__ void bot_copy (const bmg_geom & gg, T * gp, const bmg
       if (DIM == 1) { gi = cidx<1> (gg, k, 0, 0); si = cidx<1> (gs, k, 0, 0); }
       else if (DIM == 2) { gi = cidx<2> (gg, i, k, 0); si = cidx<2> (gs, i, k, 0); }
       else { gi = cidx<3> (gg, i, j, k); si = cidx<3> (gs, i, j, k); }
-      if (to_shared) sp[si] = gp[gi];
+      if (to_shared) cp_async_elem (&sp[si], &gp[gi], true);   /* waited for by the caller */
       else gp[gi] = sp[si];
     }
   }
@@ -558,6 +659,43 @@ __device__ __forceinline__ void bot_pass2d_any (const bmg_geom & g, void * dav, 
   else bot_pass2d<T, false, false, 1> (g, a, b, ax, ay, axc, ayc, lam, lamc, D2, bc, color, nt);
 }
 
+/* all nrelax sweeps of one 2D level, every parameter in registers (the
+   per-level parameters live in the kernel's parameter space, and reading
+   them inside the sweep loop costs a constant-cache miss per pass) */
+template <typename T, bool AST, bool LST>
+__device__ __forceinline__ void bot_sweeps2d (const bmg_geom g, T * a, const T * b, const T * ax,
+                                              const T * ay, T axc, T ayc, const T * lam, T lamc,
+                                              T D2, const BCH bc, int nrelax, int nt, bool small)
+{
+  for (int sw = 0; sw < nrelax; sw++)
+    for (int color = 0; color < 2; color++) {
+      bot_pass2d<T, AST, LST, 1> (g, a, b, ax, ay, axc, ayc, lam, lamc, D2, bc, color, nt);
+      if (small) __syncwarp ();
+      else __syncthreads ();
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ void bot_level2d (const bmg_geom g, void * dav, const void * resv,
+                                             const void * axv, const void * ayv, double axc,
+                                             double ayc, const void * lamv, double lamc,
+                                             double Delta, const BCH bc, int nrelax, int nt,
+                                             bool small)
+{
+  T * a = (T *) dav;
+  const T * b = (const T *) resv, * ax = (const T *) axv, * ay = (const T *) ayv,
+    * lam = (const T *) lamv;
+  const T D2 = (T) Delta*(T) Delta;
+  if (ax && lam)
+    bot_sweeps2d<T, true, true> (g, a, b, ax, ay, (T) axc, (T) ayc, lam, (T) lamc, D2, bc, nrelax, nt, small);
+  else if (ax)
+    bot_sweeps2d<T, true, false> (g, a, b, ax, ay, (T) axc, (T) ayc, lam, (T) lamc, D2, bc, nrelax, nt, small);
+  else if (lam)
+    bot_sweeps2d<T, false, true> (g, a, b, ax, ay, (T) axc, (T) ayc, lam, (T) lamc, D2, bc, nrelax, nt, small);
+  else
+    bot_sweeps2d<T, false, false> (g, a, b, ax, ay, (T) axc, (T) ayc, lam, (T) lamc, D2, bc, nrelax, nt, small);
+}
+
 template <int DIM>
 __device__ __forceinline__ void bot_restrict_st (int stf, const bmg_geom & gf, const void * f, int stc,
                                  const bmg_geom & gc, void * c)
@@ -582,7 +720,8 @@ template <int DIM>
 __global__ void __launch_bounds__ (1024, 1) k_bottom (const __grid_constant__ BotParams P)
 {
   extern __shared__ __align__ (16) unsigned char bsm[];
-  /* stage the coefficients of every level */
+  const BCH bc = P.bc;
+  /* stage the coefficients of every level (asynchronous copies) */
   for (int m = 0; m < P.nlev; m++) {
     const BotLevel & L = P.lv[m];
     const BotStage & S = P.sm[m];
@@ -600,6 +739,7 @@ __global__ void __launch_bounds__ (1024, 1) k_bottom (const __grid_constant__ Bo
   else
     bot_copy_st<DIM> (P.lv[top].st, P.lv[top].g, P.lv[top].res, P.sm[top].gs,
                       sm_at (bsm, P.sm[top].off_res), 1);
+  cp_async_wait_all ();
   __syncthreads ();
   /* restriction down to the coarsest level (multigrid-common.h:368-404) */
   for (int m = top - 1; m >= 0; m--) {
@@ -624,20 +764,26 @@ __global__ void __launch_bounds__ (1024, 1) k_bottom (const __grid_constant__ Bo
     const void * lam = sm_at (bsm, S.off_lambda);
     /* levels of at most BOT_WARP_CELLS cells are relaxed by warp 0 alone,
        with warp barriers; the other warps wait at the level's end */
-    const bool small = S.gs.size <= BOT_WARP_CELLS;
-    if (!small || threadIdx.x < 32)
-      for (int sw = 0; sw < P.nrelax; sw++)
+    const bmg_geom gs = S.gs;
+    const bool small = gs.size <= BOT_WARP_CELLS;
+    const int nt = small ? 32 : blockDim.x, nrelax = P.nrelax, st = L.st;
+    if (DIM == 2 && (al[0] == NULL) == (al[1] == NULL)) {
+      /* x and y coefficients both stored or both constant */
+      const double axc = L.alpha[0].c, ayc = L.alpha[1].c, lamc = L.lambda.c, Delta = L.Delta;
+      if (!small || threadIdx.x < 32) {
+        if (st == BMG_ST_F64)
+          bot_level2d<double> (gs, da, res, al[0], al[1], axc, ayc, lam, lamc, Delta, bc, nrelax, nt, small);
+        else
+          bot_level2d<float> (gs, da, res, al[0], al[1], axc, ayc, lam, lamc, Delta, bc, nrelax, nt, small);
+      }
+    }
+    else if (!small || threadIdx.x < 32)
+      for (int sw = 0; sw < nrelax; sw++)
         for (int color = 0; color < 2; color++) {
-          const int nt = small ? 32 : blockDim.x;
-          if (DIM == 2) {
-            /* x and y coefficients are both stored or both constant */
-            if (L.st == BMG_ST_F64) bot_pass2d_any<double> (S.gs, da, res, al, L, lam, P.bc, color, nt);
-            else bot_pass2d_any<float> (S.gs, da, res, al, L, lam, P.bc, color, nt);
-          }
-          else if (L.st == BMG_ST_F64)
-            bot_pass<DIM, double> (S.gs, da, res, al, L, lam, P.bc, color, 0, nt);
+          if (st == BMG_ST_F64)
+            bot_pass<DIM, double> (gs, da, res, al, L, lam, bc, color, 0, nt);
           else
-            bot_pass<DIM, float> (S.gs, da, res, al, L, lam, P.bc, color, 0, nt);
+            bot_pass<DIM, float> (gs, da, res, al, L, lam, bc, color, 0, nt);
           if (small) __syncwarp ();
           else __syncthreads ();
         }
