@@ -148,3 +148,106 @@ def poisson1d_program(make, depths=(5, 6, 7, 8)):
         err = np.max(np.abs(g.get_a() - solution(x, y, z)))
         lines.append("%d %g" % (depth, err))
     return lines, g
+
+
+# ---------------------------------------------------------------------
+# quadtree programs: a *tree factory* ``make(maxdepth, origin)`` returns an
+# object with the interface of ``oracle.tree.Tree`` (the CPU oracle) or of
+# ``basilisk_b200.TreeGrid`` (the CUDA library).
+# ---------------------------------------------------------------------
+
+def dirichlet_tree(t, solution):
+    """``a[side] = dirichlet(solution)`` on every side and level: a tree
+    applies the condition on every level (tree_boundary_level)."""
+    for l in range(t.depth + 1):
+        for side in range(4):
+            x, y = t.boundary_points(l, side)
+            t.set_bc(side, DIRICHLET, level=l, values=solution(x, y, 0.0))
+
+
+def set_cells(t, which, func):
+    """A cell field from its expression, on every level (only leaf values
+    are read by the solver; the others are overwritten by restriction and
+    prolongation)."""
+    for l in range(t.depth + 1):
+        x, y = t.centers(l)
+        t.set_level(which, l, func(x, y))
+
+
+def leaf_max_error(t, which, solution):
+    err = 0.0
+    for l in range(t.depth + 1):
+        leaf = (t.flags(l) & 2) != 0
+        if leaf.any():
+            x, y = t.centers(l)
+            e = np.abs(t.get_level(which, l) - solution(x, y, 0.0))[leaf]
+            err = max(err, float(e.max()))
+    return err
+
+
+def circle_refinement(depth):
+    """``refine (level < depth - 2 || level <= depth*(1. - sqrt(x*x + y*y)))``
+    (test/circle.c:70, z = 0 in two dimensions)."""
+    def cond(level, x, y):
+        return level < depth - 2 or level <= depth * (1. - math.sqrt(x * x + y * y + 0. * 0.))
+    return cond
+
+
+def circle_program(make, depths=(7, 8, 9, 10), niter=15):
+    """test/circle.c: Dirichlet cos(3πx)cos(3πy) on a quadtree refined inside
+    a circle, 15 direct mg_cycle calls (nrelax 4, minlevel 0)."""
+    from oracle.tree import A, B  # field ids are shared with the library
+    lines, t = [], None
+    for depth in depths:
+        t = make(depth, (-0.5, -0.5))
+        t.refine(circle_refinement(depth))
+
+        def solution(x, y, z):
+            return cos(3. * PI * x) * cos(3. * PI * y) * cos(3. * PI * z)
+
+        dirichlet_tree(t, solution)
+        set_cells(t, B, lambda x, y: - 9. * 2 * PI * PI * cos(3. * PI * x) * cos(3. * PI * y) * cos(3. * PI * 0.))
+        set_cells(t, A, lambda x, y: np.zeros_like(x))
+        t.set_alpha_const(1.0)
+        t.set_lambda_const(0.0)
+        t.residual()
+        maxres = []
+        for _ in range(niter):
+            t.mg_cycle(4, 0, t.depth)
+            maxres.append(t.residual())
+        lines += ["residual %d %d %.1g" % (depth, i, r) for i, r in enumerate(maxres)]
+        lines.append("max error %d %g" % (depth, leaf_max_error(t, A, solution)))
+    return lines, t
+
+
+def circle_variable_program(make, depths=(7, 8, 9, 10), niter=13):
+    """test/circle-variable.c: alpha = x + y + 2 on the faces, Dirichlet
+    sin(3πx)sin(3πy), 13 direct mg_cycle calls after restriction({c})."""
+    from oracle.tree import A, B, ALPHA_X, ALPHA_Y
+    lines, t = [], None
+    for depth in depths:
+        t = make(depth, (-0.5, -0.5))
+        t.refine(circle_refinement(depth))
+
+        def solution(x, y, z):
+            return sin(3. * PI * x) * sin(3. * PI * y)
+
+        dirichlet_tree(t, solution)
+        set_cells(t, B, lambda x, y: (-18. * PI ** 2 * sin(3. * PI * x) * sin(3. * PI * y) * (x + y + 2.) +
+                                      3. * PI * cos(3. * PI * x) * sin(3. * PI * y) +
+                                      3. * PI * sin(3. * PI * x) * cos(3. * PI * y)))
+        set_cells(t, A, lambda x, y: np.zeros_like(x))
+        for l in range(t.depth + 1):
+            for d, which in ((0, ALPHA_X), (1, ALPHA_Y)):
+                fx, fy = t.face_centers(l, d)
+                t.set_level(which, l, fx + fy + 2.)
+        t.set_lambda_const(0.0)
+        t.restrict_coefficients()
+        t.residual()
+        maxres = []
+        for _ in range(niter):
+            t.mg_cycle(4, 0, t.depth)
+            maxres.append(t.residual())
+        lines += ["residual %d %d %.1g" % (depth, i, r) for i, r in enumerate(maxres)]
+        lines.append("max error %d %g" % (depth, leaf_max_error(t, A, solution)))
+    return lines, t
