@@ -9,7 +9,7 @@ of that ABI: the grid/field front end (``Grid``), the reference's Python
 """
 from . import _lib
 from ._lib import BMGError, load
-from .grid import Grid, Scalar, FaceVector, set_tolerance, get_tolerance, set_niter
+from .grid import Grid, TreeGrid, Scalar, FaceVector, set_tolerance, get_tolerance, set_niter
 from ._build import build
 
 
@@ -20,5 +20,5 @@ def poisson(a, b, alpha=None, lambda0=None, tolerance=1e-3, nrelax=0, minlevel=0
                           nrelax=nrelax, minlevel=minlevel)
 
 
-__all__ = ["Grid", "Scalar", "FaceVector", "poisson", "build", "load", "BMGError",
+__all__ = ["Grid", "TreeGrid", "Scalar", "FaceVector", "poisson", "build", "load", "BMGError",
            "set_tolerance", "get_tolerance", "set_niter"]

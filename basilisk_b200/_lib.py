@@ -55,6 +55,9 @@ class Poisson(ctypes.Structure):
 
 RELAX_FN = ctypes.CFUNCTYPE(None, ctypes.POINTER(bmg_scalar), ctypes.POINTER(bmg_scalar),
                             ctypes.c_int, ctypes.c_void_p)
+# int (*) (int level, double x, double y, double z, void * data)
+REFINE_COND = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                               ctypes.c_double, ctypes.c_void_p)
 RESIDUAL_FN = ctypes.CFUNCTYPE(ctypes.c_double, ctypes.POINTER(bmg_scalar),
                                ctypes.POINTER(bmg_scalar), ctypes.POINTER(bmg_scalar),
                                ctypes.c_void_p)
@@ -77,6 +80,9 @@ class bmg_counters(ctypes.Structure):
 
 
 # every function the header declares, with its signature
+# flags of bmg_tree_flags (basilisk_mg.h)
+TREE_ACTIVE, TREE_LEAF, TREE_HALO, TREE_PROLONGATION = 1, 2, 4, 8
+
 P = ctypes.c_void_p
 I = ctypes.c_int
 D = ctypes.c_double
@@ -116,6 +122,10 @@ SIGNATURES = {
     "mg_cycle": (None, [ctypes.POINTER(bmg_scalar), ctypes.POINTER(bmg_scalar),
                         ctypes.POINTER(bmg_scalar), P, P, I, I, I]),
     "bmg_restriction": (I, [P, ctypes.POINTER(bmg_scalar)]),
+    "bmg_tree_refine": (I, [P, REFINE_COND, P]),
+    "bmg_tree_info": (I, [P, ctypes.POINTER(I), ctypes.POINTER(ctypes.c_longlong)]),
+    "bmg_tree_flags": (I, [P, I, ctypes.POINTER(ctypes.c_ubyte)]),
+    "bmg_bc_level": (I, [P, bmg_scalar, I, I, I, DP, I]),
     "bmg_get_counters": (I, [P, ctypes.POINTER(bmg_counters)]),
     "bmg_reset_counters": (I, [P]),
     "bmg_set_timing": (I, [P, I]),

@@ -18,6 +18,7 @@
 
 #include "basilisk_mg.h"
 #include "mg_launch.h"
+#include "mg_grid.h"
 
 int NITERMAX = 100, NITERMIN = 1;   /* poisson.h:102 */
 double TOLERANCE = 1e-3;            /* poisson.h:103 */
@@ -31,42 +32,7 @@ static bmg_grid * current_grid = NULL;
    kernel on the red-black path */
 #define BMG_BOTTOM_CELLS 4096
 
-typedef struct {
-  int used;
-  int face_dim;         /* -1: cell field; d: component d of a face vector */
-  int is_const;
-  double cval;
-  double * buf;         /* all levels */
-  double * lv[BMG_MAXLEVEL + 1];
-  int bctype[6];
-  double bccval[6];
-  double * bcval[6];    /* device, n^(dim-1) values of the finest level */
-} field_t;
 
-struct bmg_grid {
-  int dim, depth, device;
-  double L0, X0, Y0, Z0;
-  int periodic[3];
-  int relax, precision, use_graphs, timing;
-  cudaStream_t stream;
-  int own_stream;
-  bmg_geom g64[BMG_MAXLEVEL + 1], g32[BMG_MAXLEVEL + 1];
-  size_t off64[BMG_MAXLEVEL + 2], off32[BMG_MAXLEVEL + 2];
-  field_t * fields;
-  int nfields, cap;
-  /* workspace (allocated on first solve) */
-  double * ws64;        /* da, da2, res: 3 all-level FP64 arrays */
-  float * ws32;         /* da, da2, res, alpha x/y/z, lambda: FP32 levels */
-  double * bproj;       /* zero-mean copy of b (mixed form, singular problems) */
-  unsigned long long * d_maxres;
-  double * d_sum, * d_partials;
-  int npartials;
-  double * h_pinned;
-  bmg_counters counters;
-  cudaEvent_t ev0, ev1, evr0, evr1;
-  struct graph_entry * graphs;     /* captured V-cycles, see run_cycle() */
-  unsigned long long clock;
-};
 
 const char * bmg_error_string (int s)
 {
@@ -101,7 +67,6 @@ static int fail (int s) { last_error = s; return s; }
    captured once into a CUDA graph and replayed afterwards */
 #define NGRAPH_MAX 256
 #define NGRAPH_DEFAULT 64
-typedef struct { double bytes; long long launches, sweeps; double relax_bytes; long long relax_sweeps; } work_t;
 struct graph_entry {
   int valid;
   unsigned long long stamp;
@@ -113,6 +78,7 @@ struct graph_entry {
 
 static void graphs_clear (struct bmg_grid * g)
 {
+  bmg_tree_graphs_clear (g);
   if (!g->graphs) return;
   for (int i = 0; i < NGRAPH_MAX; i++)
     if (g->graphs[i].valid) {
@@ -223,11 +189,15 @@ void bmg_grid_free (bmg_grid * g)
   cudaSetDevice (g->device);
   cudaStreamSynchronize (g->stream);
   graphs_clear (g);
+  bmg_tree_free (g);
   free (g->graphs);
   for (int i = 1; i < g->nfields; i++)
     if (g->fields[i].used) {
       cudaFree (g->fields[i].buf);
-      for (int s = 0; s < 6; s++) cudaFree (g->fields[i].bcval[s]);
+      for (int s = 0; s < 6; s++) {
+        cudaFree (g->fields[i].bcval[s]);
+        for (int l = 0; l <= BMG_MAXLEVEL; l++) cudaFree (g->fields[i].bclv[s][l]);
+      }
     }
   free (g->fields);
   cudaFree (g->ws64); cudaFree (g->ws32); cudaFree (g->bproj);
@@ -423,7 +393,10 @@ int bmg_field_delete (bmg_grid * g, bmg_scalar s)
   cudaSetDevice (g->device);
   cudaStreamSynchronize (g->stream);
   cudaFree (f->buf);
-  for (int k = 0; k < 6; k++) cudaFree (f->bcval[k]);
+  for (int k = 0; k < 6; k++) {
+    cudaFree (f->bcval[k]);
+    for (int l = 0; l <= BMG_MAXLEVEL; l++) cudaFree (f->bclv[k][l]);
+  }
   memset (f, 0, sizeof *f);
   graphs_clear (g);
   return BMG_OK;
@@ -562,6 +535,29 @@ int bmg_bc (bmg_grid * g, bmg_scalar s, int side, int type, double value,
   return BMG_OK;
 }
 
+int bmg_bc_level (bmg_grid * g, bmg_scalar s, int side, int type, int level,
+                  const double * values, int memory)
+{
+  field_t * f = field_get (g, s.i);
+  if (!f || side < 0 || side >= 2*g->dim || level < 0 || level > g->depth || !values ||
+      (type != BMG_NEUMANN && type != BMG_DIRICHLET) || f->face_dim >= 0 ||
+      (memory != BMG_HOST && memory != BMG_DEVICE))
+    return fail (BMG_EINVAL);
+  if (g->periodic[side/2]) return fail (BMG_EINVAL);
+  CK (cudaSetDevice (g->device));
+  f->bctype[side] = type;
+  size_t n = 1;
+  for (int d = 1; d < g->dim; d++) n *= (size_t) 1 << level;
+  if (!f->bclv[side][level])
+    CK (cudaMalloc ((void **) &f->bclv[side][level], n*sizeof (double)));
+  CK (cudaMemcpyAsync (f->bclv[side][level], values, n*sizeof (double),
+                       memory == BMG_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                       g->stream));
+  CK (cudaStreamSynchronize (g->stream));
+  graphs_clear (g);
+  return BMG_OK;
+}
+
 /* ------------------------------------------------------------------ */
 /* workspace                                                           */
 /* ------------------------------------------------------------------ */
@@ -591,6 +587,11 @@ static int ensure_workspace (bmg_grid * g, int mixed)
   }
   return BMG_OK;
 }
+
+int bmg_i_fail (int status) { return fail (status); }
+field_t * bmg_i_field (bmg_grid * g, int handle) { return field_get (g, handle); }
+int bmg_i_workspace (bmg_grid * g) { return ensure_workspace (g, 0); }
+double * bmg_i_ws64 (bmg_grid * g, int which, int level) { return ws64 (g, which, level); }
 
 /* ------------------------------------------------------------------ */
 /* the solver proper                                                   */
@@ -1094,6 +1095,7 @@ int bmg_poisson (bmg_grid * g, struct Poisson p, mgstats * out)
   if (out) *out = zero;
   if (!g || !out) return fail (BMG_EINVAL);
   CK (cudaSetDevice (g->device));
+  if (g->tree) return bmg_tree_poisson (g, p, out);
   field_t * a, * b, * res = NULL;
   if (check_cell (g, p.a.i, &a) || check_cell (g, p.b.i, &b)) return fail (BMG_EINVAL);
   if (p.res && p.res[0].i && check_cell (g, p.res[0].i, &res)) return fail (BMG_EINVAL);
@@ -1127,6 +1129,7 @@ void bmg_relax (bmg_scalar * da, bmg_scalar * res, int l, void * data)
   field_t * fa, * fr;
   if (!g || !p || !da || !res || check_cell (g, da[0].i, &fa) || check_cell (g, res[0].i, &fr) ||
       l < 0 || l > g->depth) { fail (BMG_EINVAL); return; }
+  if (g->tree) { bmg_tree_relax (g, fa, fr, l, p); return; }
   coefs_t c;
   if (resolve_coefs (g, p->alpha, p->lambda, &c)) return;
   bmg_bcdesc bc;
@@ -1159,6 +1162,11 @@ double bmg_residual (bmg_scalar * al, bmg_scalar * bl, bmg_scalar * resl, void *
     fail (BMG_EINVAL);
     return NAN;
   }
+  if (g->tree) {
+    double m = NAN;
+    if (bmg_tree_residual (g, a, b, res, p, &m)) return NAN;
+    return m;
+  }
   coefs_t c;
   if (resolve_coefs (g, p->alpha, p->lambda, &c)) return NAN;
   double m = NAN;
@@ -1179,6 +1187,7 @@ mgstats mg_solve (struct MGSolve p)
     return s;
   }
   if (cudaSetDevice (g->device) != cudaSuccess) { fail (BMG_ECUDA); return s; }
+  if (g->tree) { bmg_tree_mg_solve (g, p, &s); return s; }
   struct Poisson * pp = (struct Poisson *) p.data;
   field_t * a, * b, * res = NULL;
   if (check_cell (g, p.a[0].i, &a) || check_cell (g, p.b[0].i, &b)) return s;
@@ -1203,6 +1212,7 @@ void mg_cycle (bmg_scalar * al, bmg_scalar * resl, bmg_scalar * dal,
   field_t * a, * res, * da;
   if (check_cell (g, al[0].i, &a) || check_cell (g, resl[0].i, &res) ||
       check_cell (g, dal[0].i, &da)) return;
+  if (g->tree) { bmg_tree_mg_cycle (g, a, res, da, p, nrelax, minlevel, maxlevel); return; }
   coefs_t c;
   if (resolve_coefs (g, p->alpha, p->lambda, &c)) return;
   if (ensure_workspace (g, 0)) return;
@@ -1239,6 +1249,7 @@ int bmg_adjoint_gradients (bmg_grid * g, bmg_scalar mu, bmg_scalar a, double * c
 {
   field_t * fm, * fa;
   if (!g || check_cell (g, mu.i, &fm) || check_cell (g, a.i, &fa)) return fail (BMG_EINVAL);
+  if (g->tree) return fail (BMG_EUNSUPPORTED);
   if (memory != BMG_DEVICE && memory != BMG_HOST) return fail (BMG_EINVAL);
   CK (cudaSetDevice (g->device));
   const int L = g->depth;
@@ -1278,6 +1289,7 @@ int bmg_restriction (bmg_grid * g, const bmg_scalar * list)
 {
   if (!g || !list) return fail (BMG_EINVAL);
   CK (cudaSetDevice (g->device));
+  if (g->tree) return bmg_tree_restriction (g, list);
   for (const bmg_scalar * s = list; s->i; s++) {
     field_t * f = field_get (g, s->i);
     if (!f) return fail (BMG_EINVAL);

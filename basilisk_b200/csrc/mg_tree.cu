@@ -1,0 +1,421 @@
+/*
+ * mg_tree.cu -- CUDA kernels of the quadtree path (two dimensions, FP64).
+ *
+ * Every kernel walks a cell list (mg_tree.h) with a grid-stride loop: the
+ * tree's cells of one kind on one or several levels, whose data sit in the
+ * dense level arrays of the grid.  The arithmetic follows the reference's
+ * evaluation order, so that FP64 results are bit-identical to the oracle
+ * (built with --fmad=false like the rest of the library):
+ *   restriction_average, face_average   grid/multigrid-common.h:26-55
+ *   bilinear, refine_bilinear           grid/multigrid-common.h:124-146
+ *   box boundary on trees               grid/tree.h:1139-1209, 1286-1367
+ *   relax                               poisson.h:303-320
+ *   residual, tree branch + halo_face   poisson.h:355-372,
+ *                                       grid/tree-common.h:374-411
+ */
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "basilisk_mg.h"
+#include "mg_device.cuh"
+#include "mg_tree.h"
+
+using namespace bmgd;
+
+namespace {
+
+typedef bmg_tree_levels TL;
+
+__device__ __forceinline__ void unpack (uint32_t e, int & l, int & i, int & j)
+{
+  l = (int) (e >> 28);
+  i = (int) ((e >> 14) & 0x3FFFu) - 1;
+  j = (int) (e & 0x3FFFu) - 1;
+}
+
+/* element index of cell (i, j) of level l in an all-level buffer */
+__device__ __forceinline__ long long gidx (const TL & T, int l, int i, int j)
+{
+  return T.off[l] + cidx<2> (T.g[l], i, j, 0);
+}
+
+__device__ __forceinline__ double coef (const bmg_tree_coef & c, long long id)
+{
+  return c.p ? c.p[id] : c.c;
+}
+
+#define GRID_STRIDE(k, n) \
+  for (long k = (long) blockIdx.x*blockDim.x + threadIdx.x; k < (n); k += (long) gridDim.x*blockDim.x)
+
+__global__ void k_set (const uint32_t * __restrict__ list, long n, TL T, double * s, double v)
+{
+  GRID_STRIDE (k, n) {
+    int l, i, j;
+    unpack (list[k], l, i, j);
+    s[gidx (T, l, i, j)] = v;
+  }
+}
+
+/* bilinear (multigrid-common.h:124-140) of child (i, j) of level l from
+   level l - 1 */
+__device__ __forceinline__ double bilinear (const TL & T, const double * s, int l, int i, int j)
+{
+  const int pi = i >> 1, pj = j >> 1, cx = (i & 1) ? 1 : -1, cy = (j & 1) ? 1 : -1;
+  const double * c = s + T.off[l - 1];
+  const bmg_geom & gc = T.g[l - 1];
+  return (9.*c[cidx<2> (gc, pi, pj, 0)] +
+          3.*(c[cidx<2> (gc, pi + cx, pj, 0)] + c[cidx<2> (gc, pi, pj + cy, 0)]) +
+          c[cidx<2> (gc, pi + cx, pj + cy, 0)])/16.;
+}
+
+/* foreach_level (l) s[] = bilinear (point, s) (poisson.h:64-68) */
+__global__ void k_prolong (const uint32_t * __restrict__ list, long n, TL T, double * s)
+{
+  GRID_STRIDE (k, n) {
+    int l, i, j;
+    unpack (list[k], l, i, j);
+    s[gidx (T, l, i, j)] = bilinear (T, s, l, i, j);
+  }
+}
+
+/* refine_bilinear of the halo children of prolongation leaves: one thread
+   per child */
+__global__ void k_halo (const uint32_t * __restrict__ list, long n, TL T, double * s)
+{
+  GRID_STRIDE (k, 4*n) {
+    int l, i, j;
+    unpack (list[k >> 2], l, i, j);
+    const int ci = 2*i + (int) ((k >> 1) & 1), cj = 2*j + (int) (k & 1);
+    s[gidx (T, l + 1, ci, cj)] = bilinear (T, s, l + 1, ci, cj);
+  }
+}
+
+/* restriction_average (multigrid-common.h:26-32), children in foreach_child
+   order */
+__global__ void k_restrict (const uint32_t * __restrict__ list, long n, TL T, double * s)
+{
+  GRID_STRIDE (k, n) {
+    int l, i, j;
+    unpack (list[k], l, i, j);
+    const double * f = s + T.off[l + 1];
+    const bmg_geom & gf = T.g[l + 1];
+    double sum = 0.;
+    sum += f[cidx<2> (gf, 2*i, 2*j, 0)];
+    sum += f[cidx<2> (gf, 2*i, 2*j + 1, 0)];
+    sum += f[cidx<2> (gf, 2*i + 1, 2*j, 0)];
+    sum += f[cidx<2> (gf, 2*i + 1, 2*j + 1, 0)];
+    s[gidx (T, l, i, j)] = sum/(1 << 2);
+  }
+}
+
+__device__ __forceinline__ bool refined_at (const TL & T, const unsigned char * fl, int l, int i, int j)
+{
+  const int n = T.g[l].n;
+  if (i < 0 || j < 0 || i >= n || j >= n) return false;
+  const unsigned char f = fl[gidx (T, l, i, j)];
+  return (f & BMG_T_ACTIVE) && !(f & BMG_T_LEAF);
+}
+
+/* face_average (multigrid-common.h:42-55) of the refined cells of one
+   level: each cell writes its left and bottom faces, and its right and top
+   faces unless the neighbour there is refined too (which writes the same
+   value as its own left/bottom face) */
+__global__ void k_restrict_faces (const uint32_t * __restrict__ list, long n, TL T,
+                                  const unsigned char * __restrict__ fl, double * ax, double * ay)
+{
+  GRID_STRIDE (k, n) {
+    int l, i, j;
+    unpack (list[k], l, i, j);
+    const bmg_geom & gf = T.g[l + 1];
+    const double * fx = ax + T.off[l + 1], * fy = ay + T.off[l + 1];
+    ax[gidx (T, l, i, j)] = (fx[cidx<2> (gf, 2*i, 2*j, 0)] + fx[cidx<2> (gf, 2*i, 2*j + 1, 0)])/2.;
+    if (!refined_at (T, fl, l, i + 1, j))
+      ax[gidx (T, l, i + 1, j)] = (fx[cidx<2> (gf, 2*i + 2, 2*j, 0)] +
+                                   fx[cidx<2> (gf, 2*i + 2, 2*j + 1, 0)])/2.;
+    ay[gidx (T, l, i, j)] = (fy[cidx<2> (gf, 2*i, 2*j, 0)] + fy[cidx<2> (gf, 2*i + 1, 2*j, 0)])/2.;
+    if (!refined_at (T, fl, l, i, j + 1))
+      ay[gidx (T, l, i, j + 1)] = (fy[cidx<2> (gf, 2*i, 2*j + 2, 0)] +
+                                   fy[cidx<2> (gf, 2*i + 1, 2*j + 2, 0)])/2.;
+  }
+}
+
+/* s.boundary[side](interior, ghost) of common.h:957-960 */
+__device__ __forceinline__ double bc_of (const bmg_tree_bc & bc, int side, int l, int tidx,
+                                         double sn, double Delta, int homog)
+{
+  const double * v = bc.val[side][l];
+  const double val = v ? v[tidx] : bc.cval[side];
+  if (bc.type[side] == BMG_DIRICHLET)
+    return homog ? - sn : 2.*val - sn;
+  return homog ? sn : Delta*val + sn;
+}
+
+__global__ void k_bc (const bmg_tree_rule * __restrict__ rules, long n, TL T, double * s,
+                      bmg_tree_bc bc, int homog)
+{
+  GRID_STRIDE (k, n) {
+    const bmg_tree_rule r = rules[k];
+    int l, gi, gj, l2, a, b;
+    unpack (r.ghost, l, gi, gj);
+    unpack (r.inner, l2, a, b);
+    const long long nid = gidx (T, l, a, b);
+    const double sn = s[nid], D = T.Delta[l];
+    const int s1 = r.kind_sides & 15, s2 = (r.kind_sides >> 4) & 15, kind = r.kind_sides >> 8;
+    const int t1 = r.tidx & 0xFFFF, t2 = r.tidx >> 16;
+    double v = bc_of (bc, s1, l, t1, sn, D, homog);
+    if (kind == BMG_T_DIAGONAL)
+      v = (v + bc_of (bc, s2, l, t2, sn, D, homog) - sn);
+    s[gidx (T, l, gi, gj)] = v;
+  }
+}
+
+/* relax (poisson.h:303-320); x is the first index (stride P), y the second */
+__global__ void k_relax (const uint32_t * __restrict__ list, long n, TL T,
+                         const double * a, const double * __restrict__ b,
+                         bmg_tree_coef ax, bmg_tree_coef ay, bmg_tree_coef lam, double * out)
+{
+  GRID_STRIDE (k, n) {
+    int l, i, j;
+    unpack (list[k], l, i, j);
+    const long long id = gidx (T, l, i, j), P = T.g[l].P;
+    const double Delta = T.Delta[l];
+    double nn = - (Delta*Delta)*b[id], d = - coef (lam, id)*(Delta*Delta);
+    const double x1 = coef (ax, id + P), x0 = coef (ax, id);
+    nn += x1*a[id + P] + x0*a[id - P];
+    d += x1 + x0;
+    const double y1 = coef (ay, id + 1), y0 = coef (ay, id);
+    nn += y1*a[id + 1] + y0*a[id - 1];
+    d += y1 + y0;
+    out[id] = nn/d;
+  }
+}
+
+/* weighted Jacobi (poisson.h:325-328) */
+__global__ void k_jacobi (const uint32_t * __restrict__ list, long n, TL T, double * a,
+                          const double * __restrict__ c)
+{
+  GRID_STRIDE (k, n) {
+    int l, i, j;
+    unpack (list[k], l, i, j);
+    const long long id = gidx (T, l, i, j);
+    a[id] = (a[id] + 2.*c[id])/3.;
+  }
+}
+
+/* g.x = alpha.x face_gradient_x (a, 0) on the left face of (i, j) */
+__device__ __forceinline__ double gx (const TL & T, const double * a, const bmg_tree_coef & ax,
+                                      int l, int i, int j)
+{
+  const long long id = gidx (T, l, i, j);
+  return coef (ax, id)*((a[id] - a[id - T.g[l].P])/T.Delta[l]);
+}
+
+__device__ __forceinline__ double gy (const TL & T, const double * a, const bmg_tree_coef & ay,
+                                      int l, int i, int j)
+{
+  const long long id = gidx (T, l, i, j);
+  return coef (ay, id)*((a[id] - a[id - 1])/T.Delta[l]);
+}
+
+/* atomicMax on the bits of a non-negative double (NaN sorts above inf) */
+__device__ __forceinline__ void max_bits (unsigned long long * m, double v)
+{
+  atomicMax (m, (unsigned long long) __double_as_longlong (v));
+}
+
+/* residual, tree branch (poisson.h:355-372): a leaf face shared with a
+   refined neighbour carries the mean of the two fine fluxes (halo_face) */
+__global__ void k_residual (const uint32_t * __restrict__ list, long n, TL T,
+                            const unsigned char * __restrict__ fl, const double * __restrict__ a,
+                            const double * __restrict__ b, bmg_tree_coef ax, bmg_tree_coef ay,
+                            bmg_tree_coef lam, double * res, unsigned long long * maxres)
+{
+  double m = 0.;
+  GRID_STRIDE (k, n) {
+    int l, i, j;
+    unpack (list[k], l, i, j);
+    const long long id = gidx (T, l, i, j);
+    const double Delta = T.Delta[l];
+    const double gl = refined_at (T, fl, l, i - 1, j) ?
+      (gx (T, a, ax, l + 1, 2*i, 2*j) + gx (T, a, ax, l + 1, 2*i, 2*j + 1))/2. : gx (T, a, ax, l, i, j);
+    const double gr = refined_at (T, fl, l, i + 1, j) ?
+      (gx (T, a, ax, l + 1, 2*i + 2, 2*j) + gx (T, a, ax, l + 1, 2*i + 2, 2*j + 1))/2. :
+      gx (T, a, ax, l, i + 1, j);
+    const double gb = refined_at (T, fl, l, i, j - 1) ?
+      (gy (T, a, ay, l + 1, 2*i, 2*j) + gy (T, a, ay, l + 1, 2*i + 1, 2*j))/2. : gy (T, a, ay, l, i, j);
+    const double gt = refined_at (T, fl, l, i, j + 1) ?
+      (gy (T, a, ay, l + 1, 2*i, 2*j + 2) + gy (T, a, ay, l + 1, 2*i + 1, 2*j + 2))/2. :
+      gy (T, a, ay, l, i, j + 1);
+    double r = b[id] - coef (lam, id)*a[id];
+    r -= (gr - gl)/Delta;
+    r -= (gt - gb)/Delta;
+    res[id] = r;
+    const double ar = fabs (r);
+    if (m == m && !(ar <= m)) m = ar;       /* a NaN sticks */
+  }
+  /* warp maximum, then one atomic per warp */
+  for (int o = 16; o > 0; o >>= 1) {
+    const double v = __shfl_down_sync (0xffffffffu, m, o);
+    if (m == m && !(v <= m)) m = v;
+  }
+  if ((threadIdx.x & 31) == 0 && m != 0.)
+    max_bits (maxres, m);
+}
+
+__global__ void k_add (const uint32_t * __restrict__ list, long n, TL T, double * a,
+                       const double * __restrict__ da)
+{
+  GRID_STRIDE (k, n) {
+    int l, i, j;
+    unpack (list[k], l, i, j);
+    const long long id = gidx (T, l, i, j);
+    a[id] += da[id];
+  }
+}
+
+/* two-stage deterministic sum: fixed grid, fixed reduction tree */
+__global__ void k_sum_partial (const uint32_t * __restrict__ list, long n, TL T,
+                               const double * __restrict__ s, double * partials)
+{
+  __shared__ double sh[256];
+  double v = 0.;
+  GRID_STRIDE (k, n) {
+    int l, i, j;
+    unpack (list[k], l, i, j);
+    v += s[gidx (T, l, i, j)];
+  }
+  sh[threadIdx.x] = v;
+  __syncthreads ();
+  for (int w = 128; w > 0; w >>= 1) {
+    if ((int) threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+    __syncthreads ();
+  }
+  if (threadIdx.x == 0) partials[blockIdx.x] = sh[0];
+}
+
+__global__ void k_sum_final (const double * __restrict__ partials, int np, double * out)
+{
+  __shared__ double sh[1024];
+  sh[threadIdx.x] = (int) threadIdx.x < np ? partials[threadIdx.x] : 0.;
+  __syncthreads ();
+  for (int w = 512; w > 0; w >>= 1) {
+    if ((int) threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+    __syncthreads ();
+  }
+  if (threadIdx.x == 0) *out = sh[0];
+}
+
+const int NT = 256;
+
+int blocks_for (long work)
+{
+  long b = (work + NT - 1)/NT;
+  if (b > 148*16) b = 148*16;
+  return b < 1 ? 1 : (int) b;
+}
+
+int status ()
+{
+  cudaError_t e = cudaGetLastError ();
+  return e == cudaSuccess ? 0 : (int) e;
+}
+
+} // namespace
+
+extern "C" {
+
+int bmg_tree_launch_set (const uint32_t * list, long n, const bmg_tree_levels * T,
+                         double * s, double v, cudaStream_t st)
+{
+  if (n <= 0) return 0;
+  k_set<<<blocks_for (n), NT, 0, st>>> (list, n, *T, s, v);
+  return status ();
+}
+
+int bmg_tree_launch_prolong (const uint32_t * list, long n, const bmg_tree_levels * T,
+                             double * s, cudaStream_t st)
+{
+  if (n <= 0) return 0;
+  k_prolong<<<blocks_for (n), NT, 0, st>>> (list, n, *T, s);
+  return status ();
+}
+
+int bmg_tree_launch_halo (const uint32_t * list, long n, const bmg_tree_levels * T,
+                          double * s, cudaStream_t st)
+{
+  if (n <= 0) return 0;
+  k_halo<<<blocks_for (4*n), NT, 0, st>>> (list, n, *T, s);
+  return status ();
+}
+
+int bmg_tree_launch_restrict (const uint32_t * list, long n, const bmg_tree_levels * T,
+                              double * s, cudaStream_t st)
+{
+  if (n <= 0) return 0;
+  k_restrict<<<blocks_for (n), NT, 0, st>>> (list, n, *T, s);
+  return status ();
+}
+
+int bmg_tree_launch_restrict_faces (const uint32_t * list, long n, const bmg_tree_levels * T,
+                                    const unsigned char * flags, double * ax, double * ay,
+                                    cudaStream_t st)
+{
+  if (n <= 0) return 0;
+  k_restrict_faces<<<blocks_for (n), NT, 0, st>>> (list, n, *T, flags, ax, ay);
+  return status ();
+}
+
+int bmg_tree_launch_bc (const bmg_tree_rule * rules, long n, const bmg_tree_levels * T,
+                        double * s, const bmg_tree_bc * bc, int homogeneous, cudaStream_t st)
+{
+  if (n <= 0) return 0;
+  k_bc<<<blocks_for (n), NT, 0, st>>> (rules, n, *T, s, *bc, homogeneous);
+  return status ();
+}
+
+int bmg_tree_launch_relax (const uint32_t * list, long n, const bmg_tree_levels * T,
+                           const double * a, const double * b, bmg_tree_coef ax,
+                           bmg_tree_coef ay, bmg_tree_coef lambda, double * out,
+                           cudaStream_t st)
+{
+  if (n <= 0) return 0;
+  k_relax<<<blocks_for (n), NT, 0, st>>> (list, n, *T, a, b, ax, ay, lambda, out);
+  return status ();
+}
+
+int bmg_tree_launch_jacobi (const uint32_t * list, long n, const bmg_tree_levels * T,
+                            double * a, const double * c, cudaStream_t st)
+{
+  if (n <= 0) return 0;
+  k_jacobi<<<blocks_for (n), NT, 0, st>>> (list, n, *T, a, c);
+  return status ();
+}
+
+int bmg_tree_launch_residual (const uint32_t * leaves, long n, const bmg_tree_levels * T,
+                              const unsigned char * flags, const double * a, const double * b,
+                              bmg_tree_coef ax, bmg_tree_coef ay, bmg_tree_coef lambda,
+                              double * res, unsigned long long * maxres, cudaStream_t st)
+{
+  if (n <= 0) return 0;
+  k_residual<<<blocks_for (n), NT, 0, st>>> (leaves, n, *T, flags, a, b, ax, ay, lambda, res, maxres);
+  return status ();
+}
+
+int bmg_tree_launch_add (const uint32_t * leaves, long n, const bmg_tree_levels * T,
+                         double * a, const double * da, cudaStream_t st)
+{
+  if (n <= 0) return 0;
+  k_add<<<blocks_for (n), NT, 0, st>>> (leaves, n, *T, a, da);
+  return status ();
+}
+
+int bmg_tree_launch_sum (const uint32_t * list, long n, const bmg_tree_levels * T,
+                         const double * s, double * partials, int npartials, double * out,
+                         cudaStream_t st)
+{
+  if (npartials < 1 || npartials > 1024) return (int) cudaErrorInvalidValue;
+  k_sum_partial<<<npartials, 256, 0, st>>> (list, n, *T, s, partials);
+  k_sum_final<<<1, 1024, 0, st>>> (partials, npartials, out);
+  return status ();
+}
+
+} // extern "C"

@@ -1,0 +1,97 @@
+/*
+ * mg_tree.h -- internal interface of the quadtree path: the host layer
+ * (mg_tree_host.c) and its CUDA kernels (mg_tree.cu).  Plain C types only.
+ *
+ * A tree lives on the dense levels of a grid (the level layout of
+ * mg_launch.h): every level l keeps its (2^l + 2)^2 padded array, and the
+ * tree is a set of per-cell flags plus cell lists.  A list entry packs one
+ * cell as level << 28 | (i + 1) << 14 | (j + 1), interior indices i (x) and
+ * j (y) from -1 (the ghost layer) to n.
+ */
+#ifndef MG_TREE_H
+#define MG_TREE_H
+
+#include <stdint.h>
+#include <cuda_runtime_api.h>
+#include "mg_launch.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BMG_TREE_MAXLEVEL 13
+
+/* cell flags (grid/tree.h:27-47, 398-399): ACTIVE and LEAF as in the
+   reference, HALO an allocated cell that is not active (a prolongation
+   cell), PROL a leaf whose children are halo cells (the prolongation cache,
+   grid/tree.h:646-648) */
+enum { BMG_T_ACTIVE = 1, BMG_T_LEAF = 2, BMG_T_HALO = 4, BMG_T_PROL = 8 };
+
+/* rule of one ghost cell of the box boundary (grid/tree.h:1139-1209):
+   NORMAL takes bc(side1) of the interior cell, DIAGONAL
+   bc(side1) + bc(side2) - s[interior] */
+enum { BMG_T_NORMAL = 1, BMG_T_DIAGONAL = 2 };
+typedef struct {
+  uint32_t ghost, inner;   /* packed cells, same level */
+  uint32_t kind_sides;     /* kind << 8 | side2 << 4 | side1 */
+  uint32_t tidx;           /* tidx2 << 16 | tidx1: tangential face index */
+} bmg_tree_rule;
+
+/* the levels of the grid as the tree kernels see them: an all-level field
+   buffer holds level l at element offset off[l] with geometry g[l] */
+typedef struct {
+  bmg_geom g[BMG_TREE_MAXLEVEL + 1];
+  long long off[BMG_TREE_MAXLEVEL + 1];
+  double Delta[BMG_TREE_MAXLEVEL + 1];
+} bmg_tree_levels;
+
+/* a coefficient over all levels: an all-level array, or a constant */
+typedef struct {
+  const double * p;
+  double c;
+} bmg_tree_coef;
+
+/* box conditions of one cell field, per level (NULL values: the constant) */
+typedef struct {
+  int type[4];
+  double cval[4];
+  const double * val[4][BMG_TREE_MAXLEVEL + 1];
+} bmg_tree_bc;
+
+int bmg_tree_launch_set (const uint32_t * list, long n, const bmg_tree_levels * T,
+                         double * s, double v, cudaStream_t st);
+int bmg_tree_launch_prolong (const uint32_t * list, long n, const bmg_tree_levels * T,
+                             double * s, cudaStream_t st);
+int bmg_tree_launch_halo (const uint32_t * list, long n, const bmg_tree_levels * T,
+                          double * s, cudaStream_t st);
+int bmg_tree_launch_restrict (const uint32_t * list, long n, const bmg_tree_levels * T,
+                              double * s, cudaStream_t st);
+int bmg_tree_launch_restrict_faces (const uint32_t * list, long n, const bmg_tree_levels * T,
+                                    const unsigned char * flags, double * ax, double * ay,
+                                    cudaStream_t st);
+int bmg_tree_launch_bc (const bmg_tree_rule * rules, long n, const bmg_tree_levels * T,
+                        double * s, const bmg_tree_bc * bc, int homogeneous, cudaStream_t st);
+/* out = n/d of relax (poisson.h:303-320) for the listed cells: out = a for
+   an in-place colour pass, the Jacobi temporary otherwise */
+int bmg_tree_launch_relax (const uint32_t * list, long n, const bmg_tree_levels * T,
+                           const double * a, const double * b, bmg_tree_coef ax,
+                           bmg_tree_coef ay, bmg_tree_coef lambda, double * out,
+                           cudaStream_t st);
+int bmg_tree_launch_jacobi (const uint32_t * list, long n, const bmg_tree_levels * T,
+                            double * a, const double * c, cudaStream_t st);
+int bmg_tree_launch_residual (const uint32_t * leaves, long n, const bmg_tree_levels * T,
+                              const unsigned char * flags, const double * a, const double * b,
+                              bmg_tree_coef ax, bmg_tree_coef ay, bmg_tree_coef lambda,
+                              double * res, unsigned long long * maxres, cudaStream_t st);
+int bmg_tree_launch_add (const uint32_t * leaves, long n, const bmg_tree_levels * T,
+                         double * a, const double * da, cudaStream_t st);
+/* deterministic sum over the listed cells: per-block partials, then one
+   block; npartials at most 1024 */
+int bmg_tree_launch_sum (const uint32_t * list, long n, const bmg_tree_levels * T,
+                         const double * s, double * partials, int npartials, double * out,
+                         cudaStream_t st);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,822 @@
+/*
+ * mg_tree_host.c -- host layer of the quadtree path (two dimensions).
+ *
+ * A grid becomes a quadtree with bmg_tree_refine (): the device counterpart
+ * of Basilisk's init_grid (1) + refine (cond) on grid/quadtree.h.  The tree
+ * keeps the grid's dense level arrays; it adds per-cell flags and the cell
+ * lists the tree kernels walk (mg_tree.h).  The control flow follows the
+ * reference's tree branch:
+ *   refine_cell with TWO_ONE, refine ()     grid/tree-common.h:22-55, 308-326
+ *   halo cells, caches                      grid/tree.h:556-684, 929-1041
+ *   tree_boundary_level                     grid/tree-common.h:588-716
+ *   box boundary on trees                   grid/tree.h:1139-1209, 1286-1367
+ *   mg_cycle / mg_solve / poisson           poisson.h:32-90, 139-235, 402-441
+ *   relax over foreach_level_or_leaf        poisson.h:271-338, grid/tree.h:735-740
+ *   residual, tree branch                   poisson.h:355-372
+ * Every operation on field data runs in mg_tree.cu; this file builds the
+ * tree, sequences launches (captured into CUDA graphs per solve key) and
+ * reads one residual maximum back per cycle.
+ *
+ * The red-black smoother relaxes the red cells of every level of the set,
+ * refreshes the tree boundary, then the black cells; the Jacobi smoother is
+ * the reference's JACOBI branch.  The tree path computes in FP64.
+ */
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <math.h>
+#include <stdint.h>
+#include <cuda_runtime_api.h>
+
+#include "mg_grid.h"
+#include "mg_tree.h"
+
+#define TMAX BMG_TREE_MAXLEVEL
+#define NTGRAPH 16
+
+typedef struct { long off, n; } span_t;
+
+/* everything a captured solve iteration depends on */
+typedef struct {
+  int nrelax, minlevel, maxlevel, relax;
+  const void * a, * b, * da, * res, * tmp;
+  bmg_tree_coef ax, ay, lam;
+  bmg_tree_bc abc;
+  cudaStream_t stream;
+  const void * maxres, * pinned;
+} tkey;
+
+struct tgraph {
+  int valid;
+  unsigned long long stamp;
+  tkey key;
+  cudaGraphExec_t exec;
+  long long launches;
+};
+
+struct bmg_tree {
+  int depth, hmax;
+  long long nleaves;
+  int full;
+  unsigned char * fl[TMAX + 1];       /* host flags, (n + 2)^2 with the ghost ring */
+  unsigned short * nb[TMAX + 1];      /* refined cells in the 3x3 neighbourhood */
+  unsigned char * dflags;             /* device flags, FP64 level layout */
+  uint32_t * dlist;
+  bmg_tree_rule * drules;
+  span_t act[TMAX + 1], ref[TMAX + 1], prol[TMAX + 1], rl[TMAX + 1], ghost[TMAX + 1], leaves;
+  long rl1[TMAX + 1];                 /* colour-1 part of rl[l] starts here */
+  bmg_tree_levels T;
+  double * dpart;
+  int npart;
+  struct tgraph graphs[NTGRAPH];
+  unsigned long long clock;
+};
+
+#define FAIL(s) bmg_i_fail (s)
+#define CKT(call) do { cudaError_t e_ = (call); if (e_ != cudaSuccess) { \
+      fprintf (stderr, "bmg: %s failed: %s (%s:%d)\n", #call,            \
+               cudaGetErrorString (e_), __FILE__, __LINE__);              \
+      return FAIL (e_ == cudaErrorMemoryAllocation ? BMG_ENOMEM : BMG_ECUDA); } } while (0)
+#define LT(call) do { int e_ = (call); if (e_) {                          \
+      fprintf (stderr, "bmg: launch %s failed: %s (%s:%d)\n", #call,      \
+               cudaGetErrorString ((cudaError_t) e_), __FILE__, __LINE__); \
+      return FAIL (BMG_ECUDA); } (*nl)++; } while (0)
+
+static inline size_t HX (int l, int i, int j) { return (size_t) (i + 1)*((1 << l) + 2) + (j + 1); }
+
+static inline uint32_t pack (int l, int i, int j)
+{
+  return ((uint32_t) l << 28) | ((uint32_t) (i + 1) << 14) | (uint32_t) (j + 1);
+}
+
+/* ------------------------------------------------------------------ */
+/* building the tree                                                   */
+/* ------------------------------------------------------------------ */
+
+static void tree_release (struct bmg_tree * t)
+{
+  if (!t) return;
+  for (int i = 0; i < NTGRAPH; i++)
+    if (t->graphs[i].valid) cudaGraphExecDestroy (t->graphs[i].exec);
+  for (int l = 0; l <= TMAX; l++) { free (t->fl[l]); free (t->nb[l]); }
+  cudaFree (t->dflags); cudaFree (t->dlist); cudaFree (t->drules); cudaFree (t->dpart);
+  free (t);
+}
+
+void bmg_tree_free (bmg_grid * g)
+{
+  if (!g || !g->tree) return;
+  tree_release (g->tree);
+  g->tree = NULL;
+}
+
+void bmg_tree_graphs_clear (bmg_grid * g)
+{
+  if (!g || !g->tree) return;
+  for (int i = 0; i < NTGRAPH; i++)
+    if (g->tree->graphs[i].valid) {
+      cudaGraphExecDestroy (g->tree->graphs[i].exec);
+      g->tree->graphs[i].valid = 0;
+    }
+}
+
+/* refine_cell (tree-common.h:22-55): the leaves among the parent's
+   neighbours on this child's side are refined first (TWO_ONE), then the
+   cell; its 3x3 neighbourhood counts it (increment_neighbors) */
+static int split (struct bmg_tree * t, int l, int i, int j)
+{
+  if (l + 1 > t->hmax) return BMG_EINVAL;
+  if (l > 0) {
+    const int pi = i >> 1, pj = j >> 1, np = 1 << (l - 1);
+    const int sx = (i & 1) ? 1 : -1, sy = (j & 1) ? 1 : -1;
+    const int side[3][2] = {{0, sy}, {sx, 0}, {sx, sy}};
+    for (int q = 0; q < 3; q++) {
+      const int ni = pi + side[q][0], nj = pj + side[q][1];
+      if (ni < 0 || nj < 0 || ni >= np || nj >= np) continue;
+      if (t->fl[l - 1][HX (l - 1, ni, nj)] & BMG_T_LEAF) {
+        int r = split (t, l - 1, ni, nj);
+        if (r) return r;
+      }
+    }
+  }
+  const int n = 1 << l;
+  for (int a = i - 1; a <= i + 1; a++)
+    for (int b = j - 1; b <= j + 1; b++)
+      if (a >= 0 && b >= 0 && a < n && b < n)
+        t->nb[l][HX (l, a, b)]++;
+  for (int c = 0; c < 4; c++)
+    t->fl[l + 1][HX (l + 1, 2*i + (c >> 1), 2*j + (c & 1))] |= BMG_T_ACTIVE | BMG_T_LEAF;
+  t->fl[l][HX (l, i, j)] &= ~BMG_T_LEAF;
+  if (l + 1 > t->depth) t->depth = l + 1;
+  return BMG_OK;
+}
+
+/* one foreach_leaf () pass of refine (): depth first, children in the
+   order (left,bottom), (left,top), (right,bottom), (right,top) */
+static int refine_pass (bmg_grid * g, struct bmg_tree * t, bmg_refine_cond cond, void * data,
+                        long * count)
+{
+  struct { int l, i, j; } stack[4*(TMAX + 2)];
+  int top = 0;
+  stack[top].l = 0; stack[top].i = 0; stack[top].j = 0; top++;
+  while (top > 0) {
+    top--;
+    const int l = stack[top].l, i = stack[top].i, j = stack[top].j;
+    const unsigned char f = t->fl[l][HX (l, i, j)];
+    if (!(f & BMG_T_ACTIVE)) continue;
+    if (f & BMG_T_LEAF) {
+      const double Delta = g->L0*(1./(1 << l));
+      const double x = (i + 0.5)*Delta + g->X0, y = (j + 0.5)*Delta + g->Y0;
+      if (cond (l, x, y, 0., data)) {
+        int r = split (t, l, i, j);
+        if (r) return r;
+        (*count)++;
+      }
+      continue;
+    }
+    for (int c = 3; c >= 0; c--) {          /* pushed in reverse: popped in order */
+      stack[top].l = l + 1; stack[top].i = 2*i + (c >> 1); stack[top].j = 2*j + (c & 1);
+      top++;
+    }
+  }
+  return BMG_OK;
+}
+
+static inline int interior_allocated (const struct bmg_tree * t, int l, int i, int j)
+{
+  const int n = 1 << l;
+  if (i < 0 || j < 0 || i >= n || j >= n) return 0;
+  return (t->fl[l][HX (l, i, j)] & (BMG_T_ACTIVE | BMG_T_HALO)) != 0;
+}
+
+static inline int ghost_at (int l, int i, int j)
+{
+  const int n = 1 << l;
+  if (i < -1 || j < -1 || i > n || j > n) return 0;
+  return i == -1 || j == -1 || i == n || j == n;
+}
+
+/* boundary id of a ghost: init_grid's pids give corners their x side
+   (tree.h:1530-1542) */
+static inline int ghost_side (int l, int i, int j)
+{
+  const int n = 1 << l;
+  if (i < 0) return BMG_LEFT;
+  if (i >= n) return BMG_RIGHT;
+  if (j >= n) return BMG_TOP;
+  return BMG_BOTTOM;
+}
+
+static inline int tangential (int side, int i, int j)
+{
+  return (side == BMG_LEFT || side == BMG_RIGHT) ? j : i;
+}
+
+/* the rule of ghost (gi, gj): normal_neighbor, else diagonal_neighbor_2D
+   (tree.h:1139-1209); 0 when the ghost touches no allocated cell */
+static int ghost_rule (const struct bmg_tree * t, int l, int gi, int gj, bmg_tree_rule * r)
+{
+  static const int nrm[4][2] = {{-1, 0}, {1, 0}, {0, -1}, {0, 1}};
+  for (int q = 0; q < 4; q++) {
+    const int a = gi + nrm[q][0], b = gj + nrm[q][1];
+    if (interior_allocated (t, l, a, b)) {
+      const int s = ghost_side (l, gi, gj);
+      r->ghost = pack (l, gi, gj); r->inner = pack (l, a, b);
+      r->kind_sides = (BMG_T_NORMAL << 8) | s;
+      r->tidx = (uint32_t) tangential (s, a, b);
+      return 1;
+    }
+  }
+  for (int di = -1; di <= 1; di += 2)
+    for (int dj = -1; dj <= 1; dj += 2) {
+      const int a = gi + di, b = gj + dj;
+      if (interior_allocated (t, l, a, b) && ghost_at (l, a, gj) && ghost_at (l, gi, b)) {
+        const int s1 = ghost_side (l, a, gj), s2 = ghost_side (l, gi, b);
+        r->ghost = pack (l, gi, gj); r->inner = pack (l, a, b);
+        r->kind_sides = (BMG_T_DIAGONAL << 8) | (s2 << 4) | s1;
+        r->tidx = ((uint32_t) tangential (s2, a, b) << 16) | (uint32_t) tangential (s1, a, b);
+        return 1;
+      }
+    }
+  return 0;
+}
+
+/* flags of halo cells and prolongation leaves, cell lists, ghost rules:
+   the caches of update_cache_f (tree.h:556-684), uploaded */
+static int derive (bmg_grid * g, struct bmg_tree * t)
+{
+  const int D = t->depth;
+  long nact[TMAX + 1] = {0}, nref[TMAX + 1] = {0}, nprol[TMAX + 1] = {0}, nleaf[TMAX + 1] = {0};
+  long long leaves = 0;
+  for (int l = 0; l <= t->hmax; l++) {
+    const size_t m = (size_t) ((1 << l) + 2)*((1 << l) + 2);
+    for (size_t k = 0; k < m; k++) t->fl[l][k] &= ~(BMG_T_HALO | BMG_T_PROL);
+  }
+  for (int l = 0; l <= D; l++) {
+    const int n = 1 << l;
+    for (int i = 0; i < n; i++)
+      for (int j = 0; j < n; j++) {
+        unsigned char * f = &t->fl[l][HX (l, i, j)];
+        if (!(*f & BMG_T_ACTIVE)) continue;
+        nact[l]++;
+        if (!(*f & BMG_T_LEAF)) { nref[l]++; continue; }
+        nleaf[l]++; leaves++;
+        if (t->nb[l][HX (l, i, j)] > 0) {
+          *f |= BMG_T_PROL;
+          nprol[l]++;
+          for (int c = 0; c < 4; c++)
+            t->fl[l + 1][HX (l + 1, 2*i + (c >> 1), 2*j + (c & 1))] |= BMG_T_HALO;
+        }
+      }
+  }
+  t->nleaves = leaves;
+  t->full = leaves == (1LL << (2*D));
+
+  /* list layout: act, ref, prol per level, leaves, relax sets per level */
+  long total = 0;
+  for (int l = 0; l <= D; l++) {
+    t->act[l].off = total; t->act[l].n = nact[l]; total += nact[l];
+    t->ref[l].off = total; t->ref[l].n = nref[l]; total += nref[l];
+    t->prol[l].off = total; t->prol[l].n = nprol[l]; total += nprol[l];
+  }
+  t->leaves.off = total; t->leaves.n = leaves; total += leaves;
+  long below = 0;                      /* leaves of the levels under l */
+  for (int l = 0; l <= D; l++) {
+    t->rl[l].off = total; t->rl[l].n = nact[l] + below; total += t->rl[l].n;
+    below += nleaf[l];
+  }
+  uint32_t * h = malloc ((total + 1)*sizeof (uint32_t));
+  if (!h) return FAIL (BMG_ENOMEM);
+  long pa[TMAX + 1], pr[TMAX + 1], pp[TMAX + 1], pl = t->leaves.off;
+  for (int l = 0; l <= D; l++) { pa[l] = t->act[l].off; pr[l] = t->ref[l].off; pp[l] = t->prol[l].off; }
+  for (int l = 0; l <= D; l++) {
+    const int n = 1 << l;
+    for (int i = 0; i < n; i++)
+      for (int j = 0; j < n; j++) {
+        const unsigned char f = t->fl[l][HX (l, i, j)];
+        if (!(f & BMG_T_ACTIVE)) continue;
+        const uint32_t e = pack (l, i, j);
+        h[pa[l]++] = e;
+        if (!(f & BMG_T_LEAF)) h[pr[l]++] = e;
+        else {
+          h[pl++] = e;
+          if (f & BMG_T_PROL) h[pp[l]++] = e;
+        }
+      }
+  }
+  /* relax set of level l (foreach_level_or_leaf): its active cells and the
+     leaves below, red first */
+  for (int l = 0; l <= D; l++) {
+    long w = t->rl[l].off;
+    for (int c = 0; c < 2; c++) {
+      if (c == 1) t->rl1[l] = w - t->rl[l].off;
+      for (int m = l; m >= 0; m--) {
+        const int n = 1 << m;
+        for (int i = 0; i < n; i++)
+          for (int j = 0; j < n; j++) {
+            const unsigned char f = t->fl[m][HX (m, i, j)];
+            if (!(f & BMG_T_ACTIVE) || (m < l && !(f & BMG_T_LEAF)) || ((i + j) & 1) != c) continue;
+            h[w++] = pack (m, i, j);
+          }
+      }
+    }
+  }
+  /* ghost rules */
+  long nrules = 0;
+  for (int l = 0; l <= D; l++) nrules += 4L*(1 << l) + 4;
+  bmg_tree_rule * hr = malloc ((nrules + 1)*sizeof (bmg_tree_rule));
+  if (!hr) { free (h); return FAIL (BMG_ENOMEM); }
+  long k = 0;
+  for (int l = 0; l <= D; l++) {
+    const int n = 1 << l;
+    t->ghost[l].off = k;
+    for (int gi = -1; gi <= n; gi++)
+      for (int gj = -1; gj <= n; gj++) {
+        if (!ghost_at (l, gi, gj)) continue;
+        if (ghost_rule (t, l, gi, gj, &hr[k])) k++;
+      }
+    t->ghost[l].n = k - t->ghost[l].off;
+  }
+  /* device flags in the FP64 level layout */
+  const size_t nfl = g->off64[g->depth + 1];
+  unsigned char * hf = calloc (nfl, 1);
+  if (!hf) { free (h); free (hr); return FAIL (BMG_ENOMEM); }
+  for (int l = 0; l <= D; l++) {
+    const int n = 1 << l;
+    const bmg_geom * gg = &g->g64[l];
+    for (int i = -1; i <= n; i++)
+      for (int j = -1; j <= n; j++)
+        hf[g->off64[l] + (size_t) (i + 1)*gg->P + gg->xo + j] = t->fl[l][HX (l, i, j)];
+  }
+  cudaFree (t->dflags); cudaFree (t->dlist); cudaFree (t->drules);
+  t->dflags = NULL; t->dlist = NULL; t->drules = NULL;
+  int st = BMG_OK;
+  if (cudaMalloc ((void **) &t->dflags, nfl) != cudaSuccess ||
+      cudaMalloc ((void **) &t->dlist, (total + 1)*sizeof (uint32_t)) != cudaSuccess ||
+      cudaMalloc ((void **) &t->drules, (k + 1)*sizeof (bmg_tree_rule)) != cudaSuccess ||
+      cudaMemcpy (t->dflags, hf, nfl, cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy (t->dlist, h, total*sizeof (uint32_t), cudaMemcpyHostToDevice) != cudaSuccess ||
+      (k && cudaMemcpy (t->drules, hr, k*sizeof (bmg_tree_rule), cudaMemcpyHostToDevice) != cudaSuccess))
+    st = BMG_ENOMEM;
+  free (h); free (hr); free (hf);
+  if (st) return FAIL (st);
+  memset (&t->T, 0, sizeof t->T);
+  for (int l = 0; l <= g->depth && l <= TMAX; l++) {
+    t->T.g[l] = g->g64[l];
+    t->T.off[l] = (long long) g->off64[l];
+    t->T.Delta[l] = g->L0*(1./(1 << l));
+  }
+  if (!t->dpart) {
+    t->npart = 256;
+    CKT (cudaMalloc ((void **) &t->dpart, (t->npart + 1)*sizeof (double)));
+  }
+  return BMG_OK;
+}
+
+int bmg_tree_refine (bmg_grid * g, bmg_refine_cond cond, void * data)
+{
+  if (!g || !cond || g->dim != 2 || g->depth > TMAX || g->periodic[0] || g->periodic[1])
+    return FAIL (BMG_EINVAL);
+  CKT (cudaSetDevice (g->device));
+  struct bmg_tree * t = g->tree;
+  if (!t) {
+    t = calloc (1, sizeof (struct bmg_tree));
+    if (!t) return FAIL (BMG_ENOMEM);
+    t->hmax = g->depth;
+    for (int l = 0; l <= t->hmax; l++) {
+      const size_t m = (size_t) ((1 << l) + 2)*((1 << l) + 2);
+      t->fl[l] = calloc (m, 1);
+      t->nb[l] = calloc (m, sizeof (unsigned short));
+      if (!t->fl[l] || !t->nb[l]) { tree_release (t); return FAIL (BMG_ENOMEM); }
+    }
+    t->fl[0][HX (0, 0, 0)] = BMG_T_ACTIVE | BMG_T_LEAF;     /* init_grid (1) */
+    g->tree = t;
+  }
+  long count = 0, pass;
+  int r;
+  do {
+    pass = 0;
+    r = refine_pass (g, t, cond, data, &pass);
+    count += pass;
+  } while (!r && pass);
+  if (r) { bmg_tree_free (g); return FAIL (r); }
+  bmg_tree_graphs_clear (g);
+  r = derive (g, t);
+  if (r) { bmg_tree_free (g); return r; }
+  FAIL (BMG_OK);
+  return (int) (count > 0x7fffffff ? 0x7fffffff : count);
+}
+
+int bmg_tree_info (const bmg_grid * g, int * depth, long long * leaves)
+{
+  if (!g || !g->tree) return FAIL (BMG_EINVAL);
+  if (depth) *depth = g->tree->depth;
+  if (leaves) *leaves = g->tree->nleaves;
+  return FAIL (BMG_OK);
+}
+
+int bmg_tree_flags (const bmg_grid * g, int level, unsigned char * out)
+{
+  if (!g || !g->tree || !out || level < 0 || level > g->tree->hmax) return FAIL (BMG_EINVAL);
+  const int n = 1 << level;
+  for (int i = 0; i < n; i++)
+    for (int j = 0; j < n; j++)
+      out[(size_t) i*n + j] = g->tree->fl[level][HX (level, i, j)];
+  return FAIL (BMG_OK);
+}
+
+/* ------------------------------------------------------------------ */
+/* launch sequences                                                    */
+/* ------------------------------------------------------------------ */
+
+static bmg_tree_coef coef_of_field (bmg_grid * g, int handle, int want_face, double dflt, int * ok)
+{
+  bmg_tree_coef c = {NULL, dflt};
+  if (!handle) return c;
+  field_t * f = bmg_i_field (g, handle);
+  if (!f || f->face_dim != want_face) { *ok = 0; return c; }
+  if (f->is_const) c.c = f->cval;
+  else c.p = f->buf;
+  return c;
+}
+
+typedef struct { bmg_tree_coef ax, ay, lam; int ax_h, lam_h; } tcoefs;
+
+static int resolve (bmg_grid * g, const struct Poisson * p, tcoefs * c)
+{
+  int ok = 1;
+  memset (c, 0, sizeof *c);
+  c->ax_h = p->alpha.x.i;
+  c->lam_h = p->lambda.i;
+  c->ax = coef_of_field (g, p->alpha.x.i, 0, 1., &ok);      /* unityf */
+  c->ay = coef_of_field (g, p->alpha.x.i ? p->alpha.y.i : 0, 1, 1., &ok);
+  c->lam = coef_of_field (g, p->lambda.i, -1, 0., &ok);     /* zeroc */
+  return ok ? BMG_OK : FAIL (BMG_EINVAL);
+}
+
+/* the box conditions of field f on every level of the tree */
+static void bc_of_field (const bmg_grid * g, const field_t * f, bmg_tree_bc * bc)
+{
+  memset (bc, 0, sizeof *bc);
+  for (int s = 0; s < 4; s++) {
+    bc->type[s] = f->bctype[s];
+    bc->cval[s] = f->bccval[s];
+    for (int l = 0; l <= g->depth && l <= TMAX; l++)
+      bc->val[s][l] = f->bclv[s][l] ? f->bclv[s][l] : (l == g->depth ? f->bcval[s] : NULL);
+  }
+}
+
+#define LIST(sp) (t->dlist + (sp).off), (sp).n
+
+static int t_bc (bmg_grid * g, struct bmg_tree * t, double * s, int l, const bmg_tree_bc * bc,
+                 int homog, long long * nl)
+{
+  if (t->ghost[l].n)
+    LT (bmg_tree_launch_bc (t->drules + t->ghost[l].off, t->ghost[l].n, &t->T, s, bc, homog, g->stream));
+  return BMG_OK;
+}
+
+/* tree_boundary_level (tree-common.h:588-716) of a cell field up to level l */
+static int t_boundary (bmg_grid * g, struct bmg_tree * t, double * s, int l, const bmg_tree_bc * bc,
+                       int homog, long long * nl)
+{
+  if (t->full) return t_bc (g, t, s, l, bc, homog, nl);
+  for (int m = l - 1; m >= 0; m--)
+    if (t->ref[m].n) LT (bmg_tree_launch_restrict (LIST (t->ref[m]), &t->T, s, g->stream));
+  int r = t_bc (g, t, s, 0, bc, homog, nl);
+  if (r) return r;
+  for (int i = 0; i < l; i++) {
+    if (t->prol[i].n) LT (bmg_tree_launch_halo (LIST (t->prol[i]), &t->T, s, g->stream));
+    r = t_bc (g, t, s, i + 1, bc, homog, nl);
+    if (r) return r;
+  }
+  return BMG_OK;
+}
+
+/* relax (poisson.h:271-338) of foreach_level_or_leaf (l) */
+static int t_relax (bmg_grid * g, struct bmg_tree * t, double * da, const double * res, double * tmp,
+                    const tcoefs * c, int l, const bmg_tree_bc * dabc, long long * nl)
+{
+  const span_t all = t->rl[l];
+  if (g->relax == BMG_RELAX_JACOBI) {
+    LT (bmg_tree_launch_relax (LIST (all), &t->T, da, res, c->ax, c->ay, c->lam, tmp, g->stream));
+    LT (bmg_tree_launch_jacobi (LIST (all), &t->T, da, tmp, g->stream));
+    return BMG_OK;
+  }
+  const span_t red = {all.off, t->rl1[l]}, black = {all.off + t->rl1[l], all.n - t->rl1[l]};
+  if (red.n) LT (bmg_tree_launch_relax (LIST (red), &t->T, da, res, c->ax, c->ay, c->lam, da, g->stream));
+  int r = t_boundary (g, t, da, l, dabc, 1, nl);
+  if (r) return r;
+  if (black.n) LT (bmg_tree_launch_relax (LIST (black), &t->T, da, res, c->ax, c->ay, c->lam, da, g->stream));
+  return BMG_OK;
+}
+
+/* mg_cycle (poisson.h:32-90) on the tree */
+static int t_cycle (bmg_grid * g, struct bmg_tree * t, double * a, double * da, double * res,
+                    double * tmp, const tcoefs * c, const bmg_tree_bc * dabc, int nrelax,
+                    int minlevel, int maxlevel, long long * nl)
+{
+  /* restriction (res): the restriction part of tree_restriction */
+  for (int m = t->depth - 1; m >= 0; m--)
+    if (t->ref[m].n) LT (bmg_tree_launch_restrict (LIST (t->ref[m]), &t->T, res, g->stream));
+  for (int l = minlevel; l <= maxlevel; l++) {
+    if (l == minlevel)
+      LT (bmg_tree_launch_set (LIST (t->rl[l]), &t->T, da, 0., g->stream));
+    else
+      LT (bmg_tree_launch_prolong (LIST (t->act[l]), &t->T, da, g->stream));
+    int r = t_boundary (g, t, da, l, dabc, 1, nl);
+    if (r) return r;
+    for (int i = 0; i < nrelax; i++) {
+      r = t_relax (g, t, da, res, tmp, c, l, dabc, nl);
+      if (r) return r;
+      r = t_boundary (g, t, da, l, dabc, 1, nl);
+      if (r) return r;
+    }
+  }
+  LT (bmg_tree_launch_add (LIST (t->leaves), &t->T, a, da, g->stream));
+  return BMG_OK;
+}
+
+/* residual (poisson.h:355-372) into res, maximum into g->d_maxres */
+static int t_residual (bmg_grid * g, struct bmg_tree * t, double * a, const double * b, double * res,
+                       const tcoefs * c, const bmg_tree_bc * abc, long long * nl)
+{
+  int r = t_boundary (g, t, a, t->depth, abc, 0, nl);
+  if (r) return r;
+  CKT (cudaMemsetAsync (g->d_maxres, 0, sizeof (unsigned long long), g->stream));
+  LT (bmg_tree_launch_residual (LIST (t->leaves), &t->T, t->dflags, a, b, c->ax, c->ay, c->lam,
+                                res, g->d_maxres, g->stream));
+  return BMG_OK;
+}
+
+static int read_max (bmg_grid * g, double * m)
+{
+  CKT (cudaMemcpyAsync (g->h_pinned, g->d_maxres, sizeof (double), cudaMemcpyDeviceToHost, g->stream));
+  CKT (cudaStreamSynchronize (g->stream));
+  *m = g->h_pinned[0];
+  return BMG_OK;
+}
+
+/* one mg_solve iteration (cycle, residual, maximum to pinned memory),
+   captured once per key and replayed */
+static int t_iteration (bmg_grid * g, struct bmg_tree * t, const tkey * key, double * a,
+                        const double * b, double * da, double * res, double * tmp, const tcoefs * c,
+                        const bmg_tree_bc * abc)
+{
+  long long launches = 0, * nl = &launches;
+  if (!g->use_graphs) {
+    int r = t_cycle (g, t, a, da, res, tmp, c, abc, key->nrelax, key->minlevel, key->maxlevel, nl);
+    if (!r) r = t_residual (g, t, a, b, res, c, abc, nl);
+    if (r) return r;
+    CKT (cudaMemcpyAsync (g->h_pinned, g->d_maxres, sizeof (double), cudaMemcpyDeviceToHost, g->stream));
+    g->counters.launches += launches;
+    return BMG_OK;
+  }
+  struct tgraph * e = NULL, * victim = &t->graphs[0];
+  for (int i = 0; i < NTGRAPH; i++) {
+    struct tgraph * q = &t->graphs[i];
+    if (q->valid && !memcmp (&q->key, key, sizeof *key)) { e = q; break; }
+    if (!q->valid || q->stamp < victim->stamp) victim = q;
+  }
+  if (!e) {
+    if (victim->valid) { cudaGraphExecDestroy (victim->exec); victim->valid = 0; }
+    cudaGraph_t graph;
+    CKT (cudaStreamBeginCapture (g->stream, cudaStreamCaptureModeThreadLocal));
+    int r = t_cycle (g, t, a, da, res, tmp, c, abc, key->nrelax, key->minlevel, key->maxlevel, nl);
+    if (!r) r = t_residual (g, t, a, b, res, c, abc, nl);
+    cudaError_t me = cudaMemcpyAsync (g->h_pinned, g->d_maxres, sizeof (double),
+                                      cudaMemcpyDeviceToHost, g->stream);
+    cudaError_t ee = cudaStreamEndCapture (g->stream, &graph);
+    if (r) { if (ee == cudaSuccess) cudaGraphDestroy (graph); return r; }
+    CKT (me);
+    CKT (ee);
+    cudaError_t ie = cudaGraphInstantiate (&victim->exec, graph, 0);
+    cudaGraphDestroy (graph);
+    CKT (ie);
+    victim->key = *key;
+    victim->launches = launches;
+    victim->valid = 1;
+    e = victim;
+  }
+  e->stamp = ++t->clock;
+  CKT (cudaGraphLaunch (e->exec, g->stream));
+  g->counters.launches += e->launches;
+  return BMG_OK;
+}
+
+/* mg_solve (poisson.h:139-235) on the tree, Poisson callbacks */
+static int t_solve (bmg_grid * g, field_t * a, field_t * b, const tcoefs * c, int nrelax,
+                    field_t * resout, int minlevel, double tolerance, mgstats * out)
+{
+  struct bmg_tree * t = g->tree;
+  if (g->precision != BMG_FP64) return FAIL (BMG_EUNSUPPORTED);
+  int r = bmg_i_workspace (g);
+  if (r) return r;
+  if (minlevel > t->depth) minlevel = t->depth;
+  if (minlevel < 0) minlevel = 0;
+  double * da = bmg_i_ws64 (g, BMG_WS_DA, 0), * tmp = bmg_i_ws64 (g, BMG_WS_DA2, 0);
+  double * res = bmg_i_ws64 (g, BMG_WS_RES, 0);
+  bmg_tree_bc abc;
+  bc_of_field (g, a, &abc);
+  mgstats s;
+  memset (&s, 0, sizeof s);
+  long long launches = 0, * nl = &launches;
+  /* sum of the r.h.s. over the leaves (poisson.h:162-167) */
+  LT (bmg_tree_launch_sum (LIST (t->leaves), &t->T, b->buf, t->dpart, t->npart, g->d_sum, g->stream));
+  CKT (cudaMemcpyAsync (g->h_pinned + 1, g->d_sum, sizeof (double), cudaMemcpyDeviceToHost, g->stream));
+  CKT (cudaStreamSynchronize (g->stream));
+  s.sum = g->h_pinned[1];
+  s.nrelax = nrelax > 0 ? nrelax : 4;
+  r = t_residual (g, t, a->buf, b->buf, res, c, &abc, nl);
+  if (r) return r;
+  r = read_max (g, &s.resb);
+  if (r) return r;
+  g->counters.launches += launches;
+  double resb = s.resa = s.resb;
+  if (tolerance == 0.)
+    tolerance = TOLERANCE;
+  tkey key;
+  memset (&key, 0, sizeof key);
+  key.minlevel = minlevel; key.maxlevel = t->depth; key.relax = g->relax;
+  key.a = a->buf; key.b = b->buf; key.da = da; key.res = res; key.tmp = tmp;
+  key.ax = c->ax; key.ay = c->ay; key.lam = c->lam; key.abc = abc;
+  key.stream = g->stream; key.maxres = g->d_maxres; key.pinned = g->h_pinned;
+  int status = BMG_OK;
+  for (s.i = 0; s.i < NITERMAX && (s.i < NITERMIN || s.resa > tolerance); s.i++) {
+    key.nrelax = s.nrelax;
+    if (g->timing) CKT (cudaEventRecord (g->ev0, g->stream));
+    r = t_iteration (g, t, &key, a->buf, b->buf, da, res, tmp, c, &abc);
+    if (r) return r;
+    if (g->timing) CKT (cudaEventRecord (g->ev1, g->stream));
+    CKT (cudaStreamSynchronize (g->stream));
+    s.resa = g->h_pinned[0];
+    g->counters.cycles++;
+    if (g->timing) {
+      float ms = 0.f;
+      CKT (cudaEventElapsedTime (&ms, g->ev0, g->ev1));
+      g->counters.cycle_ms += ms;
+    }
+    if (!isfinite (s.resa)) { status = BMG_ENAN; s.i++; break; }
+    if (s.resa > tolerance) {
+      if (resb/s.resa < 1.2 && s.nrelax < 100)
+        s.nrelax++;
+      else if (resb/s.resa > 10 && s.nrelax > 2)
+        s.nrelax--;
+    }
+    resb = s.resa;
+  }
+  s.minlevel = minlevel;
+  if (s.resa > tolerance) {
+    fprintf (stderr,
+             "WARNING: convergence for %s not reached after %d iterations\n"
+             "  res: %g sum: %g nrelax: %d\n", "a",
+             s.i, s.resa, s.sum, s.nrelax), fflush (stderr);
+    if (status == BMG_OK) status = BMG_ENOTCONV;
+  }
+  if (resout && !resout->is_const && resout->face_dim < 0)
+    CKT (cudaMemcpyAsync (resout->buf, res, g->off64[g->depth + 1]*sizeof (double),
+                          cudaMemcpyDeviceToDevice, g->stream));
+  CKT (cudaStreamSynchronize (g->stream));
+  *out = s;
+  return FAIL (status);
+}
+
+/* restriction ({alpha, lambda}) on the tree (poisson.h:418-420) */
+static int t_restrict_coefs (bmg_grid * g, struct bmg_tree * t, const tcoefs * c)
+{
+  long long n0 = 0, * nl = &n0;
+  for (int m = t->depth - 1; m >= 0; m--) {
+    if (c->ax.p && c->ay.p && t->ref[m].n)
+      LT (bmg_tree_launch_restrict_faces (LIST (t->ref[m]), &t->T, t->dflags,
+                                          (double *) c->ax.p, (double *) c->ay.p, g->stream));
+    if (c->lam.p && t->ref[m].n)
+      LT (bmg_tree_launch_restrict (LIST (t->ref[m]), &t->T, (double *) c->lam.p, g->stream));
+  }
+  return BMG_OK;
+}
+
+static int cell_field (bmg_grid * g, int h, field_t ** f)
+{
+  *f = bmg_i_field (g, h);
+  if (!*f || (*f)->is_const || (*f)->face_dim >= 0) return FAIL (BMG_EINVAL);
+  return BMG_OK;
+}
+
+int bmg_tree_poisson (bmg_grid * g, struct Poisson p, mgstats * out)
+{
+  field_t * a, * b, * res = NULL;
+  if (cell_field (g, p.a.i, &a) || cell_field (g, p.b.i, &b)) return FAIL (BMG_EINVAL);
+  if (p.res && p.res[0].i && cell_field (g, p.res[0].i, &res)) return FAIL (BMG_EINVAL);
+  tcoefs c;
+  int r = resolve (g, &p, &c);
+  if (r) return r;
+  r = t_restrict_coefs (g, g->tree, &c);
+  if (r) return r;
+  const double defaultol = TOLERANCE;
+  if (p.tolerance)
+    TOLERANCE = p.tolerance;
+  r = t_solve (g, a, b, &c, p.nrelax, res, p.minlevel > 1 ? p.minlevel : 1, 0., out);
+  if (p.tolerance)
+    TOLERANCE = defaultol;
+  return FAIL (r);
+}
+
+int bmg_tree_mg_solve (bmg_grid * g, struct MGSolve p, mgstats * out)
+{
+  field_t * a, * b, * res = NULL;
+  if (cell_field (g, p.a[0].i, &a) || cell_field (g, p.b[0].i, &b)) return FAIL (BMG_EINVAL);
+  if (p.res && p.res[0].i && cell_field (g, p.res[0].i, &res)) return FAIL (BMG_EINVAL);
+  tcoefs c;
+  int r = resolve (g, (struct Poisson *) p.data, &c);
+  if (r) return r;
+  return t_solve (g, a, b, &c, p.nrelax, res, p.minlevel, p.tolerance, out);
+}
+
+int bmg_tree_mg_cycle (bmg_grid * g, field_t * a, field_t * res, field_t * da,
+                       struct Poisson * p, int nrelax, int minlevel, int maxlevel)
+{
+  struct bmg_tree * t = g->tree;
+  tcoefs c;
+  int r = resolve (g, p, &c);
+  if (r) return r;
+  r = bmg_i_workspace (g);
+  if (r) return r;
+  if (maxlevel > t->depth) maxlevel = t->depth;
+  minlevel = minlevel < maxlevel ? minlevel : maxlevel;      /* poisson.h:48 */
+  if (minlevel < 0) minlevel = 0;
+  bmg_tree_bc dabc;
+  bc_of_field (g, da, &dabc);
+  long long launches = 0;
+  r = t_cycle (g, t, a->buf, da->buf, res->buf, bmg_i_ws64 (g, BMG_WS_DA2, 0), &c, &dabc,
+               nrelax, minlevel, maxlevel, &launches);
+  if (r) return r;
+  CKT (cudaStreamSynchronize (g->stream));
+  g->counters.launches += launches;
+  g->counters.cycles++;
+  return FAIL (BMG_OK);
+}
+
+int bmg_tree_relax (bmg_grid * g, field_t * da, field_t * res, int level, struct Poisson * p)
+{
+  struct bmg_tree * t = g->tree;
+  if (level > t->depth) return FAIL (BMG_EINVAL);
+  tcoefs c;
+  int r = resolve (g, p, &c);
+  if (r) return r;
+  r = bmg_i_workspace (g);
+  if (r) return r;
+  bmg_tree_bc dabc;
+  bc_of_field (g, da, &dabc);
+  long long launches = 0;
+  r = t_relax (g, t, da->buf, res->buf, bmg_i_ws64 (g, BMG_WS_DA2, 0), &c, level, &dabc, &launches);
+  if (r) return r;
+  CKT (cudaStreamSynchronize (g->stream));
+  return FAIL (BMG_OK);
+}
+
+int bmg_tree_residual (bmg_grid * g, field_t * a, field_t * b, field_t * res,
+                       struct Poisson * p, double * maxres)
+{
+  tcoefs c;
+  int r = resolve (g, p, &c);
+  if (r) return r;
+  bmg_tree_bc abc;
+  bc_of_field (g, a, &abc);
+  long long launches = 0;
+  r = t_residual (g, g->tree, a->buf, b->buf, res->buf, &c, &abc, &launches);
+  if (r) return r;
+  r = read_max (g, maxres);
+  if (r) return r;
+  return FAIL (BMG_OK);
+}
+
+/* restriction (list) on a tree (tree_restriction = boundary (list),
+   tree-common.h:795-799): face vectors by face_average, cell fields by the
+   whole tree boundary with their own conditions */
+int bmg_tree_restriction (bmg_grid * g, const bmg_scalar * list)
+{
+  struct bmg_tree * t = g->tree;
+  long long launches = 0, * nl = &launches;
+  for (const bmg_scalar * s = list; s->i; s++) {
+    field_t * f = bmg_i_field (g, s->i);
+    if (!f) return FAIL (BMG_EINVAL);
+    if (f->is_const) continue;
+    if (f->face_dim >= 0) {
+      if (f->face_dim != 0) continue;
+      field_t * fy = bmg_i_field (g, s->i + 1);
+      if (!fy || fy->face_dim != 1) return FAIL (BMG_EINVAL);
+      for (int m = t->depth - 1; m >= 0; m--)
+        if (t->ref[m].n)
+          LT (bmg_tree_launch_restrict_faces (LIST (t->ref[m]), &t->T, t->dflags, f->buf, fy->buf,
+                                              g->stream));
+    }
+    else {
+      bmg_tree_bc bc;
+      bc_of_field (g, f, &bc);
+      int r = t_boundary (g, t, f->buf, t->depth, &bc, 0, nl);
+      if (r) return r;
+    }
+  }
+  CKT (cudaStreamSynchronize (g->stream));
+  return FAIL (BMG_OK);
+}

@@ -110,6 +110,19 @@ class Field:
                   "bmg_bc")
         return self
 
+    def bc_level(self, side, kind, level, values):
+        """``s[side] = dirichlet / neumann`` with the values of one level's
+        boundary faces (a tree applies a field's conditions on every level)."""
+        g = self.grid
+        kind = KINDS[kind] if isinstance(kind, str) else int(kind)
+        if _is_torch(values):
+            values = values.detach().cpu().numpy()
+        v = np.ascontiguousarray(values, dtype=np.float64).ravel()
+        check(_lib.load().bmg_bc_level(g.ptr, self.scalar, _side(side), kind, level,
+                                       v.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                       _lib.HOST), "bmg_bc_level")
+        return self
+
 
 class Scalar(Field):
     pass
@@ -352,3 +365,63 @@ def set_niter(nitermax=None, nitermin=None):
         _lib.global_var("NITERMAX").value = nitermax
     if nitermin is not None:
         _lib.global_var("NITERMIN").value = nitermin
+
+
+class TreeGrid(Grid):
+    """A quadtree (grid/quadtree.h) over the levels of a two-dimensional grid
+    of depth ``maxdepth``: ``init_grid (1)`` then ``refine (cond)``.
+
+    Field values live in the level arrays (``Field.set(values, level=l)`` /
+    ``get(level=l)``); the solver reads the leaves, whose mask
+    ``leaf_mask(l)`` gives.  ``poisson``, ``mg_solve``, ``mg_cycle``,
+    ``residual`` and ``restriction`` follow the reference's tree branch.
+    """
+
+    def __init__(self, maxdepth, L0=1.0, origin=(0.0, 0.0), relax="rbgs", graphs=True):
+        super().__init__(2, maxdepth, L0=L0, origin=origin, relax=relax, precision="fp64",
+                         graphs=graphs)
+        self.maxdepth = maxdepth
+
+    def refine(self, cond):
+        """``refine (cond)`` (tree-common.h:308-326) with ``cond(level, x, y)``
+        evaluated at leaf centres; returns the number of refined cells."""
+        cb = _lib.REFINE_COND(lambda l, x, y, z, d: 1 if cond(l, x, y) else 0)
+        r = _lib.load().bmg_tree_refine(self.ptr, cb, None)
+        if r < 0:
+            check(r, "bmg_tree_refine")
+        return r
+
+    def info(self):
+        d = ctypes.c_int()
+        n = ctypes.c_longlong()
+        check(_lib.load().bmg_tree_info(self.ptr, ctypes.byref(d), ctypes.byref(n)),
+              "bmg_tree_info")
+        return d.value, n.value
+
+    @property
+    def tree_depth(self):
+        return self.info()[0]
+
+    @property
+    def leaves(self):
+        return self.info()[1]
+
+    def flags(self, level):
+        n = 1 << level
+        out = np.zeros((n, n), dtype=np.uint8)
+        check(_lib.load().bmg_tree_flags(self.ptr, level,
+                                         out.ctypes.data_as(ctypes.POINTER(ctypes.c_ubyte))),
+              "bmg_tree_flags")
+        return out
+
+    def leaf_mask(self, level):
+        return (self.flags(level) & _lib.TREE_LEAF) != 0
+
+    def level_delta(self, level):
+        return self.L0 * (1.0 / (1 << level))
+
+    def centers(self, level):
+        """Cell centres of one level, ``x = (i + 0.5) Delta + X0``."""
+        n = 1 << level
+        c = (np.arange(n) + 0.5) * self.level_delta(level)
+        return np.meshgrid(c + self.origin[0], c + self.origin[1], indexing="ij")

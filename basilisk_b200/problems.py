@@ -19,6 +19,12 @@ x = (i + 0.5)*Delta (cartesian-common.h:15), face d at x = i*Delta.
                         b ~ N(0, 1) smoothed by 4 weighted-Jacobi sweeps
                         u <- (1 - w) u + w (sum of 6 neighbours)/6, w = 2/3,
                         periodic wrap
+  two_phase_tree        the two_phase_2d problem on a quadtree: level < 5
+                        everywhere, and every cell whose centre lies within 4
+                        of its own cells of the circle r = 0.25 refined, up to
+                        level 11 (2:1 graded); the interface width is that of
+                        the finest level on every level, b ~ N(0, 1) drawn per
+                        level (the solver reads the leaves)
   random_field_2d       512^2 periodic Poisson with alpha = exp(kappa) on faces,
                         kappa a Gaussian random field (FFT, squared-exponential
                         covariance sigma^2 exp(-r^2 / (2 l^2)), l = 0.05,
@@ -54,8 +60,10 @@ def poisson_periodic_2d(depth=7, seed=0):
             "alpha": None, "lambda": None, "bc": {}, "tolerance": 1e-6}
 
 
-def two_phase_alpha(n, rho1=1.0, rho2=1000.0, radius=0.25):
-    D = 1.0 / n
+def two_phase_alpha(n, rho1=1.0, rho2=1000.0, radius=0.25, width_n=None):
+    """Face coefficients of a level with n cells per side; the interface
+    width is 2 Delta of a level with width_n cells (default: this one)."""
+    D = 1.0 / (width_n or n)
     x, y = centers(2, n)
     r = np.sqrt((x - 0.5) ** 2 + (y - 0.5) ** 2)
     f = 0.5 * (1.0 - np.tanh((r - radius) / (2.0 * D)))
@@ -150,3 +158,30 @@ def setup(grid, prob):
     else:
         lam_f = grid.scalar(lam)
     return a, b, alpha, lam_f
+
+
+def band_refinement(depth, base, width=4.0, radius=0.25, center=(0.5, 0.5)):
+    """``refine`` predicate of two_phase_tree: every cell below level base,
+    and the cells whose centre lies within ``width`` cells of their own level
+    of the circle, up to level depth."""
+    def cond(level, x, y):
+        if level < base:
+            return True
+        if level >= depth:
+            return False
+        r = math.sqrt((x - center[0]) ** 2 + (y - center[1]) ** 2)
+        return abs(r - radius) < width * (1.0 / (1 << level))
+    return cond
+
+
+def two_phase_tree_levels(depth, seed=1):
+    """Dense per-level inputs of two_phase_tree: {level: (b, alpha_x,
+    alpha_y)}; the leaves of any tree of this depth read their cells."""
+    rng = np.random.default_rng(seed)
+    n_fine = 1 << depth
+    out = {}
+    for l in range(depth + 1):
+        n = 1 << l
+        ax, ay = two_phase_alpha(n, width_n=n_fine)
+        out[l] = (rng.standard_normal((n, n)), ax, ay)
+    return out

@@ -185,6 +185,37 @@ void mg_cycle (bmg_scalar * a, bmg_scalar * res, bmg_scalar * da,
    as test/variable.c calls it for its face coefficients; list ends with .i=0 */
 int bmg_restriction (bmg_grid * grid, const bmg_scalar * list);
 
+/* ---- quadtree grids: grid/quadtree.h (grid/tree.h, tree-common.h) --- */
+
+/* refine (cond) (tree-common.h:308-326) on a two-dimensional, non-periodic
+   grid: the grid's levels become a quadtree whose root is init_grid (1);
+   every leaf for which cond (level, x, y, z, data) is non-zero is refined,
+   with the 2:1 balance of refine_cell (tree-common.h:22-55), until no leaf
+   asks for refinement.  The tree's depth is at most the grid's depth
+   (deeper refinement fails with BMG_EINVAL).  Returns the number of
+   refined cells (>= 0) or a negative status.  Once a grid is a tree,
+   poisson, mg_solve, mg_cycle, bmg_relax, bmg_residual and bmg_restriction
+   follow the reference's tree branch: relaxation over
+   foreach_level_or_leaf, the tree boundary (restriction then bilinear halo
+   prolongation, tree-common.h:588-716), the conservative residual
+   (poisson.h:355-372).  Cell values live in the grid's level arrays
+   (bmg_field_set_level / get_level); a field's leaves are the cells whose
+   flags have BMG_TREE_LEAF.  The tree path computes in FP64. */
+typedef int (* bmg_refine_cond) (int level, double x, double y, double z, void * data);
+int bmg_tree_refine (bmg_grid * grid, bmg_refine_cond cond, void * data);
+/* depth () and the number of leaves of a tree grid */
+int bmg_tree_info (const bmg_grid * grid, int * depth, long long * leaves);
+/* cell flags of one level, n x n bytes in the compact layout
+   (grid/tree.h:27-47, 398-399): */
+enum { BMG_TREE_ACTIVE = 1, BMG_TREE_LEAF = 2, BMG_TREE_HALO = 4, BMG_TREE_PROLONGATION = 8 };
+int bmg_tree_flags (const bmg_grid * grid, int level, unsigned char * flags);
+/* s[side] = dirichlet / neumann with one value per boundary face of one
+   level (n values over the tangential index): a tree applies the condition
+   of a field on every level (tree_boundary_level), with the expression
+   evaluated at that level's face centres */
+int bmg_bc_level (bmg_grid * grid, bmg_scalar s, int side, int type, int level,
+                  const double * values, int memory);
+
 /* ---- differentiation ----------------------------------------------- */
 
 /* Gradients of a loss l(a) with respect to the coefficients of the solve

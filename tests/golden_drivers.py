@@ -251,3 +251,25 @@ def circle_variable_program(make, depths=(7, 8, 9, 10), niter=13):
         lines += ["residual %d %d %.1g" % (depth, i, r) for i, r in enumerate(maxres)]
         lines.append("max error %d %g" % (depth, leaf_max_error(t, A, solution)))
     return lines, t
+
+
+def band_refinement(depth, base, width=4.0):
+    from basilisk_b200.problems import band_refinement as br
+    return br(depth, base, width)
+
+
+def two_phase_tree(t, seed=1):
+    """The two-phase variable-coefficient problem (basilisk_b200.problems,
+    two_phase_tree) on an already refined tree: Dirichlet a = 0, lambda = 0."""
+    from basilisk_b200.problems import two_phase_tree_levels
+    from oracle.tree import A, B, ALPHA_X, ALPHA_Y
+    lv = two_phase_tree_levels(t.depth, seed)
+    for side in range(4):
+        t.set_bc(side, DIRICHLET, 0.0)
+    for l, (b, ax, ay) in lv.items():
+        t.set_level(B, l, b)
+        t.set_level(A, l, np.zeros_like(b))
+        t.set_level(ALPHA_X, l, ax)
+        t.set_level(ALPHA_Y, l, ay)
+    t.set_lambda_const(0.0)
+    return t

@@ -94,3 +94,111 @@ def random_problem(dim, depth, rng, periodic=(), bc=None, alpha="field", lam=Non
     if a0:
         prob["a0"] = rng.standard_normal(shape)
     return prob
+
+
+class GpuTree:
+    """The interface of ``oracle.tree.Tree`` on the CUDA library's
+    ``TreeGrid``, so that the tree programs of ``golden_drivers`` run on
+    both; the field ids are the oracle's."""
+
+    def __init__(self, maxdepth, origin=(0.0, 0.0), relax="rbgs", L0=1.0, graphs=True):
+        import basilisk_b200 as bmg
+        from oracle import tree as ot
+        self.ot = ot
+        self.g = bmg.TreeGrid(maxdepth, L0=L0, origin=origin, relax=relax, graphs=graphs)
+        self.L0, self.X0, self.Y0 = float(L0), float(origin[0]), float(origin[1])
+        self.f = {ot.A: self.g.scalar(), ot.B: self.g.scalar(), ot.RES: self.g.scalar(),
+                  ot.DA: self.g.scalar()}
+        self.alpha = None
+        self.lam = None
+
+    def close(self):
+        self.g.close()
+
+    def refine(self, cond):
+        return self.g.refine(cond)
+
+    @property
+    def depth(self):
+        return self.g.tree_depth
+
+    @property
+    def leaves(self):
+        return self.g.leaves
+
+    def flags(self, level):
+        return self.g.flags(level)
+
+    def delta(self, level):
+        return self.L0 * (1.0 / (1 << level))
+
+    # geometry shared with the oracle's Tree
+    def centers(self, level):
+        return self.ot.Tree.centers(self, level)
+
+    def face_centers(self, level, d):
+        return self.ot.Tree.face_centers(self, level, d)
+
+    def boundary_points(self, level, side):
+        return self.ot.Tree.boundary_points(self, level, side)
+
+    def _field(self, which):
+        ot = self.ot
+        if which == ot.LAMBDA:
+            if self.lam is None or self.lam.const is not None:
+                self.lam = self.g.scalar()
+            return self.lam
+        if which in (ot.ALPHA_X, ot.ALPHA_Y):
+            if self.alpha is None or self.alpha.const is not None:
+                self.alpha = self.g.face_vector()
+            return self.alpha.components[0 if which == ot.ALPHA_X else 1]
+        return self.f[which]
+
+    def set_level(self, which, level, values):
+        self._field(which).set(np.ascontiguousarray(values, dtype=np.float64), level=level)
+
+    def get_level(self, which, level):
+        return self._field(which).get(level=level)
+
+    def set_bc(self, side, kind, value=0.0, level=None, values=None):
+        ot = self.ot
+        k = "dirichlet" if kind == ot.DIRICHLET else "neumann"
+        if values is None:
+            self.f[ot.A].bc(side, k, float(value))
+        else:
+            self.f[ot.A].bc_level(side, k, level, values)
+        self.f[ot.DA].bc(side, k, 0.0)
+
+    def set_relax(self, mode):
+        ot = self.ot
+        self.g.set_relax({ot.RELAX_RBGS: "rbgs", ot.RELAX_JACOBI: "jacobi"}[mode])
+
+    def set_alpha_const(self, v):
+        self.alpha = None if v == 1.0 else self.g.const_face_vector(v)
+
+    def set_lambda_const(self, v):
+        self.lam = None if v == 0.0 else self.g.const_scalar(v)
+
+    def restrict_coefficients(self):
+        fs = [f for f in (self.alpha, self.lam) if f is not None and f.const is None]
+        if fs:
+            self.g.restriction(fs)
+
+    def residual(self):
+        ot = self.ot
+        return self.g.residual(self.f[ot.A], self.f[ot.B], self.f[ot.RES], self.alpha, self.lam)
+
+    def mg_cycle(self, nrelax, minlevel, maxlevel):
+        ot = self.ot
+        self.g.mg_cycle(self.f[ot.A], self.f[ot.RES], self.f[ot.DA], nrelax, minlevel, maxlevel,
+                        self.alpha, self.lam)
+
+    def mg_solve(self, tolerance=0.0, nrelax=4, minlevel=0):
+        ot = self.ot
+        return self.g.mg_solve(self.f[ot.A], self.f[ot.B], self.alpha, self.lam,
+                               tolerance=tolerance, nrelax=nrelax, minlevel=minlevel)
+
+    def poisson(self, tolerance=0.0, nrelax=4, minlevel=0):
+        ot = self.ot
+        return self.g.poisson(self.f[ot.A], self.f[ot.B], self.alpha, self.lam,
+                              tolerance=tolerance, nrelax=nrelax, minlevel=minlevel)

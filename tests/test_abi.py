@@ -17,6 +17,8 @@ HEADER = os.path.join(ROOT, "include", "basilisk_mg.h")
 def declared_functions():
     text = open(HEADER).read()
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    # typedefs of function-pointer types declare no symbol
+    text = re.sub(r"^\s*typedef[^;]*;", "", text, flags=re.M | re.S)
     names = set()
     for m in re.finditer(r"^\s*[A-Za-z_][\w\s\*]*?\b([A-Za-z_]\w*)\s*\(", text, flags=re.M):
         name = m.group(1)
