@@ -79,32 +79,40 @@ __global__ void k_prolong (const uint32_t * __restrict__ list, long n, TL T, dou
 
 /* refine_bilinear of the halo children of prolongation leaves: one thread
    per child */
+__device__ __forceinline__ void halo_child (const uint32_t * list, long k, const TL & T, double * s)
+{
+  int l, i, j;
+  unpack (list[k >> 2], l, i, j);
+  const int ci = 2*i + (int) ((k >> 1) & 1), cj = 2*j + (int) (k & 1);
+  s[gidx (T, l + 1, ci, cj)] = bilinear (T, s, l + 1, ci, cj);
+}
+
 __global__ void k_halo (const uint32_t * __restrict__ list, long n, TL T, double * s)
 {
-  GRID_STRIDE (k, 4*n) {
-    int l, i, j;
-    unpack (list[k >> 2], l, i, j);
-    const int ci = 2*i + (int) ((k >> 1) & 1), cj = 2*j + (int) (k & 1);
-    s[gidx (T, l + 1, ci, cj)] = bilinear (T, s, l + 1, ci, cj);
-  }
+  GRID_STRIDE (k, 4*n)
+    halo_child (list, k, T, s);
 }
 
 /* restriction_average (multigrid-common.h:26-32), children in foreach_child
    order */
+__device__ __forceinline__ void restrict_cell (const uint32_t * list, long k, const TL & T, double * s)
+{
+  int l, i, j;
+  unpack (list[k], l, i, j);
+  const double * f = s + T.off[l + 1];
+  const bmg_geom & gf = T.g[l + 1];
+  double sum = 0.;
+  sum += f[cidx<2> (gf, 2*i, 2*j, 0)];
+  sum += f[cidx<2> (gf, 2*i, 2*j + 1, 0)];
+  sum += f[cidx<2> (gf, 2*i + 1, 2*j, 0)];
+  sum += f[cidx<2> (gf, 2*i + 1, 2*j + 1, 0)];
+  s[gidx (T, l, i, j)] = sum/(1 << 2);
+}
+
 __global__ void k_restrict (const uint32_t * __restrict__ list, long n, TL T, double * s)
 {
-  GRID_STRIDE (k, n) {
-    int l, i, j;
-    unpack (list[k], l, i, j);
-    const double * f = s + T.off[l + 1];
-    const bmg_geom & gf = T.g[l + 1];
-    double sum = 0.;
-    sum += f[cidx<2> (gf, 2*i, 2*j, 0)];
-    sum += f[cidx<2> (gf, 2*i, 2*j + 1, 0)];
-    sum += f[cidx<2> (gf, 2*i + 1, 2*j, 0)];
-    sum += f[cidx<2> (gf, 2*i + 1, 2*j + 1, 0)];
-    s[gidx (T, l, i, j)] = sum/(1 << 2);
-  }
+  GRID_STRIDE (k, n)
+    restrict_cell (list, k, T, s);
 }
 
 __device__ __forceinline__ bool refined_at (const TL & T, const unsigned char * fl, int l, int i, int j)
@@ -149,22 +157,41 @@ __device__ __forceinline__ double bc_of (const bmg_tree_bc & bc, int side, int l
   return homog ? sn : Delta*val + sn;
 }
 
+__device__ __forceinline__ void ghost_value (const bmg_tree_rule & r, const TL & T, double * s,
+                                             const bmg_tree_bc & bc, int homog)
+{
+  int l, gi, gj, l2, a, b;
+  unpack (r.ghost, l, gi, gj);
+  unpack (r.inner, l2, a, b);
+  const long long nid = gidx (T, l, a, b);
+  const double sn = s[nid], D = T.Delta[l];
+  const int s1 = r.kind_sides & 15, s2 = (r.kind_sides >> 4) & 15, kind = r.kind_sides >> 8;
+  const int t1 = r.tidx & 0xFFFF, t2 = r.tidx >> 16;
+  double v = bc_of (bc, s1, l, t1, sn, D, homog);
+  if (kind == BMG_T_DIAGONAL)
+    v = (v + bc_of (bc, s2, l, t2, sn, D, homog) - sn);
+  s[gidx (T, l, gi, gj)] = v;
+}
+
 __global__ void k_bc (const bmg_tree_rule * __restrict__ rules, long n, TL T, double * s,
                       bmg_tree_bc bc, int homog)
 {
-  GRID_STRIDE (k, n) {
-    const bmg_tree_rule r = rules[k];
-    int l, gi, gj, l2, a, b;
-    unpack (r.ghost, l, gi, gj);
-    unpack (r.inner, l2, a, b);
-    const long long nid = gidx (T, l, a, b);
-    const double sn = s[nid], D = T.Delta[l];
-    const int s1 = r.kind_sides & 15, s2 = (r.kind_sides >> 4) & 15, kind = r.kind_sides >> 8;
-    const int t1 = r.tidx & 0xFFFF, t2 = r.tidx >> 16;
-    double v = bc_of (bc, s1, l, t1, sn, D, homog);
-    if (kind == BMG_T_DIAGONAL)
-      v = (v + bc_of (bc, s2, l, t2, sn, D, homog) - sn);
-    s[gidx (T, l, gi, gj)] = v;
+  GRID_STRIDE (k, n)
+    ghost_value (rules[k], T, s, bc, homog);
+}
+
+/* one stage of a scheduled tree boundary: a restriction or halo
+   prolongation level (op) and, in the same launch, ghost cells whose
+   interior values were final before it and which it does not read */
+__global__ void k_stage (const uint32_t * __restrict__ list, long n, int op,
+                         const bmg_tree_rule * __restrict__ rules, long nr, TL T, double * s,
+                         bmg_tree_bc bc, int homog)
+{
+  const long w = op == BMG_T_OP_HALO ? 4*n : op == BMG_T_OP_RESTRICT ? n : 0;
+  GRID_STRIDE (k, w + nr) {
+    if (k >= w) ghost_value (rules[k - w], T, s, bc, homog);
+    else if (op == BMG_T_OP_HALO) halo_child (list, k, T, s);
+    else restrict_cell (list, k, T, s);
   }
 }
 
@@ -369,6 +396,16 @@ int bmg_tree_launch_bc (const bmg_tree_rule * rules, long n, const bmg_tree_leve
 {
   if (n <= 0) return 0;
   k_bc<<<blocks_for (n), NT, 0, st>>> (rules, n, *T, s, *bc, homogeneous);
+  return status ();
+}
+
+int bmg_tree_launch_stage (const uint32_t * list, long n, int op, const bmg_tree_rule * rules,
+                           long nrules, const bmg_tree_levels * T, double * s,
+                           const bmg_tree_bc * bc, int homogeneous, cudaStream_t st)
+{
+  const long w = (op == BMG_T_OP_HALO ? 4*n : op == BMG_T_OP_RESTRICT ? n : 0) + nrules;
+  if (w <= 0) return 0;
+  k_stage<<<blocks_for (w), NT, 0, st>>> (list, n, op, rules, nrules, *T, s, *bc, homogeneous);
   return status ();
 }
 

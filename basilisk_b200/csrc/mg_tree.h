@@ -71,6 +71,14 @@ int bmg_tree_launch_restrict_faces (const uint32_t * list, long n, const bmg_tre
                                     cudaStream_t st);
 int bmg_tree_launch_bc (const bmg_tree_rule * rules, long n, const bmg_tree_levels * T,
                         double * s, const bmg_tree_bc * bc, int homogeneous, cudaStream_t st);
+/* one stage of a scheduled tree boundary: op (restriction of the listed
+   refined cells, or bilinear prolongation into the halo children of the
+   listed prolongation leaves, or nothing) together with a span of ghost
+   rules, in one launch */
+enum { BMG_T_OP_NONE = 0, BMG_T_OP_RESTRICT = 1, BMG_T_OP_HALO = 2 };
+int bmg_tree_launch_stage (const uint32_t * list, long n, int op, const bmg_tree_rule * rules,
+                           long nrules, const bmg_tree_levels * T, double * s,
+                           const bmg_tree_bc * bc, int homogeneous, cudaStream_t st);
 /* out = n/d of relax (poisson.h:303-320) for the listed cells: out = a for
    an in-place colour pass, the Jacobi temporary otherwise */
 int bmg_tree_launch_relax (const uint32_t * list, long n, const bmg_tree_levels * T,

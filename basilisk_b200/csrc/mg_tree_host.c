@@ -36,6 +36,10 @@
 
 typedef struct { long off, n; } span_t;
 
+/* one launch of a scheduled tree boundary (bmg_tree_launch_stage) */
+typedef struct { int op; span_t list; span_t rules; } tstage;
+enum { SCHED_FULL = 0, SCHED_PRUNED = 1 };
+
 /* everything a captured solve iteration depends on */
 typedef struct {
   int nrelax, minlevel, maxlevel, relax;
@@ -65,6 +69,12 @@ struct bmg_tree {
   bmg_tree_rule * drules;
   span_t act[TMAX + 1], ref[TMAX + 1], prol[TMAX + 1], rl[TMAX + 1], ghost[TMAX + 1], leaves;
   long rl1[TMAX + 1];                 /* colour-1 part of rl[l] starts here */
+  /* tree boundary schedules: [SCHED_FULL / SCHED_PRUNED][level] spans of
+     stages, whose rules live in dsrules */
+  tstage * stages;
+  long nstages;
+  span_t sched[2][TMAX + 1];
+  bmg_tree_rule * dsrules;
   bmg_tree_levels T;
   double * dpart;
   int npart;
@@ -100,6 +110,8 @@ static void tree_release (struct bmg_tree * t)
     if (t->graphs[i].valid) cudaGraphExecDestroy (t->graphs[i].exec);
   for (int l = 0; l <= TMAX; l++) { free (t->fl[l]); free (t->nb[l]); }
   cudaFree (t->dflags); cudaFree (t->dlist); cudaFree (t->drules); cudaFree (t->dpart);
+  cudaFree (t->dsrules);
+  free (t->stages);
   free (t);
 }
 
@@ -241,6 +253,87 @@ static int ghost_rule (const struct bmg_tree * t, int l, int gi, int gj, bmg_tre
   return 0;
 }
 
+/* The launches of tree_boundary_level (s, l), as stages.  The events are
+   the restriction of levels l-1 down to mlo, then the halo prolongation of
+   levels mlo up to l-1 (tree-common.h:672-712); the ghost cells of levels
+   mlo..l ride along: a ghost can run in the first event after the one that
+   produces its interior value (restriction of its level for a refined
+   cell, halo prolongation of the level below for a halo cell, none for a
+   leaf or a cell of level l), provided that event does not read it (the
+   halo prolongation of its own level does); otherwise it gets a launch of
+   its own at that point.  With mlo = 0 every value of the reference's
+   sequence is computed; SCHED_PRUNED starts at the coarsest level holding a
+   leaf, below which no value computed here is ever read (no leaf relaxes
+   there, no halo is prolonged from there). */
+static int schedule (struct bmg_tree * t, int l, int mlo, const bmg_tree_rule * hr,
+                     tstage ** st, long * nst, long * cap, bmg_tree_rule ** rs, long * nrs,
+                     long * rcap)
+{
+  typedef struct { int op, level; } event_t;
+  event_t ev[2*(TMAX + 1)];
+  int E = 0, Ridx[TMAX + 1], Hidx[TMAX + 1];
+  for (int m = 0; m <= TMAX; m++) Ridx[m] = Hidx[m] = -1;
+  if (mlo > l) mlo = l;
+  for (int m = l - 1; m >= mlo; m--)
+    if (t->ref[m].n) { Ridx[m] = E; ev[E].op = BMG_T_OP_RESTRICT; ev[E++].level = m; }
+  for (int i = mlo; i < l; i++)
+    if (t->prol[i].n) { Hidx[i] = E; ev[E].op = BMG_T_OP_HALO; ev[E++].level = i; }
+  /* slot of every rule: 2*k = a launch of its own before event k,
+     2*k + 1 = fused into event k */
+  long nr = 0;
+  for (int m = mlo; m <= l; m++) nr += t->ghost[m].n;
+  int * slot = malloc ((nr + 1)*sizeof (int));
+  const bmg_tree_rule ** rp = malloc ((nr + 1)*sizeof (*rp));
+  if (!slot || !rp) { free (slot); free (rp); return BMG_ENOMEM; }
+  long q = 0;
+  for (int m = mlo; m <= l; m++)
+    for (long k = 0; k < t->ghost[m].n; k++, q++) {
+      const bmg_tree_rule * r = &hr[t->ghost[m].off + k];
+      const int ii = (int) ((r->inner >> 14) & 0x3FFF) - 1, jj = (int) (r->inner & 0x3FFF) - 1;
+      const unsigned char f = t->fl[m][HX (m, ii, jj)];
+      int p = -1;
+      if (m < l && (f & BMG_T_ACTIVE) && !(f & BMG_T_LEAF)) p = Ridx[m];
+      else if (f & BMG_T_HALO) p = m >= 1 ? Hidx[m - 1] : -1;
+      const int c = (m < l && Hidx[m] >= 0) ? Hidx[m] : E;
+      const int e = p + 1;
+      slot[q] = (e < c && e < E) ? 2*e + 1 : 2*e;
+      rp[q] = r;
+    }
+  for (int sl = 0; sl <= 2*E; sl++) {
+    const int k = sl/2, fused = sl & 1;
+    if (fused && k >= E) break;
+    long first = *nrs;
+    for (long u = 0; u < nr; u++)
+      if (slot[u] == sl) {
+        if (*nrs == *rcap) {
+          *rcap = 2*(*rcap) + 1024;
+          bmg_tree_rule * nrp = realloc (*rs, *rcap*sizeof (bmg_tree_rule));
+          if (!nrp) { free (slot); free (rp); return BMG_ENOMEM; }
+          *rs = nrp;
+        }
+        (*rs)[(*nrs)++] = *rp[u];
+      }
+    if (!fused && *nrs == first) continue;          /* no launch of its own needed */
+    if (*nst == *cap) {
+      *cap = 2*(*cap) + 64;
+      tstage * ns = realloc (*st, *cap*sizeof (tstage));
+      if (!ns) { free (slot); free (rp); return BMG_ENOMEM; }
+      *st = ns;
+    }
+    tstage * sg = &(*st)[(*nst)++];
+    memset (sg, 0, sizeof *sg);
+    sg->rules.off = first; sg->rules.n = *nrs - first;
+    if (fused) {
+      sg->op = ev[k].op;
+      sg->list = ev[k].op == BMG_T_OP_RESTRICT ? t->ref[ev[k].level] : t->prol[ev[k].level];
+    }
+    else
+      sg->op = BMG_T_OP_NONE;
+  }
+  free (slot); free (rp);
+  return BMG_OK;
+}
+
 /* flags of halo cells and prolongation leaves, cell lists, ghost rules:
    the caches of update_cache_f (tree.h:556-684), uploaded */
 static int derive (bmg_grid * g, struct bmg_tree * t)
@@ -358,7 +451,29 @@ static int derive (bmg_grid * g, struct bmg_tree * t)
       cudaMemcpy (t->dlist, h, total*sizeof (uint32_t), cudaMemcpyHostToDevice) != cudaSuccess ||
       (k && cudaMemcpy (t->drules, hr, k*sizeof (bmg_tree_rule), cudaMemcpyHostToDevice) != cudaSuccess))
     st = BMG_ENOMEM;
-  free (h); free (hr); free (hf);
+  free (h); free (hf);
+  if (st) { free (hr); return FAIL (st); }
+  /* boundary schedules */
+  int mleaf = D;
+  for (int l = D; l >= 0; l--) if (nleaf[l]) mleaf = l;
+  free (t->stages); t->stages = NULL; t->nstages = 0;
+  long cap = 0, nrs = 0, rcap = 0;
+  bmg_tree_rule * rs = NULL;
+  for (int kind = 0; kind < 2 && !st; kind++)
+    for (int l = 0; l <= D && !st; l++) {
+      const long first = t->nstages;
+      st = schedule (t, l, kind == SCHED_FULL ? 0 : mleaf, hr, &t->stages, &t->nstages, &cap,
+                     &rs, &nrs, &rcap);
+      t->sched[kind][l].off = first;
+      t->sched[kind][l].n = t->nstages - first;
+    }
+  free (hr);
+  cudaFree (t->dsrules); t->dsrules = NULL;
+  if (!st && (cudaMalloc ((void **) &t->dsrules, (nrs + 1)*sizeof (bmg_tree_rule)) != cudaSuccess ||
+              (nrs && cudaMemcpy (t->dsrules, rs, nrs*sizeof (bmg_tree_rule),
+                                  cudaMemcpyHostToDevice) != cudaSuccess)))
+    st = BMG_ENOMEM;
+  free (rs);
   if (st) return FAIL (st);
   memset (&t->T, 0, sizeof t->T);
   for (int l = 0; l <= g->depth && l <= TMAX; l++) {
@@ -476,19 +591,18 @@ static int t_bc (bmg_grid * g, struct bmg_tree * t, double * s, int l, const bmg
   return BMG_OK;
 }
 
-/* tree_boundary_level (tree-common.h:588-716) of a cell field up to level l */
+/* tree_boundary_level (tree-common.h:588-716) of a cell field up to level
+   l, by the stages of schedule () */
 static int t_boundary (bmg_grid * g, struct bmg_tree * t, double * s, int l, const bmg_tree_bc * bc,
-                       int homog, long long * nl)
+                       int homog, int kind, long long * nl)
 {
   if (t->full) return t_bc (g, t, s, l, bc, homog, nl);
-  for (int m = l - 1; m >= 0; m--)
-    if (t->ref[m].n) LT (bmg_tree_launch_restrict (LIST (t->ref[m]), &t->T, s, g->stream));
-  int r = t_bc (g, t, s, 0, bc, homog, nl);
-  if (r) return r;
-  for (int i = 0; i < l; i++) {
-    if (t->prol[i].n) LT (bmg_tree_launch_halo (LIST (t->prol[i]), &t->T, s, g->stream));
-    r = t_bc (g, t, s, i + 1, bc, homog, nl);
-    if (r) return r;
+  const span_t sp = t->sched[kind][l];
+  for (long k = 0; k < sp.n; k++) {
+    const tstage * sg = &t->stages[sp.off + k];
+    LT (bmg_tree_launch_stage (t->dlist + sg->list.off, sg->list.n, sg->op,
+                               t->dsrules + sg->rules.off, sg->rules.n, &t->T, s, bc, homog,
+                               g->stream));
   }
   return BMG_OK;
 }
@@ -505,7 +619,7 @@ static int t_relax (bmg_grid * g, struct bmg_tree * t, double * da, const double
   }
   const span_t red = {all.off, t->rl1[l]}, black = {all.off + t->rl1[l], all.n - t->rl1[l]};
   if (red.n) LT (bmg_tree_launch_relax (LIST (red), &t->T, da, res, c->ax, c->ay, c->lam, da, g->stream));
-  int r = t_boundary (g, t, da, l, dabc, 1, nl);
+  int r = t_boundary (g, t, da, l, dabc, 1, SCHED_PRUNED, nl);
   if (r) return r;
   if (black.n) LT (bmg_tree_launch_relax (LIST (black), &t->T, da, res, c->ax, c->ay, c->lam, da, g->stream));
   return BMG_OK;
@@ -524,12 +638,12 @@ static int t_cycle (bmg_grid * g, struct bmg_tree * t, double * a, double * da, 
       LT (bmg_tree_launch_set (LIST (t->rl[l]), &t->T, da, 0., g->stream));
     else
       LT (bmg_tree_launch_prolong (LIST (t->act[l]), &t->T, da, g->stream));
-    int r = t_boundary (g, t, da, l, dabc, 1, nl);
+    int r = t_boundary (g, t, da, l, dabc, 1, SCHED_PRUNED, nl);
     if (r) return r;
     for (int i = 0; i < nrelax; i++) {
       r = t_relax (g, t, da, res, tmp, c, l, dabc, nl);
       if (r) return r;
-      r = t_boundary (g, t, da, l, dabc, 1, nl);
+      r = t_boundary (g, t, da, l, dabc, 1, SCHED_PRUNED, nl);
       if (r) return r;
     }
   }
@@ -541,7 +655,7 @@ static int t_cycle (bmg_grid * g, struct bmg_tree * t, double * a, double * da, 
 static int t_residual (bmg_grid * g, struct bmg_tree * t, double * a, const double * b, double * res,
                        const tcoefs * c, const bmg_tree_bc * abc, long long * nl)
 {
-  int r = t_boundary (g, t, a, t->depth, abc, 0, nl);
+  int r = t_boundary (g, t, a, t->depth, abc, 0, SCHED_FULL, nl);
   if (r) return r;
   CKT (cudaMemsetAsync (g->d_maxres, 0, sizeof (unsigned long long), g->stream));
   LT (bmg_tree_launch_residual (LIST (t->leaves), &t->T, t->dflags, a, b, c->ax, c->ay, c->lam,
@@ -813,7 +927,7 @@ int bmg_tree_restriction (bmg_grid * g, const bmg_scalar * list)
     else {
       bmg_tree_bc bc;
       bc_of_field (g, f, &bc);
-      int r = t_boundary (g, t, f->buf, t->depth, &bc, 0, nl);
+      int r = t_boundary (g, t, f->buf, t->depth, &bc, 0, SCHED_FULL, nl);
       if (r) return r;
     }
   }
