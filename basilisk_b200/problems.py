@@ -185,3 +185,19 @@ def two_phase_tree_levels(depth, seed=1):
         ax, ay = two_phase_alpha(n, width_n=n_fine)
         out[l] = (rng.standard_normal((n, n)), ax, ay)
     return out
+
+
+def setup_tree(grid, depth=11, base=5, seed=1):
+    """two_phase_tree on ``grid`` (a basilisk_b200.TreeGrid of depth >=
+    depth): refine, then create the fields; returns (a, b, alpha) with a = 0
+    on every level, Dirichlet a = 0 on the four walls."""
+    grid.refine(band_refinement(depth, base))
+    a, b = grid.scalar(), grid.scalar()
+    for side in range(4):
+        a.bc(side, "dirichlet", 0.0)
+    alpha = grid.face_vector()
+    for l, (bl, ax, ay) in two_phase_tree_levels(grid.tree_depth, seed).items():
+        b.set(bl, level=l)
+        a.set(np.zeros_like(bl), level=l)
+        alpha.set([ax, ay], level=l)
+    return a, b, alpha

@@ -245,6 +245,108 @@ def cpu_solve(prob, threads=None):
     return time.perf_counter() - t0, st, threads
 
 
+def run_workload(args, ws, rank, local):
+    """The other workloads of the scope table, one JSON line each (not the
+    headline): the quadtree problem (two_phase_tree, depth 11) and the 3D
+    periodic Helmholtz problem (helmholtz_3d, 256^3).  One step = one
+    poisson () solve from a = 0."""
+    import torch
+    import basilisk_b200 as bmg
+    from basilisk_b200 import problems
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    clocks = ClockSampler(local)
+    if args.workload == "two_phase_tree":
+        g = bmg.TreeGrid(11, relax="rbgs")
+        g.set_stream(torch.cuda.current_stream().cuda_stream)
+        a, b, alpha = problems.setup_tree(g, 11, 5, seed=1 + rank)
+        zeros = [torch.zeros((1 << l, 1 << l), dtype=torch.float64, device="cuda")
+                 for l in range(g.tree_depth + 1)]
+        tol, dtype = TOL, "f64"
+
+        def reset():
+            for l, z in enumerate(zeros):
+                a.set(z, level=l)
+
+        def solve():
+            return g.poisson(a, b, alpha=alpha, tolerance=tol)
+        config = {"workload": "two_phase_tree: the two_phase_2d problem on a quadtree, level < 5 "
+                              "everywhere and cells within 4 cells of r = 0.25 refined up to "
+                              "level 11 (%d leaves), tolerance 1e-6, at most 100 V-cycles"
+                              % g.leaves,
+                  "grid": "quadtree levels 5-11", "relax": "red-black Gauss-Seidel",
+                  "parallelism": "replicas" if ws > 1 else "1 gpu"}
+    else:
+        prob = problems.helmholtz_3d(depth=8, seed=2 + rank)
+        g = bmg.Grid(3, 8, relax="rbgs", precision=args.precision)
+        g.set_stream(torch.cuda.current_stream().cuda_stream)
+        a, b, alpha, lam = problems.setup(g, prob)
+        zero = torch.zeros(prob["b"].shape, dtype=torch.float64, device="cuda")
+        tol, dtype = prob["tolerance"], "f64" if args.precision == "fp64" else "f32+f64"
+
+        def reset():
+            a.set(zero)
+
+        def solve():
+            return g.poisson(a, b, alpha=alpha, lambda_=lam, tolerance=tol)
+        config = {"workload": "helmholtz_3d: 256^3 periodic Helmholtz, alpha = 1e-2 stored on "
+                              "every face, lambda = -1000, b ~ N(0,1) smoothed, tolerance %g"
+                              % tol,
+                  "grid": "256^3 (depth 8)", "form": args.precision,
+                  "relax": "red-black Gauss-Seidel",
+                  "parallelism": "replicas" if ws > 1 else "1 gpu"}
+    g.set_timing(True)
+    for _ in range(args.warmup):
+        reset()
+        solve()
+    torch.cuda.synchronize()
+    barrier(ws)
+    g.reset_counters()
+    times, st = [], None
+    clocks.start()
+    for _ in range(args.steps):
+        flush_l2(flush)
+        reset()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        st = solve()
+        e1.record()
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+    clk = clocks.stop()
+    barrier(ws)
+    c = g.counters()
+    ms = max_over_ranks(ws, sum(times) / len(times))
+    if rank != 0:
+        return
+    line = {"metric": "time-to-residual, %s" % args.workload, "value": ws * 1e3 / ms,
+            "unit": "solves/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": dtype, "data": "synthetic", "config": config,
+            "mgstats": {k: st[k] for k in ("i", "resb", "resa", "nrelax")},
+            "vcycle": {"cycles": c["cycles"], "ms_per_cycle": c["cycle_ms"] / max(1, c["cycles"]),
+                       "launches_per_cycle": c["launches"] / max(1, c["cycles"]),
+                       "vcycle_gbs": c["bytes"] / (c["cycle_ms"] * 1e-3) / 1e9
+                       if c["cycle_ms"] and c["bytes"] else None},
+            "clocks": clk, "gpu_launches": int(c["launches"])}
+    if not args.no_cpu and args.workload == "two_phase_tree":
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        from oracle import tree as otree
+        import golden_drivers as gd
+        t = otree.Tree(11, 1.0, (0.0, 0.0))
+        t.set_relax(otree.RELAX_GS)
+        t.refine(problems.band_refinement(11, 5))
+        gd.two_phase_tree(t, seed=1)
+        t0 = time.perf_counter()
+        cst = t.poisson(tolerance=TOL, nrelax=4, minlevel=1)
+        dt = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": 1.0 / dt, "unit": "solves/s", "cores": 1, "kind": "port",
+                                "sample": "1 full solve of the same tree (%d V-cycles), the "
+                                          "reference's traversal-order Gauss-Seidel, 1 thread"
+                                          % cst["i"]}
+    print(json.dumps(line), flush=True)
+
+
 def run_reference(args, ws, rank):
     """The reference arm: the CPU implementation, full solves of the same
     workload, on rank 0 only."""
@@ -287,8 +389,19 @@ def main():
     ap.add_argument("--profile", choices=["fp64", "mixed"], default=None,
                     help="profiling run: only this form, no e2e, no CPU baseline, no JSON")
     ap.add_argument("--depth", type=int, default=DEPTH, help="grid depth (profiling runs)")
+    ap.add_argument("--workload", choices=["two_phase_2d", "two_phase_tree", "helmholtz_3d"],
+                    default="two_phase_2d",
+                    help="two_phase_2d: the headline; the others print their own line")
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64",
+                    help="form of the helmholtz_3d workload")
     args = ap.parse_args()
     ws, rank, local = dist_init()
+    if args.impl == "bmg" and args.workload != "two_phase_2d":
+        run_workload(args, ws, rank, local)
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
     if args.impl == "reference":
         run_reference(args, ws, rank)
         if ws > 1:
