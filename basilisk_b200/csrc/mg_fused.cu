@@ -167,15 +167,16 @@ k_relax_tile2d (bmg_geom g, T * __restrict__ out, const T * __restrict__ in,
   static_assert (M % 2 == 0 && M <= 2*BX && W - 2 <= BY, "one pair of cells per thread per row");
   typedef typename Pair<T>::type T2;
   extern __shared__ __align__ (16) unsigned char smem_raw[];
-  T * sa[2], * sr[2], * sx[2], * sy[2], * sl[2];
-  {
-    T * p = (T *) smem_raw;
-    for (int c = 0; c < 2; c++) { sa[c] = p; p += W*M; }
-    for (int c = 0; c < 2; c++) { sr[c] = p; p += W*M; }
-    for (int c = 0; c < 2; c++) { sx[c] = p; p += (W + 1)*M; }
-    for (int c = 0; c < 2; c++) { sy[c] = p; p += W*MY; }
-    for (int c = 0; c < 2; c++) { sl[c] = p; p += LAM ? W*M : 0; }
-  }
+  /* the colour-c arrays, as offsets from one shared base (no pointer
+     tables: those would live in local memory) */
+  T * const smb = (T *) smem_raw;
+  constexpr int WM = W*M, WX = (W + 1)*M, WY = W*MY;
+  constexpr int OR = 2*WM, OX = 4*WM, OY = OX + 2*WX, OL = OY + 2*WY;
+  auto sa = [smb] (int c) { return smb + c*WM; };
+  auto sr = [smb] (int c) { return smb + OR + c*WM; };
+  auto sx = [smb] (int c) { return smb + OX + c*WX; };
+  auto sy = [smb] (int c) { return smb + OY + c*WY; };
+  auto sl = [smb] (int c) { return smb + OL + c*WM; };
   const int n = g.n, tx = threadIdx.x, ty = threadIdx.y;
   const int tid = ty*BX + tx, nth = BX*BY;
   constexpr int RW = 32/BX;     /* rows per warp */
@@ -204,11 +205,11 @@ k_relax_tile2d (bmg_geom g, T * __restrict__ out, const T * __restrict__ in,
       else vx.x = vx.y = vx.z = vx.w = ax.c;
       if (ay.p) vy = load_quad (ay.p + id);
       else vy.x = vy.y = vy.z = vy.w = ay.c;
-      put_quad (sa[c0], sa[c0 ^ 1], p*M + 2*k, va);
-      put_quad (sr[c0], sr[c0 ^ 1], p*M + 2*k, vr);
-      if (LAM) put_quad (sl[c0], sl[c0 ^ 1], p*M + 2*k, vl);
-      put_quad (sx[c0], sx[c0 ^ 1], p*M + 2*k, vx);
-      put_quad (sy[c0], sy[c0 ^ 1], p*MY + 2*k, vy);
+      put_quad (sa(c0), sa(c0 ^ 1), p*M + 2*k, va);
+      put_quad (sr(c0), sr(c0 ^ 1), p*M + 2*k, vr);
+      if (LAM) put_quad (sl(c0), sl(c0 ^ 1), p*M + 2*k, vl);
+      put_quad (sx(c0), sx(c0 ^ 1), p*M + 2*k, vx);
+      put_quad (sy(c0), sy(c0 ^ 1), p*MY + 2*k, vy);
     }
     /* the last x-face row (face i0 + W <= n) and y-face column (j0 + W <= n;
        face n of a periodic direction is face 0) */
@@ -219,11 +220,11 @@ k_relax_tile2d (bmg_geom g, T * __restrict__ out, const T * __restrict__ in,
         Quad<T> vx;
         if (ax.p) vx = load_quad (ax.p + cidx<2> (g, fi, j0 + q, 0));
         else vx.x = vx.y = vx.z = vx.w = ax.c;
-        put_quad (sx[c0], sx[c0 ^ 1], W*M + 2*idx, vx);
+        put_quad (sx(c0), sx(c0 ^ 1), W*M + 2*idx, vx);
       }
       else {
         const int p = idx - QW, c = (base + p + W) & 1;
-        sy[c][p*MY + W/2] = ay.p ? ay.p[cidx<2> (g, i0 + p, fj, 0)] : ay.c;
+        sy(c)[p*MY + W/2] = ay.p ? ay.p[cidx<2> (g, i0 + p, fj, 0)] : ay.c;
       }
     }
   }
@@ -235,9 +236,9 @@ k_relax_tile2d (bmg_geom g, T * __restrict__ out, const T * __restrict__ in,
     const int ri = real_index (i0 + p, n, px), rj = real_index (j0 + q, n, py);
     const bool ok = ri >= 0 && rj >= 0;
     const long long id = ok ? cidx<2> (g, ri, rj, 0) : 0;
-    cp_async_elem (&sa[c][p*M + m], in + id, ok);
-    cp_async_elem (&sr[c][p*M + m], res + id, ok);
-    if (LAM) cp_async_elem (&sl[c][p*M + m], lam.p + id, ok);
+    cp_async_elem (&sa(c)[p*M + m], in + id, ok);
+    cp_async_elem (&sr(c)[p*M + m], res + id, ok);
+    if (LAM) cp_async_elem (&sl(c)[p*M + m], lam.p + id, ok);
   }
   /* x faces: W+1 rows of W (face (p, q): lower face of cell (p, q)) */
   for (int idx = tid; idx < (W + 1)*W; idx += nth) {
@@ -245,8 +246,8 @@ k_relax_tile2d (bmg_geom g, T * __restrict__ out, const T * __restrict__ in,
     const int c = (base + p + q) & 1;
     const int fi = real_face (i0 + p, n, px), rj = real_index (j0 + q, n, py);
     const bool ok = fi >= 0 && rj >= 0;
-    if (ax.p) cp_async_elem (&sx[c][p*M + (q >> 1)], ax.p + (ok ? cidx<2> (g, fi, rj, 0) : 0), ok);
-    else sx[c][p*M + (q >> 1)] = ok ? ax.c : T(0);
+    if (ax.p) cp_async_elem (&sx(c)[p*M + (q >> 1)], ax.p + (ok ? cidx<2> (g, fi, rj, 0) : 0), ok);
+    else sx(c)[p*M + (q >> 1)] = ok ? ax.c : T(0);
   }
   /* y faces: W rows of W+1 (face (p, q): left face of cell (p, q)) */
   for (int idx = tid; idx < W*(W + 1); idx += nth) {
@@ -254,8 +255,8 @@ k_relax_tile2d (bmg_geom g, T * __restrict__ out, const T * __restrict__ in,
     const int c = (base + p + q) & 1;
     const int ri = real_index (i0 + p, n, px), fj = real_face (j0 + q, n, py);
     const bool ok = ri >= 0 && fj >= 0;
-    if (ay.p) cp_async_elem (&sy[c][p*MY + (q >> 1)], ay.p + (ok ? cidx<2> (g, ri, fj, 0) : 0), ok);
-    else sy[c][p*MY + (q >> 1)] = ok ? ay.c : T(0);
+    if (ay.p) cp_async_elem (&sy(c)[p*MY + (q >> 1)], ay.p + (ok ? cidx<2> (g, ri, fj, 0) : 0), ok);
+    else sy(c)[p*MY + (q >> 1)] = ok ? ay.c : T(0);
   }
   }
   cp_async_wait_all ();
@@ -281,7 +282,7 @@ k_relax_tile2d (bmg_geom g, T * __restrict__ out, const T * __restrict__ in,
       if (line < 2 ? real_index (j0 + q, n, py) < 0 : real_index (i0 + p, n, px) < 0)
         continue;
       const int c = (base + p + q) & 1;
-      sa[c][p*M + (q >> 1)] = sa[c ^ 1][pm*M + (qm >> 1)]*T(f);
+      sa(c)[p*M + (q >> 1)] = sa(c ^ 1)[pm*M + (qm >> 1)]*T(f);
     }
   };
   if (has_ghosts) refresh ();
@@ -289,15 +290,16 @@ k_relax_tile2d (bmg_geom g, T * __restrict__ out, const T * __restrict__ in,
 
   const T D2 = Delta*Delta;
   for (int sw = 0; sw < nsweeps; sw++)
+#pragma unroll
     for (int c = 0; c < 2; c++) {
       const int k = 2*sw + c;
       const int lo = k + 1, hi = W - k - 1;      /* valid update region [lo, hi)^2 */
-      const T * __restrict__ o_a = sa[c ^ 1];
-      const T * __restrict__ xr = sx[c], * __restrict__ xo = sx[c ^ 1];
-      const T * __restrict__ yr = sy[c], * __restrict__ yo = sy[c ^ 1];
-      T * __restrict__ a = sa[c];
-      const T * __restrict__ r = sr[c];
-      const T * __restrict__ l = sl[c];
+      const T * __restrict__ o_a = sa(c ^ 1);
+      const T * __restrict__ xr = sx(c), * __restrict__ xo = sx(c ^ 1);
+      const T * __restrict__ yr = sy(c), * __restrict__ yo = sy(c ^ 1);
+      T * __restrict__ a = sa(c);
+      const T * __restrict__ r = sr(c);
+      const T * __restrict__ l = sl(c);
       /* thread (tx, ty): cells m0 = 2 tx and m0 + 1 of colour c in row lo + pr;
          a warp covers RW rows of one parity (pr interleaves them), so the
          colour offset o, and every branch on it, is uniform per warp */
@@ -363,8 +365,8 @@ k_relax_tile2d (bmg_geom g, T * __restrict__ out, const T * __restrict__ in,
       const int rr = idx/QT, k = idx - rr*QT;
       const int p = rr + H, q = H + 4*k, c0 = (base + p + q) & 1, m = q >> 1;
       Quad<T> v;
-      v.x = sa[c0][p*M + m]; v.z = sa[c0][p*M + m + 1];
-      v.y = sa[c0 ^ 1][p*M + m]; v.w = sa[c0 ^ 1][p*M + m + 1];
+      v.x = sa(c0)[p*M + m]; v.z = sa(c0)[p*M + m + 1];
+      v.y = sa(c0 ^ 1)[p*M + m]; v.w = sa(c0 ^ 1)[p*M + m + 1];
       store_quad (out + cidx<2> (g, blockIdx.y*TS + rr, blockIdx.x*TS + 4*k, 0), v);
     }
     return;
@@ -374,7 +376,7 @@ k_relax_tile2d (bmg_geom g, T * __restrict__ out, const T * __restrict__ in,
     const int gi = blockIdx.y*TS + rr, gj = blockIdx.x*TS + s;
     if (gi >= n || gj >= n) continue;
     const int p = rr + H, q = s + H;
-    const T v = sa[(base + p + q) & 1][p*M + (q >> 1)];
+    const T v = sa((base + p + q) & 1)[p*M + (q >> 1)];
     out[cidx<2> (g, gi, gj, 0)] = v;
     ghosts_homog<2, T> (out, g, gi, gj, 0, v, bc);
   }
