@@ -109,6 +109,17 @@ struct TileShape {
 __device__ __forceinline__ double relax_div (double n, double d) { return n/d; }
 __device__ __forceinline__ float relax_div (float n, float d) { return __fdividef (n, d); }
 
+/* n += x1 v1 + x0 v0: the reference's order in FP64, fused multiply-adds
+   in FP32 */
+__device__ __forceinline__ double tile_acc (double n, double x1, double v1, double x0, double v0)
+{
+  return n + (x1*v1 + x0*v0);
+}
+__device__ __forceinline__ float tile_acc (float n, float x1, float v1, float x0, float v0)
+{
+  return fmaf (x0, v0, fmaf (x1, v1, n));
+}
+
 template <typename T> struct Pair;
 template <> struct Pair<float> { typedef float2 type; };
 template <> struct Pair<double> { typedef double2 type; };
@@ -340,10 +351,10 @@ k_relax_tile2d (bmg_geom g, T * __restrict__ out, const T * __restrict__ in,
           /* relax_value's expression and order (poisson.h:303-319), two cells */
           T n0 = (-D2)*rr.x, d0 = (-lv.x)*D2;
           T n1 = (-D2)*rr.y, d1 = (-lv.y)*D2;
-          n0 += xu.x*dn.x + xl.x*up.x; d0 += xu.x + xl.x;
-          n1 += xu.y*dn.y + xl.y*up.y; d1 += xu.y + xl.y;
-          n0 += yr0*vm + yl.x*vl;      d0 += yr0 + yl.x;
-          n1 += yr1*vr + yl.y*vm;      d1 += yr1 + yl.y;
+          n0 = tile_acc (n0, xu.x, dn.x, xl.x, up.x); d0 += xu.x + xl.x;
+          n1 = tile_acc (n1, xu.y, dn.y, xl.y, up.y); d1 += xu.y + xl.y;
+          n0 = tile_acc (n0, yr0, vm, yl.x, vl);      d0 += yr0 + yl.x;
+          n1 = tile_acc (n1, yr1, vr, yl.y, vm);      d1 += yr1 + yl.y;
           const T a0 = relax_div (n0, d0), a1 = relax_div (n1, d1);
           if (ok0 && ok1) { T2 w; w.x = a0; w.y = a1; *(T2 *) &a[ci] = w; }
           else if (ok0) a[ci] = a0;
