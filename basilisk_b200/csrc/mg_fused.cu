@@ -92,7 +92,7 @@ struct TileShape {
   static constexpr int W = TS + 2*H;   /* staged cells per side (even) */
   static constexpr int M = W/2;        /* cells of one colour per row */
   static_assert (W % 2 == 0, "staged width must be even");
-  static constexpr int MY = M + 2;     /* y-face row pitch (even: aligned pairs) */
+  static constexpr int MY = M + 4;     /* y-face row pitch (16-byte aligned rows) */
   /* da, res, (lambda): 2 colours x W x M; alpha_x faces: 2 x (W+1) x M;
      alpha_y faces: 2 x W x MY */
   static constexpr size_t elems (bool lam)
@@ -165,17 +165,22 @@ __device__ __forceinline__ void put_quad (T * a0, T * a1, int off, const Quad<T>
   *(T2 *) (a1 + off) = o;
 }
 
-/* BX x BY threads: thread (tx, ty) updates the cell pair 2 tx, 2 tx + 1 of
-   row ty + lo in every colour pass */
-template <typename T, int TS, int S, bool LAM, int BX, int BY>
-__global__ void __launch_bounds__ (BX*BY)
+/* BX x BY threads: thread (tx, ty) updates the CPT cells CPT tx ..
+   CPT tx + CPT - 1 of each colour of row ty + lo in every colour pass
+   (CPT = 2 or 4); MINB CTAs per SM bound the registers */
+template <typename T> struct Vec4;
+template <> struct Vec4<float> { typedef float4 type; };
+
+template <typename T, int TS, int S, bool LAM, int BX, int BY, int CPT, int MINB>
+__global__ void __launch_bounds__ (BX*BY, MINB)
 k_relax_tile2d (bmg_geom g, T * __restrict__ out, const T * __restrict__ in,
                 const T * __restrict__ res, Coef<T> ax, Coef<T> ay, Coef<T> lam, T Delta, BCH bc,
                 int nsweeps)
 {
   typedef TileShape<T, TS, S> Sh;
   constexpr int H = Sh::H, W = Sh::W, M = Sh::M, MY = Sh::MY;
-  static_assert (M % 2 == 0 && M <= 2*BX && W - 2 <= BY, "one pair of cells per thread per row");
+  static_assert (M % CPT == 0 && M <= CPT*BX && W - 2 <= BY, "CPT cells per thread per row");
+  static_assert (CPT == 2 || (CPT == 4 && sizeof (T) == 4), "pairs, or quads of FP32 cells");
   typedef typename Pair<T>::type T2;
   extern __shared__ __align__ (16) unsigned char smem_raw[];
   /* the colour-c arrays, as offsets from one shared base (no pointer
@@ -311,11 +316,70 @@ k_relax_tile2d (bmg_geom g, T * __restrict__ out, const T * __restrict__ in,
       T * __restrict__ a = sa(c);
       const T * __restrict__ r = sr(c);
       const T * __restrict__ l = sl(c);
-      /* thread (tx, ty): cells m0 = 2 tx and m0 + 1 of colour c in row lo + pr;
-         a warp covers RW rows of one parity (pr interleaves them), so the
-         colour offset o, and every branch on it, is uniform per warp */
+      /* thread (tx, ty): cells m0 = CPT tx .. m0 + CPT - 1 of colour c in row
+         lo + pr; a warp covers RW rows of one parity (pr interleaves them),
+         so the colour offset o, and every branch on it, is uniform per warp */
       const int p = lo + pr;
-      if (p < hi) {
+      if constexpr (CPT == 4) {
+        typedef typename Vec4<T>::type T4;
+        if (p < hi) {
+          const int o = (c - base - p) & 1;
+          const int mlo = (lo - o + 1) >> 1, mhi = (hi - o + 1) >> 1;
+          const int m0 = 4*tx;
+          bool ok[4];
+#pragma unroll
+          for (int e = 0; e < 4; e++) ok[e] = m0 + e >= mlo && m0 + e < mhi;
+          if (!inner) {
+            const int gi = i0 + p, gj = j0 + 2*m0 + o;
+            const bool rowok = px || (unsigned) gi < (unsigned) n;
+#pragma unroll
+            for (int e = 0; e < 4; e++)
+              ok[e] = ok[e] && rowok && (py || (unsigned) (gj + 2*e) < (unsigned) n);
+          }
+          if (ok[0] || ok[1] || ok[2] || ok[3]) {
+            const int ci = p*M + m0;
+            const T4 up = *(const T4 *) &o_a[ci - M], dn = *(const T4 *) &o_a[ci + M];
+            const T4 mid = *(const T4 *) &o_a[ci];
+            /* the other colour's cells [m0 - 1 + o .. m0 + 3 + o]: cell e has
+               v[e] on its left and v[e + 1] on its right */
+            T v[5];
+            if (o == 0) { v[0] = o_a[ci - 1]; v[1] = mid.x; v[2] = mid.y; v[3] = mid.z; v[4] = mid.w; }
+            else { v[0] = mid.x; v[1] = mid.y; v[2] = mid.z; v[3] = mid.w; v[4] = o_a[ci + 4]; }
+            const T4 rr = *(const T4 *) &r[ci];
+            const T4 xl = *(const T4 *) &xr[ci], xu = *(const T4 *) &xo[ci + M];
+            const T4 yl = *(const T4 *) &yr[p*MY + m0], y4 = *(const T4 *) &yo[p*MY + m0];
+            T yrv[4];
+            if (o == 0) { yrv[0] = y4.x; yrv[1] = y4.y; yrv[2] = y4.z; yrv[3] = y4.w; }
+            else { yrv[0] = y4.y; yrv[1] = y4.z; yrv[2] = y4.w; yrv[3] = yo[p*MY + m0 + 4]; }
+            T4 lv;
+            if (LAM) lv = *(const T4 *) &l[ci];
+            else { lv.x = lam.c; lv.y = lam.c; lv.z = lam.c; lv.w = lam.c; }
+            const T rrv[4] = {rr.x, rr.y, rr.z, rr.w}, lvv[4] = {lv.x, lv.y, lv.z, lv.w};
+            const T xlv[4] = {xl.x, xl.y, xl.z, xl.w}, xuv[4] = {xu.x, xu.y, xu.z, xu.w};
+            const T ylv[4] = {yl.x, yl.y, yl.z, yl.w};
+            const T upv[4] = {up.x, up.y, up.z, up.w}, dnv[4] = {dn.x, dn.y, dn.z, dn.w};
+            T out[4];
+#pragma unroll
+            for (int e = 0; e < 4; e++) {
+              /* relax_value's expression (poisson.h:303-319) */
+              T nn = (-D2)*rrv[e], d = (-lvv[e])*D2;
+              nn = tile_acc (nn, xuv[e], dnv[e], xlv[e], upv[e]); d += xuv[e] + xlv[e];
+              nn = tile_acc (nn, yrv[e], v[e + 1], ylv[e], v[e]); d += yrv[e] + ylv[e];
+              out[e] = relax_div (nn, d);
+            }
+            if (ok[0] && ok[1] && ok[2] && ok[3]) {
+              T4 w; w.x = out[0]; w.y = out[1]; w.z = out[2]; w.w = out[3];
+              *(T4 *) &a[ci] = w;
+            }
+            else {
+#pragma unroll
+              for (int e = 0; e < 4; e++)
+                if (ok[e]) a[ci + e] = out[e];
+            }
+          }
+        }
+      }
+      else if (p < hi) {
         const int o = (c - base - p) & 1;        /* column offset of colour c */
         const int mlo = (lo - o + 1) >> 1, mhi = (hi - o + 1) >> 1;
         const int m0 = 2*tx;
@@ -808,7 +872,7 @@ __global__ void __launch_bounds__ (1024, 1) k_bottom (const __grid_constant__ Bo
     bot_copy_st<DIM> (P.lv[m].st, P.lv[m].g, P.lv[m].da, P.sm[m].gs, sm_at (bsm, P.sm[m].off_da), 0);
 }
 
-template <typename T, int TS, int S, bool LAM, int BX, int BY>
+template <typename T, int TS, int S, bool LAM, int BX, int BY, int CPT, int MINB>
 int launch_tile_v (bmg_geom g, void * out, const void * in, const void * res,
                    const bmg_coef * alpha, bmg_coef lambda, double Delta, BCH h, int nsweeps,
                    cudaStream_t s)
@@ -821,26 +885,26 @@ int launch_tile_v (bmg_geom g, void * out, const void * in, const void * res,
   cudaGetDevice (&dev);
   if (dev < 0 || dev >= 64) return (int) cudaErrorInvalidDevice;
   if (!configured[dev]) {
-    cudaError_t e = cudaFuncSetAttribute (k_relax_tile2d<T, TS, S, LAM, BX, BY>,
+    cudaError_t e = cudaFuncSetAttribute (k_relax_tile2d<T, TS, S, LAM, BX, BY, CPT, MINB>,
                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int) bytes);
     if (e != cudaSuccess) return (int) e;
     configured[dev] = 1;
   }
   dim3 grid ((g.n + TS - 1)/TS, (g.n + TS - 1)/TS, 1);
-  k_relax_tile2d<T, TS, S, LAM, BX, BY><<<grid, dim3 (BX, BY, 1), bytes, s>>>
+  k_relax_tile2d<T, TS, S, LAM, BX, BY, CPT, MINB><<<grid, dim3 (BX, BY, 1), bytes, s>>>
     (g, (T *) out, (const T *) in, (const T *) res, coef_of<T> (alpha[0]), coef_of<T> (alpha[1]),
      coef_of<T> (lambda), (T) Delta, h, nsweeps);
   return 0;
 }
 
-template <typename T, int TS, int S, int BX, int BY>
+template <typename T, int TS, int S, int BX, int BY, int CPT = 2, int MINB = 1>
 int launch_tile (bmg_geom g, void * out, const void * in, const void * res,
                  const bmg_coef * alpha, bmg_coef lambda, double Delta, BCH h, int nsweeps,
                  cudaStream_t s)
 {
   if (lambda.p)
-    return launch_tile_v<T, TS, S, true, BX, BY> (g, out, in, res, alpha, lambda, Delta, h, nsweeps, s);
-  return launch_tile_v<T, TS, S, false, BX, BY> (g, out, in, res, alpha, lambda, Delta, h, nsweeps, s);
+    return launch_tile_v<T, TS, S, true, BX, BY, CPT, MINB> (g, out, in, res, alpha, lambda, Delta, h, nsweeps, s);
+  return launch_tile_v<T, TS, S, false, BX, BY, CPT, MINB> (g, out, in, res, alpha, lambda, Delta, h, nsweeps, s);
 }
 
 } // namespace
@@ -867,7 +931,7 @@ int bmg_launch_relax_tile (int dim, int st, bmg_geom g, void * out, const void *
       : launch_tile<double, 40, 4, 16, 64> (g, out, in, res, alpha, lambda, Delta, h, nsweeps, s);
   else
     e = small ? launch_tile<float, 16, 4, 8, 32> (g, out, in, res, alpha, lambda, Delta, h, nsweeps, s)
-      : launch_tile<float, 48, 4, 16, 64> (g, out, in, res, alpha, lambda, Delta, h, nsweeps, s);
+      : launch_tile<float, 48, 4, 8, 64, 4, 3> (g, out, in, res, alpha, lambda, Delta, h, nsweeps, s);
   if (e) return e;
   cudaError_t r = cudaGetLastError ();
   return r == cudaSuccess ? 0 : (int) r;
