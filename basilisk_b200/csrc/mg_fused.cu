@@ -467,7 +467,7 @@ typedef bmg_bottom_level BotLevel;
 /* levels up to this size use the small relaxation tiles */
 #define BMG_SMALL_TILE_N 256
 /* staged levels up to this many padded cells are relaxed by one warp */
-#define BOT_WARP_CELLS 400
+#define BOT_WARP_CELLS 100
 
 /* a staged level: its global arrays and their shared-memory copies, which
    use a compact padded layout described by a bmg_geom of its own (pitch
@@ -711,7 +711,7 @@ __device__ __forceinline__ void bot_pass2d (const bmg_geom & g, T * a, const T *
 #pragma unroll
     for (int k = 0; k < K; k++)
       if (ids[k] >= 0) {
-        const T v = nn[k]/dd[k];
+        const T v = relax_div (nn[k], dd[k]);
         a[ids[k]] = v;
         ghosts_homog_2d<T> (a, g, is[k], js[k], v, bc);
       }
