@@ -247,9 +247,11 @@ def cpu_solve(prob, threads=None):
 
 def run_workload(args, ws, rank, local):
     """The other workloads of the scope table, one JSON line each (not the
-    headline): the quadtree problem (two_phase_tree, depth 11) and the 3D
-    periodic Helmholtz problem (helmholtz_3d, 256^3).  One step = one
-    poisson () solve from a = 0."""
+    headline): the quadtree problem (two_phase_tree, depth 11), the 3D
+    periodic Helmholtz problem (helmholtz_3d, 256^3), one step = one
+    poisson () solve from a = 0; and the differentiable batch
+    (random_field_batch, 16 x 512^2), one step = a forward and backward pass
+    through basilisk_b200.autograd."""
     import torch
     import basilisk_b200 as bmg
     from basilisk_b200 import problems
@@ -274,6 +276,50 @@ def run_workload(args, ws, rank, local):
                               "level 11 (%d leaves), tolerance 1e-6, at most 100 V-cycles"
                               % g.leaves,
                   "grid": "quadtree levels 5-11", "relax": "red-black Gauss-Seidel",
+                  "parallelism": "replicas" if ws > 1 else "1 gpu"}
+    elif args.workload == "random_field_batch":
+        from basilisk_b200.autograd import Problem, solve as dsolve
+        B, depth = 16, 9
+        pr = Problem(2, depth, periodic=(0, 1), tolerance=1e-8, precision=args.precision)
+        g = pr.grid
+        g.set_stream(torch.cuda.current_stream().cuda_stream)
+        inst = [problems.random_field_2d(depth, seed=3 + rank, instance=k) for k in range(2*B)]
+        dev = lambda x: torch.tensor(np.stack(x), dtype=torch.float64, device="cuda")
+        kappa = dev([d["kappa"] for d in inst[:B]])
+        b = dev([d["b"] for d in inst[:B]])
+        b = b - b.mean(dim=(1, 2), keepdim=True)
+
+        def face_exp(k):
+            """alpha = exp(mean of the two cell kappas) on every face, periodic
+            (face n is the image of face 0)"""
+            kx = torch.cat([k[:, -1:], k, k[:, :1]], dim=1)
+            ky = torch.cat([k[:, :, -1:], k, k[:, :, :1]], dim=2)
+            return [torch.exp((kx[:, :-1] + kx[:, 1:]) / 2), torch.exp((ky[:, :, :-1] + ky[:, :, 1:]) / 2)]
+        with torch.no_grad():
+            a_obs = dsolve(pr, b, alpha=face_exp(dev([d["kappa"] for d in inst[B:]])))
+            a_obs = a_obs - a_obs.mean(dim=(1, 2), keepdim=True)
+        tol, dtype = 1e-8, "f64" if args.precision == "fp64" else "f32+f64"
+        grads = {}
+
+        def reset():
+            pass
+
+        def solve():
+            k = kappa.clone().requires_grad_(True)
+            a_ = dsolve(pr, b, alpha=face_exp(k))
+            a_ = a_ - a_.mean(dim=(1, 2), keepdim=True)
+            loss = 0.5 * ((a_ - a_obs) ** 2).sum()
+            loss.backward()
+            grads["kappa"] = k.grad
+            st = dict(pr.stats[-1]) if pr.stats else {"i": 0, "resb": 0, "resa": 0, "nrelax": 0}
+            return st
+        config = {"workload": "random_field_batch: 16 independent 512^2 periodic Poisson solves, "
+                              "alpha = exp(kappa) on faces (kappa a Gaussian random field, "
+                              "length 0.05), b zero-mean bumps; one step = forward solves + "
+                              "adjoint solves + face gradients of L = 1/2 |a - a_obs|^2 "
+                              "w.r.t. kappa, tolerance 1e-8",
+                  "grid": "16 x 512^2 (depth 9)", "form": args.precision,
+                  "relax": "red-black Gauss-Seidel",
                   "parallelism": "replicas" if ws > 1 else "1 gpu"}
     else:
         prob = problems.helmholtz_3d(depth=8, seed=2 + rank)
@@ -319,8 +365,10 @@ def run_workload(args, ws, rank, local):
     ms = max_over_ranks(ws, sum(times) / len(times))
     if rank != 0:
         return
+    unit = "gradient steps/s (16 instances each)" if args.workload == "random_field_batch" \
+        else "solves/s"
     line = {"metric": "time-to-residual, %s" % args.workload, "value": ws * 1e3 / ms,
-            "unit": "solves/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "unit": unit, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": dtype, "data": "synthetic", "config": config,
             "mgstats": {k: st[k] for k in ("i", "resb", "resa", "nrelax")},
@@ -389,11 +437,12 @@ def main():
     ap.add_argument("--profile", choices=["fp64", "mixed"], default=None,
                     help="profiling run: only this form, no e2e, no CPU baseline, no JSON")
     ap.add_argument("--depth", type=int, default=DEPTH, help="grid depth (profiling runs)")
-    ap.add_argument("--workload", choices=["two_phase_2d", "two_phase_tree", "helmholtz_3d"],
+    ap.add_argument("--workload", choices=["two_phase_2d", "two_phase_tree", "helmholtz_3d",
+                                           "random_field_batch"],
                     default="two_phase_2d",
                     help="two_phase_2d: the headline; the others print their own line")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64",
-                    help="form of the helmholtz_3d workload")
+                    help="form of the helmholtz_3d and random_field_batch workloads")
     args = ap.parse_args()
     ws, rank, local = dist_init()
     if args.impl == "bmg" and args.workload != "two_phase_2d":
