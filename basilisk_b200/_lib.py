@@ -53,6 +53,12 @@ class Poisson(ctypes.Structure):
                 ("res", ctypes.POINTER(bmg_scalar))]
 
 
+class Project(ctypes.Structure):
+    """``struct Project`` of poisson.h:461-467."""
+    _fields_ = [("uf", bmg_vector), ("p", bmg_scalar), ("alpha", bmg_vector),
+                ("dt", ctypes.c_double), ("nrelax", ctypes.c_int)]
+
+
 RELAX_FN = ctypes.CFUNCTYPE(None, ctypes.POINTER(bmg_scalar), ctypes.POINTER(bmg_scalar),
                             ctypes.c_int, ctypes.c_void_p)
 # int (*) (int level, double x, double y, double z, void * data)
@@ -115,6 +121,8 @@ SIGNATURES = {
     "bmg_bc": (I, [P, bmg_scalar, I, I, D, DP, I]),
     "poisson": (mgstats, [Poisson]),
     "bmg_poisson": (I, [P, Poisson, ctypes.POINTER(mgstats)]),
+    "project": (mgstats, [Project]),
+    "bmg_project": (I, [P, Project, ctypes.POINTER(mgstats)]),
     "bmg_relax": (None, [ctypes.POINTER(bmg_scalar), ctypes.POINTER(bmg_scalar), I, P]),
     "bmg_residual": (D, [ctypes.POINTER(bmg_scalar), ctypes.POINTER(bmg_scalar),
                          ctypes.POINTER(bmg_scalar), P]),

@@ -55,6 +55,7 @@ struct bmg_grid {
   cudaEvent_t ev0, ev1, evr0, evr1;
   struct graph_entry * graphs;     /* captured V-cycles, see run_cycle() */
   struct bmg_tree * tree;          /* quadtree over the levels, or NULL */
+  int div_h;                       /* handle of project ()'s div field, 0 = none yet */
   unsigned long long clock;
 };
 

@@ -1121,6 +1121,63 @@ mgstats poisson (struct Poisson p)
   return s;
 }
 
+/* project (poisson.h:468-509): div = (sum of uf.x[1] - uf.x[])/(dt Delta),
+   poisson (p, div, alpha, tolerance = TOLERANCE/sq(dt), nrelax), then
+   uf.x[] -= dt alpha.x[] face_gradient_x (p, 0) on every face */
+int bmg_project (bmg_grid * g, struct Project q, mgstats * out)
+{
+  mgstats zero;
+  memset (&zero, 0, sizeof zero);
+  if (out) *out = zero;
+  if (!g || !out) return fail (BMG_EINVAL);
+  if (g->tree) return fail (BMG_EUNSUPPORTED);
+  CK (cudaSetDevice (g->device));
+  const int L = g->depth;
+  /* scalar div[] (poisson.h:482): one field of the grid, created on first
+     use (before any field pointer is taken: creation may move the table) */
+  if (!g->div_h) {
+    int r = new_field (g, -1, 0, 0., &g->div_h);
+    if (r) return fail (r);
+  }
+  field_t * p, * div = field_get (g, g->div_h);
+  if (!div || check_cell (g, q.p.i, &p)) return fail (BMG_EINVAL);
+  const int uh[3] = {q.uf.x.i, q.uf.y.i, q.uf.z.i};
+  double * u[3] = {NULL, NULL, NULL};
+  for (int d = 0; d < g->dim; d++) {
+    field_t * f = field_get (g, uh[d]);
+    if (!f || f->face_dim != d || f->is_const) return fail (BMG_EINVAL);
+    u[d] = f->lv[L];
+  }
+  const double dt = q.dt ? q.dt : 1.;
+  const int nrelax = q.nrelax ? q.nrelax : 4;
+  CL (bmg_launch_divergence (g->dim, g->g64[L], (const double * const *) u, dt, delta_of (g, L),
+                             div->lv[L], g->stream));
+  struct Poisson pp;
+  memset (&pp, 0, sizeof pp);
+  pp.a = q.p;
+  pp.b.i = g->div_h;
+  pp.alpha = q.alpha;
+  pp.tolerance = TOLERANCE/(dt*dt);
+  pp.nrelax = nrelax;
+  int r = bmg_poisson (g, pp, out);
+  if (r != BMG_OK && r != BMG_ENOTCONV) return fail (r);
+  coefs_t c;
+  bmg_scalar nolambda = {0};
+  if (resolve_coefs (g, q.alpha, nolambda, &c)) return fail (BMG_EINVAL);
+  for (int d = 0; d < g->dim; d++)
+    CL (bmg_launch_project_faces (g->dim, g->g64[L], d, u[d], c.alpha64[L][d], p->lv[L], dt,
+                                  delta_of (g, L), g->stream));
+  CK (cudaStreamSynchronize (g->stream));
+  return fail (r);
+}
+
+mgstats project (struct Project q)
+{
+  mgstats s;
+  bmg_project (current_grid, q, &s);
+  return s;
+}
+
 /* bmg_relax / bmg_residual: the Poisson callbacks (poisson.h:271-391) */
 void bmg_relax (bmg_scalar * da, bmg_scalar * res, int l, void * data)
 {

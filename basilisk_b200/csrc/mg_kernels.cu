@@ -632,6 +632,49 @@ __global__ void k_adjoint_cells (bmg_geom g, const double * __restrict__ mu,
   out[q] = -mu[id]*a[id];
 }
 
+/* project (poisson.h:468-509), first step: div = sum over dimensions of
+   uf.x[1] - uf.x[], over dt Delta (poisson.h:482-487) */
+template <int DIM>
+__global__ void k_divergence (bmg_geom g, const double * __restrict__ ux,
+                              const double * __restrict__ uy, const double * __restrict__ uz,
+                              double dt, double Delta, double * __restrict__ div)
+{
+  int i, j, k;
+  if (!cell_of_thread<DIM> (g.n, i, j, k)) return;
+  const long long id = cidx<DIM> (g, i, j, k);
+  double d = 0.;
+  d += ux[id + cstride<DIM> (g, 0)] - ux[id];
+  if (DIM > 1) d += uy[id + cstride<DIM> (g, 1)] - uy[id];
+  if (DIM > 2) d += uz[id + cstride<DIM> (g, 2)] - uz[id];
+  d /= dt*Delta;
+  div[id] = d;
+}
+
+/* project, last step: uf.x[] -= dt alpha.x[] face_gradient_x (p, 0) on
+   every face of direction e, faces 0..n along e (foreach_face,
+   multigrid.h:255-320) */
+template <int DIM>
+__global__ void k_project_faces (bmg_geom g, int e, double * __restrict__ u, Coef<double> al,
+                                 const double * __restrict__ p, double dt, double Delta)
+{
+  const int n = g.n, ne = n + 1;
+  const long long total = DIM == 1 ? ne : DIM == 2 ? (long long) ne*n : (long long) ne*n*n;
+  for (long long q = (long long) blockIdx.x*blockDim.x + threadIdx.x; q < total;
+       q += (long long) gridDim.x*blockDim.x) {
+    int c[3] = {0, 0, 0};
+    long long r = q;
+    for (int d = DIM - 1; d >= 0; d--) {
+      const int ext = d == e ? ne : n;
+      c[d] = (int) (r % ext);
+      r /= ext;
+    }
+    const long long id = cidx<DIM> (g, c[0], c[1], c[2]);
+    const long long st = cstride<DIM> (g, e);
+    const double a = al.p ? al.p[id] : al.c;
+    u[id] -= dt*a*((p[id] - p[id - st])/Delta);
+  }
+}
+
 } // namespace
 
 
@@ -861,6 +904,29 @@ int bmg_launch_adjoint_cells (int dim, bmg_geom g, const double * mu, const doub
   if (dim == 1) k_adjoint_cells<1><<<grid_shape<1> (g.n), block_shape<1> (), 0, s>>> (g, mu, a, out);
   else if (dim == 2) k_adjoint_cells<2><<<grid_shape<2> (g.n), block_shape<2> (), 0, s>>> (g, mu, a, out);
   else k_adjoint_cells<3><<<grid_shape<3> (g.n), block_shape<3> (), 0, s>>> (g, mu, a, out);
+  return status_of_launch ();
+}
+
+int bmg_launch_divergence (int dim, bmg_geom g, const double * const * uf, double dt,
+                           double Delta, double * div, cudaStream_t s)
+{
+  const double * ux = uf[0], * uy = dim > 1 ? uf[1] : NULL, * uz = dim > 2 ? uf[2] : NULL;
+  if (dim == 1) k_divergence<1><<<grid_shape<1> (g.n), block_shape<1> (), 0, s>>> (g, ux, uy, uz, dt, Delta, div);
+  else if (dim == 2) k_divergence<2><<<grid_shape<2> (g.n), block_shape<2> (), 0, s>>> (g, ux, uy, uz, dt, Delta, div);
+  else k_divergence<3><<<grid_shape<3> (g.n), block_shape<3> (), 0, s>>> (g, ux, uy, uz, dt, Delta, div);
+  return status_of_launch ();
+}
+
+int bmg_launch_project_faces (int dim, bmg_geom g, int e, double * u, bmg_coef alpha,
+                              const double * p, double dt, double Delta, cudaStream_t s)
+{
+  long long total = (long long) (g.n + 1);
+  for (int d = 1; d < dim; d++) total *= g.n;
+  const int nb = lin_blocks (total);
+  const Coef<double> al = coef_of<double> (alpha);
+  if (dim == 1) k_project_faces<1><<<nb, 256, 0, s>>> (g, e, u, al, p, dt, Delta);
+  else if (dim == 2) k_project_faces<2><<<nb, 256, 0, s>>> (g, e, u, al, p, dt, Delta);
+  else k_project_faces<3><<<nb, 256, 0, s>>> (g, e, u, al, p, dt, Delta);
   return status_of_launch ();
 }
 

@@ -144,6 +144,13 @@ int bmg_launch_bottom (int dim, const bmg_bottom_level * lv, int nlev, bmg_geom 
 /* number of partial sums bmg_launch_sum needs for a level */
 int bmg_sum_partials (int dim, bmg_geom g);
 
+/* project (poisson.h:468-509): the divergence of a face vector over
+   dt Delta, and the face correction uf -= dt alpha grad p of direction e */
+int bmg_launch_divergence (int dim, bmg_geom g, const double * const * uf, double dt,
+                           double Delta, double * div, cudaStream_t s);
+int bmg_launch_project_faces (int dim, bmg_geom g, int e, double * u, bmg_coef alpha,
+                              const double * p, double dt, double Delta, cudaStream_t s);
+
 #ifdef __cplusplus
 }
 #endif

@@ -278,6 +278,24 @@ class Grid:
         d["status"] = status
         return d
 
+    def project(self, uf, p, alpha=None, dt=0.0, nrelax=0):
+        """``project (uf, p, alpha, dt, nrelax)`` (poisson.h:468-509): makes
+        the face vector uf discretely divergence-free with the pressure p;
+        returns the mgstats of the pressure solve as a dict (plus ``status``)."""
+        L = _lib.load()
+        q = _lib.Project()
+        q.uf, q.p = uf.vector, p.scalar
+        if alpha is not None:
+            q.alpha = alpha.vector
+        q.dt, q.nrelax = dt, nrelax
+        st = _lib.mgstats()
+        status = L.bmg_project(self.ptr, q, ctypes.byref(st))
+        if status not in (_lib.OK, _lib.ENOTCONV):
+            check(status, "bmg_project")
+        d = st.as_dict()
+        d["status"] = status
+        return d
+
     def mg_solve(self, a, b, alpha=None, lambda_=None, tolerance=0.0, nrelax=0, minlevel=0,
                  res=None):
         """``mg_solve`` (poisson.h:139-235) with the Poisson callbacks; unlike

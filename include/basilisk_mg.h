@@ -152,6 +152,21 @@ struct Poisson {
 mgstats poisson (struct Poisson p);
 /* the same on a given grid, returning a status */
 int bmg_poisson (bmg_grid * grid, struct Poisson p, mgstats * stats);
+/* struct Project (poisson.h:461-467), same members and order */
+struct Project {
+  bmg_vector uf;         /* face velocity, corrected in place */
+  bmg_scalar p;          /* pressure, solved in place */
+  bmg_vector alpha;      /* 0 = unityf */
+  double dt;             /* 0 = 1 */
+  int nrelax;            /* 0 = 4 */
+};
+/* project (poisson.h:468-509) on the current grid: div of uf over dt Delta,
+   poisson (p, div, alpha, tolerance = TOLERANCE/dt^2, nrelax), then
+   uf -= dt alpha grad p on every face.  Status: bmg_last_error ().
+   Uniform grids only (BMG_EUNSUPPORTED on a tree). */
+mgstats project (struct Project q);
+int bmg_project (bmg_grid * grid, struct Project q, mgstats * stats);
+
 
 /* the Poisson--Helmholtz callbacks (poisson.h:271-391); data is a
    struct Poisson *.  These are the only callbacks mg_solve/mg_cycle accept:

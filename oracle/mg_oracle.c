@@ -58,7 +58,7 @@ struct og_grid {
   double bcconst[6];
   double * bcval[6];          /* finest-level values, NULL = bcconst */
   int relax_mode;
-  field a, b, res, da, c, lambda, alpha[DIM];
+  field a, b, res, da, c, lambda, alpha[DIM], uf[DIM];
   int alpha_const, lambda_const;
   double alpha_c, lambda_c;
 };
@@ -119,11 +119,14 @@ static field * field_of (og_grid * g, int which)
   case OG_LAMBDA: return &g->lambda;
   case OG_DA: return &g->da;
   case OG_ALPHA_X: return &g->alpha[0];
+  case OG_UF_X: return &g->uf[0];
 #if DIM > 1
   case OG_ALPHA_Y: return &g->alpha[1];
+  case OG_UF_Y: return &g->uf[1];
 #endif
 #if DIM > 2
   case OG_ALPHA_Z: return &g->alpha[2];
+  case OG_UF_Z: return &g->uf[2];
 #endif
   }
   return NULL;
@@ -138,7 +141,7 @@ og_grid * og_new (int depth, double L0, double X0, double Y0, double Z0)
   for (int d = 0; d < 6; d++) g->bctype[d] = OG_NEUMANN; /* symmetry */
   field_alloc (g, &g->a); field_alloc (g, &g->b); field_alloc (g, &g->res);
   field_alloc (g, &g->da); field_alloc (g, &g->c); field_alloc (g, &g->lambda);
-  for (int d = 0; d < DIM; d++) field_alloc (g, &g->alpha[d]);
+  for (int d = 0; d < DIM; d++) { field_alloc (g, &g->alpha[d]); field_alloc (g, &g->uf[d]); }
   g->alpha_const = 1; g->alpha_c = 1.;   /* unityf, common.h:1276 */
   g->lambda_const = 1; g->lambda_c = 0.; /* zeroc, common.h:1277 */
   return g;
@@ -149,7 +152,7 @@ void og_free (og_grid * g)
   if (!g) return;
   field_free (g, &g->a); field_free (g, &g->b); field_free (g, &g->res);
   field_free (g, &g->da); field_free (g, &g->c); field_free (g, &g->lambda);
-  for (int d = 0; d < DIM; d++) field_free (g, &g->alpha[d]);
+  for (int d = 0; d < DIM; d++) { field_free (g, &g->alpha[d]); field_free (g, &g->uf[d]); }
   for (int d = 0; d < 6; d++) free (g->bcval[d]);
   free (g);
 }
@@ -346,8 +349,9 @@ static void copy_out (og_grid * g, const double * s, int l, double * v, int face
 
 static int face_dim_of (int which)
 {
-  return which == OG_ALPHA_X ? 0 : which == OG_ALPHA_Y ? 1 :
-    which == OG_ALPHA_Z ? 2 : -1;
+  return which == OG_ALPHA_X || which == OG_UF_X ? 0 :
+    which == OG_ALPHA_Y || which == OG_UF_Y ? 1 :
+    which == OG_ALPHA_Z || which == OG_UF_Z ? 2 : -1;
 }
 
 void og_set_field (og_grid * g, int which, const double * values)
@@ -357,7 +361,7 @@ void og_set_field (og_grid * g, int which, const double * values)
   int fd = face_dim_of (which);
   copy_in (g, f->lv[g->depth], g->depth, values, fd);
   if (fd >= 0) {
-    g->alpha_const = 0;
+    if (which >= OG_ALPHA_X && which <= OG_ALPHA_Z) g->alpha_const = 0;
     /* the automatic boundary of a dirty face vector copies periodic
        ghosts before the first stencil read (stencils.h:228+). */
     periodic_boundary (g, f->lv[g->depth], g->depth);
@@ -726,5 +730,45 @@ og_mgstats og_poisson (og_grid * g, double tolerance, int nrelax, int minlevel)
   og_mgstats s = og_mg_solve (g, 0., nrelax, minlevel > 1 ? minlevel : 1);
   if (tolerance)
     og_TOLERANCE = defaultol;
+  return s;
+}
+
+/* project (poisson.h:468-509) on the finest level: div = sum of the face
+   differences of uf over dt Delta, poisson (p, div, alpha, TOLERANCE/dt^2,
+   nrelax), then uf -= dt alpha grad p on every face (foreach_face visits
+   faces 0..n along their direction, multigrid.h:255-320) */
+og_mgstats og_project (og_grid * g, double dt, int nrelax)
+{
+  dt = dt ? dt : 1.;
+  nrelax = nrelax ? nrelax : 4;
+  const int l = g->depth, n = 1 << l, P = P_of (l);
+  const double Delta = g->L0*(1./(1 << l));
+  size_t st[3];
+  for (int e = 0; e < DIM; e++) st[e] = stride (P, e);
+  double * div = g->b.lv[l];
+  int J0 = DIM > 1 ? GH : 0, J1 = DIM > 1 ? n + GH : 1;
+  int K0 = DIM > 2 ? GH : 0, K1 = DIM > 2 ? n + GH : 1;
+  for (int i = GH; i < n + GH; i++)
+    for (int j = J0; j < J1; j++)
+      for (int k = K0; k < K1; k++) {
+        size_t id = IX (P, i, j, k);
+        double d = 0.;
+        for (int e = 0; e < DIM; e++)
+          d += g->uf[e].lv[l][id + st[e]] - g->uf[e].lv[l][id];
+        d /= dt*Delta;
+        div[id] = d;
+      }
+  og_mgstats s = og_poisson (g, og_TOLERANCE/sq_(dt), nrelax, 0);
+  const double * p = g->a.lv[l];
+  for (int e = 0; e < DIM; e++) {
+    double * u = g->uf[e].lv[l];
+    int I1 = n + GH + (e == 0), Jx = J1 + (e == 1 && DIM > 1), Kx = K1 + (e == 2 && DIM > 2);
+    for (int i = GH; i < I1; i++)
+      for (int j = J0; j < Jx; j++)
+        for (int k = K0; k < Kx; k++) {
+          size_t id = IX (P, i, j, k);
+          u[id] -= dt*ALPHA (e, l, id)*((p[id] - p[id - st[e]])/Delta);
+        }
+  }
   return s;
 }

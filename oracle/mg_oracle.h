@@ -49,7 +49,8 @@ typedef struct {
   int minlevel;
 } og_mgstats;
 
-enum { OG_A = 0, OG_B, OG_RES, OG_LAMBDA, OG_ALPHA_X, OG_ALPHA_Y, OG_ALPHA_Z, OG_DA };
+enum { OG_A = 0, OG_B, OG_RES, OG_LAMBDA, OG_ALPHA_X, OG_ALPHA_Y, OG_ALPHA_Z, OG_DA,
+       OG_UF_X, OG_UF_Y, OG_UF_Z };
 
 typedef struct og_grid og_grid;
 
@@ -74,6 +75,9 @@ double og_residual (og_grid * g);
 void og_mg_cycle (og_grid * g, int nrelax, int minlevel, int maxlevel);
 og_mgstats og_mg_solve (og_grid * g, double tolerance, int nrelax, int minlevel);
 og_mgstats og_poisson (og_grid * g, double tolerance, int nrelax, int minlevel);
+/* project (poisson.h:468-509): uf = the OG_UF_* face vector, p = OG_A, alpha
+   as set (unityf by default), div in OG_B; dt = 0 / nrelax = 0: defaults */
+og_mgstats og_project (og_grid * g, double dt, int nrelax);
 double og_sum_b (og_grid * g);
 /* level access for fine-grained tests: interior values of a level */
 void og_get_level (og_grid * g, int which, int level, double * out);

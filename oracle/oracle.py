@@ -21,7 +21,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 RIGHT, LEFT, TOP, BOTTOM, FRONT, BACK = range(6)
 NEUMANN, DIRICHLET, PERIODIC = 0, 1, 2
 RELAX_GS, RELAX_JACOBI, RELAX_RBGS = 0, 1, 2
-A, B, RES, LAMBDA, ALPHA_X, ALPHA_Y, ALPHA_Z, DA = range(8)
+A, B, RES, LAMBDA, ALPHA_X, ALPHA_Y, ALPHA_Z, DA, UF_X, UF_Y, UF_Z = range(11)
 
 
 class MGStats(ctypes.Structure):
@@ -70,6 +70,7 @@ def lib(dim):
         "og_mg_cycle": (None, [P, I, I, I]),
         "og_mg_solve": (MGStats, [P, D, I, I]),
         "og_poisson": (MGStats, [P, D, I, I]),
+        "og_project": (MGStats, [P, D, I]),
         "og_sum_b": (D, [P]),
         "og_get_level": (None, [P, I, I, DP]),
         "og_set_level": (None, [P, I, I, DP]),
@@ -186,6 +187,8 @@ class Grid:
     def get(self, which):
         if which in (ALPHA_X, ALPHA_Y, ALPHA_Z):
             shape = face_shape(self.n, self.dim, which - ALPHA_X)
+        elif which in (UF_X, UF_Y, UF_Z):
+            shape = face_shape(self.n, self.dim, which - UF_X)
         else:
             shape = (self.n,) * self.dim
         out = np.empty(shape, dtype=np.float64)
@@ -249,6 +252,17 @@ class Grid:
 
     def poisson(self, tolerance=0.0, nrelax=0, minlevel=0):
         return self.L.og_poisson(self.g, tolerance, nrelax, minlevel).as_dict()
+
+    def set_uf(self, comps):
+        for d, c in enumerate(comps):
+            self.set(UF_X + d, c)
+
+    def get_uf(self):
+        return [self.get(UF_X + d) for d in range(self.dim)]
+
+    def project(self, dt=0.0, nrelax=0):
+        """project (uf, p = a, alpha, dt, nrelax) (poisson.h:468-509)."""
+        return self.L.og_project(self.g, dt, nrelax).as_dict()
 
     def sum_b(self):
         return self.L.og_sum_b(self.g)

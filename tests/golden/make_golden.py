@@ -22,6 +22,7 @@ LOGS = {
     "poisson_1d":   ("test/poisson1D.c", "test/poisson1D.ref"),
     "circle_2d":    ("test/circle.c", "test/circle.ref"),
     "circle_variable_2d": ("test/circle-variable.c", "test/circle-variable.ref"),
+    "solenoidal_2d": ("test/solenoidal.c", "test/solenoidal.ref"),
 }
 
 
