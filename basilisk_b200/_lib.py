@@ -59,6 +59,13 @@ class Project(ctypes.Structure):
                 ("dt", ctypes.c_double), ("nrelax", ctypes.c_int)]
 
 
+class Viscosity(ctypes.Structure):
+    """``struct Viscosity`` of viscosity.h:3-10."""
+    _fields_ = [("u", bmg_vector), ("mu", bmg_vector), ("rho", bmg_scalar),
+                ("dt", ctypes.c_double), ("nrelax", ctypes.c_int),
+                ("res", ctypes.POINTER(bmg_scalar))]
+
+
 RELAX_FN = ctypes.CFUNCTYPE(None, ctypes.POINTER(bmg_scalar), ctypes.POINTER(bmg_scalar),
                             ctypes.c_int, ctypes.c_void_p)
 # int (*) (int level, double x, double y, double z, void * data)
@@ -122,6 +129,8 @@ SIGNATURES = {
     "poisson": (mgstats, [Poisson]),
     "bmg_poisson": (I, [P, Poisson, ctypes.POINTER(mgstats)]),
     "project": (mgstats, [Project]),
+    "viscosity": (mgstats, [Viscosity]),
+    "bmg_viscosity": (I, [P, Viscosity, ctypes.POINTER(mgstats)]),
     "bmg_project": (I, [P, Project, ctypes.POINTER(mgstats)]),
     "bmg_relax": (None, [ctypes.POINTER(bmg_scalar), ctypes.POINTER(bmg_scalar), I, P]),
     "bmg_residual": (D, [ctypes.POINTER(bmg_scalar), ctypes.POINTER(bmg_scalar),

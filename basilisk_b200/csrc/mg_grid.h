@@ -56,11 +56,13 @@ struct bmg_grid {
   struct graph_entry * graphs;     /* captured V-cycles, see run_cycle() */
   struct bmg_tree * tree;          /* quadtree over the levels, or NULL */
   int div_h;                       /* handle of project ()'s div field, 0 = none yet */
+  double * visc_ws;                /* viscosity (): da, res, w, r of each component */
   unsigned long long clock;
 };
 
 /* helpers of mg_host.c used by the tree layer */
 int bmg_i_fail (int status);                 /* sets bmg_last_error () */
+void bmg_i_bcdesc (const bmg_grid * g, const field_t * f, bmg_bcdesc * bc);
 field_t * bmg_i_field (bmg_grid * g, int handle);
 int bmg_i_workspace (bmg_grid * g);          /* FP64 da, da2, res on all levels */
 double * bmg_i_ws64 (bmg_grid * g, int which, int level);

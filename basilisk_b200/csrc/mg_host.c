@@ -200,7 +200,7 @@ void bmg_grid_free (bmg_grid * g)
       }
     }
   free (g->fields);
-  cudaFree (g->ws64); cudaFree (g->ws32); cudaFree (g->bproj);
+  cudaFree (g->ws64); cudaFree (g->ws32); cudaFree (g->bproj); cudaFree (g->visc_ws);
   cudaFree (g->d_maxres); cudaFree (g->d_partials); cudaFree (g->d_sum);
   cudaFreeHost (g->h_pinned);
   cudaEventDestroy (g->ev0); cudaEventDestroy (g->ev1);
@@ -589,6 +589,7 @@ static int ensure_workspace (bmg_grid * g, int mixed)
 }
 
 int bmg_i_fail (int status) { return fail (status); }
+void bmg_i_bcdesc (const bmg_grid * g, const field_t * f, bmg_bcdesc * bc) { bcdesc_of (g, f, bc); }
 field_t * bmg_i_field (bmg_grid * g, int handle) { return field_get (g, handle); }
 int bmg_i_workspace (bmg_grid * g) { return ensure_workspace (g, 0); }
 double * bmg_i_ws64 (bmg_grid * g, int which, int level) { return ws64 (g, which, level); }

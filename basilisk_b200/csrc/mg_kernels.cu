@@ -632,6 +632,117 @@ __global__ void k_adjoint_cells (bmg_geom g, const double * __restrict__ mu,
   out[q] = -mu[id]*a[id];
 }
 
+/* ---------------------------------------------------------------- */
+/* implicit viscosity (viscosity.h)                                  */
+/* ---------------------------------------------------------------- */
+
+/* components of a cell vector, and of a face coefficient */
+struct VecP { double * p[3]; };
+struct VecC { Coef<double> c[3]; };
+
+/* the tangential directions of component c in foreach_dimension order
+   (x -> y -> z -> x) */
+template <int DIM>
+__device__ __forceinline__ int vtang (int c, int m) { return DIM == 2 ? 1 - c : (c + 1 + m) % 3; }
+
+/* w.c of relax_viscosity (viscosity.h:36-67), lambda = 1, in the
+   reference's evaluation order */
+template <int DIM>
+__device__ double visc_w (const bmg_geom & g, int c, long long id, const VecP & U, const double * R,
+                          const VecC & mu, const Coef<double> & rho, double dt, double Delta)
+{
+  const long long sn = cstride<DIM> (g, c);
+  const double * un = U.p[c];
+  const double mn1 = mu.c[c].p ? mu.c[c].p[id + sn] : mu.c[c].c;
+  const double mn0 = mu.c[c].p ? mu.c[c].p[id] : mu.c[c].c;
+  double A = 2.*mn1*un[id + sn] + 2.*mn0*un[id - sn];
+  double den = 2.*mn1 + 2.*mn0;
+#pragma unroll
+  for (int m = 0; m < DIM - 1; m++) {
+    const int t = vtang<DIM> (c, m);
+    const long long s = cstride<DIM> (g, t);
+    const double * ut = U.p[t];
+    const double mt1 = mu.c[t].p ? mu.c[t].p[id + s] : mu.c[t].c;
+    const double mt0 = mu.c[t].p ? mu.c[t].p[id] : mu.c[t].c;
+    A = A + mt1*(un[id + s] + (ut[id + sn] + ut[id + sn + s])/4. -
+                 (ut[id - sn] + ut[id - sn + s])/4.);
+    A = A - mt0*(- un[id - s] + (ut[id + sn - s] + ut[id + sn])/4. -
+                 (ut[id - sn - s] + ut[id - sn])/4.);
+    den = den + mt1;
+    den = den + mt0;
+  }
+  const double r = rho.p ? rho.p[id] : rho.c;
+  return (dt/r*A + R[id]*(Delta*Delta))/((Delta*Delta)*1. + dt/r*den);
+}
+
+/* mode 0: every cell (Jacobi); 1 / 2: the red / black cells, all
+   computed from the values before the pass into W */
+template <int DIM>
+__global__ void k_visc_relax (bmg_geom g, int mode, VecP U, VecP R, VecP W, VecC mu,
+                              Coef<double> rho, double dt, double Delta)
+{
+  int i, j, k;
+  if (!cell_of_thread<DIM> (g.n, i, j, k)) return;
+  if (mode && ((i + j + k) & 1) != mode - 1) return;
+  const long long id = cidx<DIM> (g, i, j, k);
+#pragma unroll
+  for (int c = 0; c < DIM; c++)
+    W.p[c][id] = visc_w<DIM> (g, c, id, U, R.p[c], mu, rho, dt, Delta);
+}
+
+/* u = (u + 2 w)/3 (JACOBI, viscosity.h:71-74), or u = w on one colour */
+template <int DIM>
+__global__ void k_visc_commit (bmg_geom g, int mode, VecP U, VecP W)
+{
+  int i, j, k;
+  if (!cell_of_thread<DIM> (g.n, i, j, k)) return;
+  if (mode && ((i + j + k) & 1) != mode - 1) return;
+  const long long id = cidx<DIM> (g, i, j, k);
+#pragma unroll
+  for (int c = 0; c < DIM; c++)
+    U.p[c][id] = mode ? W.p[c][id] : (U.p[c][id] + 2.*W.p[c][id])/3.;
+}
+
+/* residual_viscosity, uniform-grid branch (viscosity.h:121-147), lambda =
+   1; max |res| over the components into maxres */
+template <int DIM>
+__global__ void k_visc_residual (bmg_geom g, VecP U, VecP R, VecP RES, VecC mu,
+                                 Coef<double> rho, double dt, double Delta,
+                                 unsigned long long * maxres)
+{
+  int i, j, k;
+  double m = 0.;
+  if (cell_of_thread<DIM> (g.n, i, j, k)) {
+    const long long id = cidx<DIM> (g, i, j, k);
+    const double rh = rho.p ? rho.p[id] : rho.c;
+#pragma unroll
+    for (int c = 0; c < DIM; c++) {
+      const long long sn = cstride<DIM> (g, c);
+      const double * un = U.p[c];
+      const double mn1 = mu.c[c].p ? mu.c[c].p[id + sn] : mu.c[c].c;
+      const double mn0 = mu.c[c].p ? mu.c[c].p[id] : mu.c[c].c;
+      double B = 2.*mn1*(un[id + sn] - un[id]) - 2.*mn0*(un[id] - un[id - sn]);
+#pragma unroll
+      for (int q = 0; q < DIM - 1; q++) {
+        const int t = vtang<DIM> (c, q);
+        const long long s = cstride<DIM> (g, t);
+        const double * ut = U.p[t];
+        const double mt1 = mu.c[t].p ? mu.c[t].p[id + s] : mu.c[t].c;
+        const double mt0 = mu.c[t].p ? mu.c[t].p[id] : mu.c[t].c;
+        B = B + mt1*(un[id + s] - un[id] + (ut[id + sn] + ut[id + sn + s])/4. -
+                     (ut[id - sn] + ut[id - sn + s])/4.);
+        B = B - mt0*(un[id] - un[id - s] + (ut[id + sn - s] + ut[id + sn])/4. -
+                     (ut[id - sn - s] + ut[id - sn])/4.);
+      }
+      const double r = R.p[c][id] - 1.*un[id] + dt/rh*B/(Delta*Delta);
+      RES.p[c][id] = r;
+      const double ar = fabs (r);
+      if (m == m && !(ar <= m)) m = ar;       /* a NaN sticks */
+    }
+  }
+  block_max_atomic (m, maxres);
+}
+
 /* project (poisson.h:468-509), first step: div = sum over dimensions of
    uf.x[1] - uf.x[], over dt Delta (poisson.h:482-487) */
 template <int DIM>
@@ -904,6 +1015,54 @@ int bmg_launch_adjoint_cells (int dim, bmg_geom g, const double * mu, const doub
   if (dim == 1) k_adjoint_cells<1><<<grid_shape<1> (g.n), block_shape<1> (), 0, s>>> (g, mu, a, out);
   else if (dim == 2) k_adjoint_cells<2><<<grid_shape<2> (g.n), block_shape<2> (), 0, s>>> (g, mu, a, out);
   else k_adjoint_cells<3><<<grid_shape<3> (g.n), block_shape<3> (), 0, s>>> (g, mu, a, out);
+  return status_of_launch ();
+}
+
+int bmg_launch_visc_relax (int dim, bmg_geom g, int mode, double * const * u,
+                           double * const * r, double * const * w, const bmg_coef * mu,
+                           bmg_coef rho, double dt, double Delta, cudaStream_t s)
+{
+  VecP U, R, W;
+  VecC M;
+  for (int c = 0; c < 3; c++) {
+    U.p[c] = c < dim ? u[c] : NULL; R.p[c] = c < dim ? r[c] : NULL;
+    W.p[c] = c < dim ? w[c] : NULL;
+    M.c[c] = coef_of<double> (mu[c]);
+  }
+  const Coef<double> rh = coef_of<double> (rho);
+  if (dim == 2) k_visc_relax<2><<<grid_shape<2> (g.n), block_shape<2> (), 0, s>>> (g, mode, U, R, W, M, rh, dt, Delta);
+  else if (dim == 3) k_visc_relax<3><<<grid_shape<3> (g.n), block_shape<3> (), 0, s>>> (g, mode, U, R, W, M, rh, dt, Delta);
+  else return (int) cudaErrorInvalidValue;
+  return status_of_launch ();
+}
+
+int bmg_launch_visc_commit (int dim, bmg_geom g, int mode, double * const * u,
+                            double * const * w, cudaStream_t s)
+{
+  VecP U, W;
+  for (int c = 0; c < 3; c++) { U.p[c] = c < dim ? u[c] : NULL; W.p[c] = c < dim ? w[c] : NULL; }
+  if (dim == 2) k_visc_commit<2><<<grid_shape<2> (g.n), block_shape<2> (), 0, s>>> (g, mode, U, W);
+  else if (dim == 3) k_visc_commit<3><<<grid_shape<3> (g.n), block_shape<3> (), 0, s>>> (g, mode, U, W);
+  else return (int) cudaErrorInvalidValue;
+  return status_of_launch ();
+}
+
+int bmg_launch_visc_residual (int dim, bmg_geom g, double * const * u, double * const * r,
+                              double * const * res, const bmg_coef * mu, bmg_coef rho,
+                              double dt, double Delta, unsigned long long * maxres,
+                              cudaStream_t s)
+{
+  VecP U, R, RES;
+  VecC M;
+  for (int c = 0; c < 3; c++) {
+    U.p[c] = c < dim ? u[c] : NULL; R.p[c] = c < dim ? r[c] : NULL;
+    RES.p[c] = c < dim ? res[c] : NULL;
+    M.c[c] = coef_of<double> (mu[c]);
+  }
+  const Coef<double> rh = coef_of<double> (rho);
+  if (dim == 2) k_visc_residual<2><<<grid_shape<2> (g.n), block_shape<2> (), 0, s>>> (g, U, R, RES, M, rh, dt, Delta, maxres);
+  else if (dim == 3) k_visc_residual<3><<<grid_shape<3> (g.n), block_shape<3> (), 0, s>>> (g, U, R, RES, M, rh, dt, Delta, maxres);
+  else return (int) cudaErrorInvalidValue;
   return status_of_launch ();
 }
 

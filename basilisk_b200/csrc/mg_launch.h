@@ -144,6 +144,20 @@ int bmg_launch_bottom (int dim, const bmg_bottom_level * lv, int nlev, bmg_geom 
 /* number of partial sums bmg_launch_sum needs for a level */
 int bmg_sum_partials (int dim, bmg_geom g);
 
+/* implicit viscosity (viscosity.h), 2D and 3D, FP64: one pass of
+   relax_viscosity into w (mode 0: every cell, 1/2: red/black cells), its
+   commit into u (Jacobi average, or the colour's cells), and
+   residual_viscosity with max |res| */
+int bmg_launch_visc_relax (int dim, bmg_geom g, int mode, double * const * u,
+                           double * const * r, double * const * w, const bmg_coef * mu,
+                           bmg_coef rho, double dt, double Delta, cudaStream_t s);
+int bmg_launch_visc_commit (int dim, bmg_geom g, int mode, double * const * u,
+                            double * const * w, cudaStream_t s);
+int bmg_launch_visc_residual (int dim, bmg_geom g, double * const * u, double * const * r,
+                              double * const * res, const bmg_coef * mu, bmg_coef rho,
+                              double dt, double Delta, unsigned long long * maxres,
+                              cudaStream_t s);
+
 /* project (poisson.h:468-509): the divergence of a face vector over
    dt Delta, and the face correction uf -= dt alpha grad p of direction e */
 int bmg_launch_divergence (int dim, bmg_geom g, const double * const * uf, double dt,

@@ -278,6 +278,33 @@ class Grid:
         d["status"] = status
         return d
 
+    def vector(self, comps=None):
+        """A cell-centred vector: one scalar per dimension (``vector u[]``)."""
+        return [self.scalar(None if comps is None else comps[d]) for d in range(self.dim)]
+
+    def viscosity(self, u, mu, rho, dt, nrelax=0, res=None):
+        """``viscosity (u, mu, rho, dt, nrelax, res)`` (viscosity.h:169-183):
+        u a list of dim cell scalars, mu a FaceVector (constant allowed), rho
+        a Scalar (constant allowed); returns mgstats as a dict (plus
+        ``status``)."""
+        L = _lib.load()
+        q = _lib.Viscosity()
+        hs = [c.handle for c in u] + [0] * (3 - len(u))
+        q.u = bmg_vector(bmg_scalar(hs[0]), bmg_scalar(hs[1]), bmg_scalar(hs[2]))
+        q.mu, q.rho = mu.vector, rho.scalar
+        q.dt, q.nrelax = dt, nrelax
+        if res is not None:
+            arr = (bmg_scalar * (len(res) + 1))(*[r.scalar for r in res], bmg_scalar(0))
+            self._keep.append(arr)
+            q.res = ctypes.cast(arr, ctypes.POINTER(bmg_scalar))
+        st = _lib.mgstats()
+        status = L.bmg_viscosity(self.ptr, q, ctypes.byref(st))
+        if status not in (_lib.OK, _lib.ENOTCONV):
+            check(status, "bmg_viscosity")
+        d = st.as_dict()
+        d["status"] = status
+        return d
+
     def project(self, uf, p, alpha=None, dt=0.0, nrelax=0):
         """``project (uf, p, alpha, dt, nrelax)`` (poisson.h:468-509): makes
         the face vector uf discretely divergence-free with the pressure p;

@@ -168,6 +168,23 @@ mgstats project (struct Project q);
 int bmg_project (bmg_grid * grid, struct Project q, mgstats * stats);
 
 
+/* struct Viscosity (viscosity.h:3-10), same members and order */
+struct Viscosity {
+  bmg_vector u;          /* cell velocity components, solved in place */
+  bmg_vector mu;         /* face viscosity (a constant face vector allowed) */
+  bmg_scalar rho;        /* density (a constant scalar allowed) */
+  double dt;
+  int nrelax;            /* 0 = 4 */
+  bmg_scalar * res;      /* optional: receives the residual of each component */
+};
+/* viscosity (viscosity.h:169-183) on the current grid: the implicit
+   viscous step rho (u - u*)/dt = div (2 mu D) as mg_solve with the
+   coupled relax_viscosity / residual_viscosity (viscosity.h:25-160),
+   lambda = 1 (no AXI), two or three dimensions, uniform grids, FP64.
+   Status: bmg_last_error (). */
+mgstats viscosity (struct Viscosity p);
+int bmg_viscosity (bmg_grid * grid, struct Viscosity p, mgstats * stats);
+
 /* the Poisson--Helmholtz callbacks (poisson.h:271-391); data is a
    struct Poisson *.  These are the only callbacks mg_solve/mg_cycle accept:
    they run on the device, host callbacks cannot. */

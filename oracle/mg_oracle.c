@@ -59,6 +59,12 @@ struct og_grid {
   double * bcval[6];          /* finest-level values, NULL = bcconst */
   int relax_mode;
   field a, b, res, da, c, lambda, alpha[DIM], uf[DIM];
+  /* viscosity: u, its r.h.s., correction, residual, work; mu, rho */
+  field vu[DIM], vr[DIM], vda[DIM], vres[DIM], vw[DIM], mu[DIM], rho;
+  int vbctype[DIM][6];
+  double vbcval[DIM][6];
+  int mu_const, rho_const;
+  double mu_c, rho_c;
   int alpha_const, lambda_const;
   double alpha_c, lambda_c;
 };
@@ -120,13 +126,20 @@ static field * field_of (og_grid * g, int which)
   case OG_DA: return &g->da;
   case OG_ALPHA_X: return &g->alpha[0];
   case OG_UF_X: return &g->uf[0];
+  case OG_U_X: return &g->vu[0];
+  case OG_MU_X: return &g->mu[0];
+  case OG_RHO: return &g->rho;
 #if DIM > 1
   case OG_ALPHA_Y: return &g->alpha[1];
   case OG_UF_Y: return &g->uf[1];
+  case OG_U_Y: return &g->vu[1];
+  case OG_MU_Y: return &g->mu[1];
 #endif
 #if DIM > 2
   case OG_ALPHA_Z: return &g->alpha[2];
   case OG_UF_Z: return &g->uf[2];
+  case OG_U_Z: return &g->vu[2];
+  case OG_MU_Z: return &g->mu[2];
 #endif
   }
   return NULL;
@@ -141,7 +154,14 @@ og_grid * og_new (int depth, double L0, double X0, double Y0, double Z0)
   for (int d = 0; d < 6; d++) g->bctype[d] = OG_NEUMANN; /* symmetry */
   field_alloc (g, &g->a); field_alloc (g, &g->b); field_alloc (g, &g->res);
   field_alloc (g, &g->da); field_alloc (g, &g->c); field_alloc (g, &g->lambda);
-  for (int d = 0; d < DIM; d++) { field_alloc (g, &g->alpha[d]); field_alloc (g, &g->uf[d]); }
+  for (int d = 0; d < DIM; d++) {
+    field_alloc (g, &g->alpha[d]); field_alloc (g, &g->uf[d]);
+    field_alloc (g, &g->vu[d]); field_alloc (g, &g->vr[d]); field_alloc (g, &g->vda[d]);
+    field_alloc (g, &g->vres[d]); field_alloc (g, &g->vw[d]); field_alloc (g, &g->mu[d]);
+    for (int s = 0; s < 6; s++) g->vbctype[d][s] = OG_NEUMANN;
+  }
+  field_alloc (g, &g->rho);
+  g->mu_const = 1; g->mu_c = 1.; g->rho_const = 1; g->rho_c = 1.;
   g->alpha_const = 1; g->alpha_c = 1.;   /* unityf, common.h:1276 */
   g->lambda_const = 1; g->lambda_c = 0.; /* zeroc, common.h:1277 */
   return g;
@@ -152,7 +172,12 @@ void og_free (og_grid * g)
   if (!g) return;
   field_free (g, &g->a); field_free (g, &g->b); field_free (g, &g->res);
   field_free (g, &g->da); field_free (g, &g->c); field_free (g, &g->lambda);
-  for (int d = 0; d < DIM; d++) { field_free (g, &g->alpha[d]); field_free (g, &g->uf[d]); }
+  for (int d = 0; d < DIM; d++) {
+    field_free (g, &g->alpha[d]); field_free (g, &g->uf[d]);
+    field_free (g, &g->vu[d]); field_free (g, &g->vr[d]); field_free (g, &g->vda[d]);
+    field_free (g, &g->vres[d]); field_free (g, &g->vw[d]); field_free (g, &g->mu[d]);
+  }
+  field_free (g, &g->rho);
   for (int d = 0; d < 6; d++) free (g->bcval[d]);
   free (g);
 }
@@ -349,9 +374,9 @@ static void copy_out (og_grid * g, const double * s, int l, double * v, int face
 
 static int face_dim_of (int which)
 {
-  return which == OG_ALPHA_X || which == OG_UF_X ? 0 :
-    which == OG_ALPHA_Y || which == OG_UF_Y ? 1 :
-    which == OG_ALPHA_Z || which == OG_UF_Z ? 2 : -1;
+  return which == OG_ALPHA_X || which == OG_UF_X || which == OG_MU_X ? 0 :
+    which == OG_ALPHA_Y || which == OG_UF_Y || which == OG_MU_Y ? 1 :
+    which == OG_ALPHA_Z || which == OG_UF_Z || which == OG_MU_Z ? 2 : -1;
 }
 
 void og_set_field (og_grid * g, int which, const double * values)
@@ -362,11 +387,13 @@ void og_set_field (og_grid * g, int which, const double * values)
   copy_in (g, f->lv[g->depth], g->depth, values, fd);
   if (fd >= 0) {
     if (which >= OG_ALPHA_X && which <= OG_ALPHA_Z) g->alpha_const = 0;
+    if (which >= OG_MU_X && which <= OG_MU_Z) g->mu_const = 0;
     /* the automatic boundary of a dirty face vector copies periodic
        ghosts before the first stencil read (stencils.h:228+). */
     periodic_boundary (g, f->lv[g->depth], g->depth);
   }
   if (which == OG_LAMBDA) g->lambda_const = 0;
+  if (which == OG_RHO) g->rho_const = 0;
 }
 
 void og_get_field (og_grid * g, int which, double * out)
@@ -431,7 +458,7 @@ static inline double finev (const double * f, int Pf, int i, int j, int k,
 
 /* face_average (grid/multigrid-common.h:42-58), with the index rotation
    that foreach_dimension applies to the fine() offsets (rotate.lex). */
-static void restrict_faces (og_grid * g, int l)
+static void restrict_faces_of (og_grid * g, field * comps, int l)
 {
   int n = 1 << l, P = P_of (l), Pf = P_of (l + 1);
 #pragma omp parallel for schedule(static)
@@ -439,8 +466,8 @@ static void restrict_faces (og_grid * g, int l)
     for (int j = (DIM > 1 ? GH : 0); j < (DIM > 1 ? n + GH : 1); j++)
       for (int k = (DIM > 2 ? GH : 0); k < (DIM > 2 ? n + GH : 1); k++) {
         for (int d = 0; d < DIM; d++) {
-          const double * f = g->alpha[d].lv[l + 1];
-          double * c = g->alpha[d].lv[l];
+          const double * f = comps[d].lv[l + 1];
+          double * c = comps[d].lv[l];
           size_t sd = stride (P, d), id = IX (P, i, j, k);
           for (int side = 0; side < 2; side++) {
             int o = 2*side;
@@ -469,6 +496,8 @@ static void restrict_faces (og_grid * g, int l)
       }
 }
 
+static void restrict_faces (og_grid * g, int l) { restrict_faces_of (g, g->alpha, l); }
+
 /* poisson.h:418-420: restriction ({alpha, lambda}) through all levels,
    each level followed by its boundary (multigrid-common.h:398). */
 void og_restrict_coefficients (og_grid * g)
@@ -493,12 +522,12 @@ void og_restrict_res (og_grid * g)
 }
 
 /* bilinear (grid/multigrid-common.h:124-140) of da from level l-1 */
-static void prolong_bilinear (og_grid * g, int l)
+static void prolong_field (og_grid * g, field * fd, int l)
 {
   int n = 1 << l, P = P_of (l), Pc = P_of (l - 1);
   (void) Pc;
-  const double * s = g->da.lv[l - 1];
-  double * f = g->da.lv[l];
+  const double * s = fd->lv[l - 1];
+  double * f = fd->lv[l];
 #pragma omp parallel for schedule(static)
   for (int i = GH; i < n + GH; i++)
     for (int j = (DIM > 1 ? GH : 0); j < (DIM > 1 ? n + GH : 1); j++)
@@ -525,6 +554,8 @@ static void prolong_bilinear (og_grid * g, int l)
 #endif
       }
 }
+
+static void prolong_bilinear (og_grid * g, int l) { prolong_field (g, &g->da, l); }
 
 /* ------------------------------------------------------------------ */
 /* relax and residual                                                  */
@@ -770,5 +801,244 @@ og_mgstats og_project (og_grid * g, double dt, int nrelax)
           u[id] -= dt*ALPHA (e, l, id)*((p[id] - p[id - st[e]])/Delta);
         }
   }
+  return s;
+}
+
+/* ------------------------------------------------------------------ */
+/* implicit viscosity (viscosity.h)                                    */
+/* ------------------------------------------------------------------ */
+
+void og_set_visc_bc (og_grid * g, int comp, int side, int type, double value)
+{
+  if (comp >= 0 && comp < DIM && side >= 0 && side < 2*DIM) {
+    g->vbctype[comp][side] = type;
+    g->vbcval[comp][side] = value;
+  }
+}
+
+void og_set_mu_const (og_grid * g, double v) { g->mu_const = 1; g->mu_c = v; }
+void og_set_rho_const (og_grid * g, double v) { g->rho_const = 1; g->rho_c = v; }
+
+#define MU(d, l, id) (g->mu_const ? g->mu_c : g->mu[d].lv[l][id])
+#define RHO(l, id) (g->rho_const ? g->rho_c : g->rho.lv[l][id])
+
+/* boundary_level of component c of the vector (its own box conditions,
+   constant data), as the list boundaries of mg_cycle apply them */
+static void comp_boundary (og_grid * g, int c, double * s, int l, int homogeneous)
+{
+  int t[6], save_t[6];
+  double v[6], save_v[6];
+  double * save_p[6];
+  for (int k = 0; k < 6; k++) {
+    t[k] = k < 2*DIM ? g->vbctype[c][k] : OG_NEUMANN; v[k] = k < 2*DIM ? g->vbcval[c][k] : 0.;
+    save_t[k] = g->bctype[k]; save_v[k] = g->bcconst[k]; save_p[k] = g->bcval[k];
+    g->bctype[k] = t[k]; g->bcconst[k] = v[k]; g->bcval[k] = NULL;
+  }
+  boundary_level (g, s, l, homogeneous);
+  for (int k = 0; k < 6; k++) {
+    g->bctype[k] = save_t[k]; g->bcconst[k] = save_v[k]; g->bcval[k] = save_p[k];
+  }
+}
+
+/* the tangential directions of component c in foreach_dimension order
+   (rotate.lex: x -> y -> z -> x) */
+static inline int tang (int c, int m) { return DIM == 2 ? 1 - c : (c + 1 + m) % 3; }
+
+/* w.c of relax_viscosity (viscosity.h:36-67) at cell id of level l, from
+   the components U and the r.h.s. R of component c */
+static double visc_w (og_grid * g, int c, int l, size_t id, double * const * U,
+                      const double * R, double dt)
+{
+  const int P = P_of (l);
+  const double Delta = g->L0*(1./(1 << l));
+  size_t st[3];
+  for (int e = 0; e < DIM; e++) st[e] = stride (P, e);
+  const size_t sn = st[c];
+  const double * un = U[c];
+  const double mn1 = MU (c, l, id + sn), mn0 = MU (c, l, id);
+  double A = 2.*mn1*un[id + sn] + 2.*mn0*un[id - sn];
+  double den = 2.*mn1 + 2.*mn0;
+  for (int m = 0; m < DIM - 1; m++) {
+    const int t = tang (c, m);
+    const size_t s = st[t];
+    const double * ut = U[t];
+    const double mt1 = MU (t, l, id + s), mt0 = MU (t, l, id);
+    A = A + mt1*(un[id + s] + (ut[id + sn] + ut[id + sn + s])/4. -
+                 (ut[id - sn] + ut[id - sn + s])/4.);
+    A = A - mt0*(- un[id - s] + (ut[id + sn - s] + ut[id + sn])/4. -
+                 (ut[id - sn - s] + ut[id - sn])/4.);
+    den = den + mt1;
+    den = den + mt0;
+  }
+  const double rho = RHO (l, id);
+  return (dt/rho*A + R[id]*sq_(Delta))/(sq_(Delta)*1. + dt/rho*den);
+}
+
+/* relax_viscosity over level l, in the variant selected: the reference's
+   in-place sweep (w = u, components in turn per cell), its JACOBI branch,
+   or red-black with every colour computed from the values before it
+   (the same-colour diagonal neighbours it reads keep their old values) */
+static void visc_relax (og_grid * g, int l, double dt)
+{
+  const int n = 1 << l, P = P_of (l);
+  double * U[3] = {NULL, NULL, NULL}, * W[3] = {NULL, NULL, NULL};
+  for (int c = 0; c < DIM; c++) { U[c] = g->vda[c].lv[l]; W[c] = g->vw[c].lv[l]; }
+  int J0 = DIM > 1 ? GH : 0, J1 = DIM > 1 ? n + GH : 1;
+  int K0 = DIM > 2 ? GH : 0, K1 = DIM > 2 ? n + GH : 1;
+  if (g->relax_mode == OG_RELAX_GS) {
+    for (int i = GH; i < n + GH; i++)
+      for (int j = J0; j < J1; j++)
+        for (int k = K0; k < K1; k++) {
+          size_t id = IX (P, i, j, k);
+          for (int c = 0; c < DIM; c++)
+            U[c][id] = visc_w (g, c, l, id, U, g->vres[c].lv[l], dt);
+        }
+    return;
+  }
+  for (int color = 0; color < 2; color++) {
+    const int jac = g->relax_mode == OG_RELAX_JACOBI;
+    if (jac && color == 1) break;
+    if (!jac && color == 1)
+      for (int c = 0; c < DIM; c++) comp_boundary (g, c, U[c], l, 1);
+    for (int i = GH; i < n + GH; i++)
+      for (int j = J0; j < J1; j++)
+        for (int k = K0; k < K1; k++) {
+          if (!jac && ((i + j + k) & 1) != color) continue;
+          size_t id = IX (P, i, j, k);
+          for (int c = 0; c < DIM; c++)
+            W[c][id] = visc_w (g, c, l, id, U, g->vres[c].lv[l], dt);
+        }
+    for (int i = GH; i < n + GH; i++)
+      for (int j = J0; j < J1; j++)
+        for (int k = K0; k < K1; k++) {
+          if (!jac && ((i + j + k) & 1) != color) continue;
+          size_t id = IX (P, i, j, k);
+          for (int c = 0; c < DIM; c++)
+            U[c][id] = jac ? (U[c][id] + 2.*W[c][id])/3. : W[c][id];
+        }
+  }
+}
+
+/* residual_viscosity, uniform-grid branch (viscosity.h:121-147), after
+   the boundary of u; res of every component, returns the maximum */
+double og_residual_viscosity (og_grid * g, double dt)
+{
+  const int l = g->depth, n = 1 << l, P = P_of (l);
+  const double Delta = g->L0*(1./(1 << l));
+  double * U[3] = {NULL, NULL, NULL};
+  for (int c = 0; c < DIM; c++) {
+    U[c] = g->vu[c].lv[l];
+    comp_boundary (g, c, U[c], l, 0);
+  }
+  size_t st[3];
+  for (int e = 0; e < DIM; e++) st[e] = stride (P, e);
+  double maxres = 0.;
+  int J0 = DIM > 1 ? GH : 0, J1 = DIM > 1 ? n + GH : 1;
+  int K0 = DIM > 2 ? GH : 0, K1 = DIM > 2 ? n + GH : 1;
+  for (int i = GH; i < n + GH; i++)
+    for (int j = J0; j < J1; j++)
+      for (int k = K0; k < K1; k++) {
+        size_t id = IX (P, i, j, k);
+        for (int c = 0; c < DIM; c++) {
+          const size_t sn = st[c];
+          const double * un = U[c];
+          double B = 2.*MU (c, l, id + sn)*(un[id + sn] - un[id]) -
+            2.*MU (c, l, id)*(un[id] - un[id - sn]);
+          for (int m = 0; m < DIM - 1; m++) {
+            const int t = tang (c, m);
+            const size_t s = st[t];
+            const double * ut = U[t];
+            B = B + MU (t, l, id + s)*(un[id + s] - un[id] +
+                                      (ut[id + sn] + ut[id + sn + s])/4. -
+                                      (ut[id - sn] + ut[id - sn + s])/4.);
+            B = B - MU (t, l, id)*(un[id] - un[id - s] +
+                                  (ut[id + sn - s] + ut[id + sn])/4. -
+                                  (ut[id - sn - s] + ut[id - sn])/4.);
+          }
+          const double r = g->vr[c].lv[l][id] - 1.*un[id] + dt/RHO (l, id)*B/sq_(Delta);
+          g->vres[c].lv[l][id] = r;
+          if (fabs (r) > maxres)
+            maxres = fabs (r);
+        }
+      }
+  return maxres;
+}
+
+/* mg_cycle (poisson.h:32-90) on the vector list {da.x, da.y, (da.z)} */
+static void visc_cycle (og_grid * g, int nrelax, int minlevel, int maxlevel, double dt)
+{
+  for (int c = 0; c < DIM; c++)
+    for (int l = g->depth - 1; l >= 0; l--)
+      restrict_average (g, g->vres[c].lv[l], g->vres[c].lv[l + 1], l);
+  minlevel = minlevel < maxlevel ? minlevel : maxlevel;
+  for (int l = minlevel; l <= maxlevel; l++) {
+    for (int c = 0; c < DIM; c++) {
+      if (l == minlevel) {
+        double * s = g->vda[c].lv[l];
+        for (size_t q = 0; q < level_size (l); q++) s[q] = 0.;
+      }
+      else
+        prolong_field (g, &g->vda[c], l);
+      comp_boundary (g, c, g->vda[c].lv[l], l, 1);
+    }
+    for (int i = 0; i < nrelax; i++) {
+      visc_relax (g, l, dt);
+      for (int c = 0; c < DIM; c++)
+        comp_boundary (g, c, g->vda[c].lv[l], l, 1);
+    }
+  }
+  const int l = g->depth, n = 1 << l, P = P_of (l);
+  for (int c = 0; c < DIM; c++)
+    for (int i = GH; i < n + GH; i++)
+      for (int j = (DIM > 1 ? GH : 0); j < (DIM > 1 ? n + GH : 1); j++)
+        for (int k = (DIM > 2 ? GH : 0); k < (DIM > 2 ? n + GH : 1); k++) {
+          size_t id = IX (P, i, j, k);
+          g->vu[c].lv[l][id] += g->vda[c].lv[l][id];
+        }
+}
+
+/* viscosity (viscosity.h:169-183): r = u, restriction ({mu, rho}), then
+   mg_solve with residual_viscosity / relax_viscosity (minlevel 0) */
+og_mgstats og_viscosity (og_grid * g, double dt, int nrelax)
+{
+  const int l = g->depth, n = 1 << l, P = P_of (l);
+  for (int c = 0; c < DIM; c++)
+    memcpy (g->vr[c].lv[l], g->vu[c].lv[l], level_size (l)*sizeof (double));
+  for (int m = g->depth - 1; m >= 0; m--) {
+    if (!g->mu_const) {
+      restrict_faces_of (g, g->mu, m);
+      for (int d = 0; d < DIM; d++) periodic_boundary (g, g->mu[d].lv[m], m);
+    }
+    if (!g->rho_const)
+      restrict_average (g, g->rho.lv[m], g->rho.lv[m + 1], m);
+  }
+  og_mgstats s = {0};
+  /* sum of the r.h.s. components (poisson.h:162-167) */
+  for (int i = GH; i < n + GH; i++)
+    for (int j = (DIM > 1 ? GH : 0); j < (DIM > 1 ? n + GH : 1); j++)
+      for (int k = (DIM > 2 ? GH : 0); k < (DIM > 2 ? n + GH : 1); k++)
+        for (int c = 0; c < DIM; c++)
+          s.sum += g->vr[c].lv[l][IX (P, i, j, k)];
+  s.nrelax = nrelax > 0 ? nrelax : 4;
+  double resb;
+  resb = s.resb = s.resa = og_residual_viscosity (g, dt);
+  const double tolerance = og_TOLERANCE;
+  for (s.i = 0; s.i < og_NITERMAX && (s.i < og_NITERMIN || s.resa > tolerance); s.i++) {
+    visc_cycle (g, s.nrelax, 0, g->depth, dt);
+    s.resa = og_residual_viscosity (g, dt);
+    if (s.resa > tolerance) {
+      if (resb/s.resa < 1.2 && s.nrelax < 100)
+        s.nrelax++;
+      else if (resb/s.resa > 10 && s.nrelax > 2)
+        s.nrelax--;
+    }
+    resb = s.resa;
+  }
+  s.minlevel = 0;
+  if (s.resa > tolerance)
+    fprintf (stderr,
+             "WARNING: convergence for %s not reached after %d iterations\n"
+             "  res: %g sum: %g nrelax: %d\n", "u.x",
+             s.i, s.resa, s.sum, s.nrelax), fflush (stderr);
   return s;
 }

@@ -50,7 +50,8 @@ typedef struct {
 } og_mgstats;
 
 enum { OG_A = 0, OG_B, OG_RES, OG_LAMBDA, OG_ALPHA_X, OG_ALPHA_Y, OG_ALPHA_Z, OG_DA,
-       OG_UF_X, OG_UF_Y, OG_UF_Z };
+       OG_UF_X, OG_UF_Y, OG_UF_Z,
+       OG_U_X, OG_U_Y, OG_U_Z, OG_MU_X, OG_MU_Y, OG_MU_Z, OG_RHO };
 
 typedef struct og_grid og_grid;
 
@@ -78,6 +79,14 @@ og_mgstats og_poisson (og_grid * g, double tolerance, int nrelax, int minlevel);
 /* project (poisson.h:468-509): uf = the OG_UF_* face vector, p = OG_A, alpha
    as set (unityf by default), div in OG_B; dt = 0 / nrelax = 0: defaults */
 og_mgstats og_project (og_grid * g, double dt, int nrelax);
+/* viscosity (viscosity.h:169-183): implicit viscous step of the cell
+   vector OG_U_* with face viscosity OG_MU_* (or a constant) and density
+   OG_RHO (or a constant); component c of u has its own box conditions */
+void og_set_visc_bc (og_grid * g, int comp, int side, int type, double value);
+void og_set_mu_const (og_grid * g, double v);
+void og_set_rho_const (og_grid * g, double v);
+og_mgstats og_viscosity (og_grid * g, double dt, int nrelax);
+double og_residual_viscosity (og_grid * g, double dt);
 double og_sum_b (og_grid * g);
 /* level access for fine-grained tests: interior values of a level */
 void og_get_level (og_grid * g, int which, int level, double * out);

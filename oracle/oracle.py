@@ -21,7 +21,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 RIGHT, LEFT, TOP, BOTTOM, FRONT, BACK = range(6)
 NEUMANN, DIRICHLET, PERIODIC = 0, 1, 2
 RELAX_GS, RELAX_JACOBI, RELAX_RBGS = 0, 1, 2
-A, B, RES, LAMBDA, ALPHA_X, ALPHA_Y, ALPHA_Z, DA, UF_X, UF_Y, UF_Z = range(11)
+A, B, RES, LAMBDA, ALPHA_X, ALPHA_Y, ALPHA_Z, DA, UF_X, UF_Y, UF_Z, U_X, U_Y, U_Z, MU_X, MU_Y, MU_Z, RHO = range(18)
 
 
 class MGStats(ctypes.Structure):
@@ -71,6 +71,11 @@ def lib(dim):
         "og_mg_solve": (MGStats, [P, D, I, I]),
         "og_poisson": (MGStats, [P, D, I, I]),
         "og_project": (MGStats, [P, D, I]),
+        "og_set_visc_bc": (None, [P, I, I, I, D]),
+        "og_set_mu_const": (None, [P, D]),
+        "og_set_rho_const": (None, [P, D]),
+        "og_viscosity": (MGStats, [P, D, I]),
+        "og_residual_viscosity": (D, [P, D]),
         "og_sum_b": (D, [P]),
         "og_get_level": (None, [P, I, I, DP]),
         "og_set_level": (None, [P, I, I, DP]),
@@ -189,6 +194,8 @@ class Grid:
             shape = face_shape(self.n, self.dim, which - ALPHA_X)
         elif which in (UF_X, UF_Y, UF_Z):
             shape = face_shape(self.n, self.dim, which - UF_X)
+        elif which in (MU_X, MU_Y, MU_Z):
+            shape = face_shape(self.n, self.dim, which - MU_X)
         else:
             shape = (self.n,) * self.dim
         out = np.empty(shape, dtype=np.float64)
@@ -259,6 +266,36 @@ class Grid:
 
     def get_uf(self):
         return [self.get(UF_X + d) for d in range(self.dim)]
+
+    def set_u(self, comps):
+        for d, c in enumerate(comps):
+            self.set(U_X + d, c)
+
+    def get_u(self):
+        return [self.get(U_X + d) for d in range(self.dim)]
+
+    def set_mu(self, comps):
+        for d, c in enumerate(comps):
+            self.set(MU_X + d, c)
+
+    def set_mu_const(self, v):
+        self.L.og_set_mu_const(self.g, float(v))
+
+    def set_rho(self, arr):
+        self.set(RHO, arr)
+
+    def set_rho_const(self, v):
+        self.L.og_set_rho_const(self.g, float(v))
+
+    def set_visc_bc(self, comp, side, kind, value=0.0):
+        self.L.og_set_visc_bc(self.g, comp, side, kind, float(value))
+
+    def viscosity(self, dt, nrelax=0):
+        """viscosity (u, mu, rho, dt, nrelax) (viscosity.h:169-183)."""
+        return self.L.og_viscosity(self.g, dt, nrelax).as_dict()
+
+    def residual_viscosity(self, dt):
+        return self.L.og_residual_viscosity(self.g, dt)
 
     def project(self, dt=0.0, nrelax=0):
         """project (uf, p = a, alpha, dt, nrelax) (poisson.h:468-509)."""
