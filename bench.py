@@ -321,6 +321,41 @@ def run_workload(args, ws, rank, local):
                   "grid": "16 x 512^2 (depth 9)", "form": args.precision,
                   "relax": "red-black Gauss-Seidel",
                   "parallelism": "replicas" if ws > 1 else "1 gpu"}
+    elif args.workload == "viscosity_2d":
+        depth = 11
+        n = 1 << depth
+        g = bmg.Grid(2, depth, relax="rbgs")
+        g.set_stream(torch.cuda.current_stream().cuda_stream)
+        lv = problems.two_phase_tree_levels(depth, seed=5 + rank)[depth]
+        rng = np.random.default_rng(6 + rank)
+        u0 = [problems.gaussian_bumps(n, rng), problems.gaussian_bumps(n, rng)]
+        # face viscosity 1/100 of the face density: mu and rho ratios 1000
+        ax, ay = problems.two_phase_alpha(n)
+        mu = g.face_vector([0.01 / ax, 0.01 / ay])
+        x, y = problems.centers(2, n)
+        f = 0.5 * (1.0 - np.tanh((np.sqrt((x - 0.5) ** 2 + (y - 0.5) ** 2) - 0.25) * n / 2.0))
+        rho = g.scalar(f * (1.0 - 1000.0) + 1000.0)
+        uu = g.vector()
+        for c in uu:
+            for side in range(4):
+                c.bc(side, "dirichlet", 0.0)
+        dev = [torch.tensor(c, dtype=torch.float64, device="cuda") for c in u0]
+        tol, dtype = TOL, "f64"
+        bmg.set_tolerance(tol)      # viscosity () solves to the global TOLERANCE
+        del lv
+
+        def reset():
+            for c, d in zip(uu, dev):
+                c.set(d)
+
+        def solve():
+            return g.viscosity(uu, mu, rho, 1e-3)
+        config = {"workload": "viscosity_2d: implicit viscous step of a 2048^2 velocity field "
+                              "(two components, Gaussian bumps), rho two-phase (ratio 1000), "
+                              "face mu = 0.01 rho_face (ratio 1000), dt = 1e-3, no-slip walls, "
+                              "TOLERANCE 1e-6",
+                  "grid": "2048x2048 (depth 11)", "relax": "red-black (colour-buffered)",
+                  "parallelism": "replicas" if ws > 1 else "1 gpu"}
     else:
         prob = problems.helmholtz_3d(depth=8, seed=2 + rank)
         g = bmg.Grid(3, 8, relax="rbgs", precision=args.precision)
@@ -438,7 +473,7 @@ def main():
                     help="profiling run: only this form, no e2e, no CPU baseline, no JSON")
     ap.add_argument("--depth", type=int, default=DEPTH, help="grid depth (profiling runs)")
     ap.add_argument("--workload", choices=["two_phase_2d", "two_phase_tree", "helmholtz_3d",
-                                           "random_field_batch"],
+                                           "random_field_batch", "viscosity_2d"],
                     default="two_phase_2d",
                     help="two_phase_2d: the headline; the others print their own line")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64",
