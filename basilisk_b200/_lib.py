@@ -143,6 +143,11 @@ SIGNATURES = {
     "bmg_tree_info": (I, [P, ctypes.POINTER(I), ctypes.POINTER(ctypes.c_longlong)]),
     "bmg_tree_flags": (I, [P, I, ctypes.POINTER(ctypes.c_ubyte)]),
     "bmg_bc_level": (I, [P, bmg_scalar, I, I, I, DP, I]),
+    "bmg_dump": (I, [P, ctypes.c_char_p, ctypes.POINTER(bmg_scalar),
+                     ctypes.POINTER(ctypes.c_char_p), D, I]),
+    "bmg_restore": (I, [P, ctypes.c_char_p, ctypes.POINTER(bmg_scalar),
+                        ctypes.POINTER(ctypes.c_char_p), ctypes.POINTER(D),
+                        ctypes.POINTER(I)]),
     "bmg_get_counters": (I, [P, ctypes.POINTER(bmg_counters)]),
     "bmg_reset_counters": (I, [P]),
     "bmg_set_timing": (I, [P, I]),

@@ -224,6 +224,7 @@ int bmg_grid_info (const bmg_grid * g, int * dim, int * depth)
 int bmg_origin (bmg_grid * g, double x, double y, double z)
 {
   if (!g) return fail (BMG_EINVAL);
+  if (g->X0 != x || g->Y0 != y || g->Z0 != z) graphs_clear (g);   /* boundary data */
   g->X0 = x; g->Y0 = y; g->Z0 = z;
   return BMG_OK;
 }
@@ -231,6 +232,7 @@ int bmg_origin (bmg_grid * g, double x, double y, double z)
 int bmg_size (bmg_grid * g, double L0)
 {
   if (!g || !(L0 > 0.)) return fail (BMG_EINVAL);
+  if (g->L0 != L0) graphs_clear (g);     /* Delta is a launch argument */
   g->L0 = L0;
   return BMG_OK;
 }

@@ -13,6 +13,7 @@ entries along ``d``.  numpy arrays go through host memory, CUDA torch tensors
 are read and written in place on the device.
 """
 import ctypes
+import os
 
 import numpy as np
 
@@ -387,6 +388,42 @@ class Grid:
         arr = (bmg_scalar * (len(hs) + 1))(*[bmg_scalar(h) for h in hs], bmg_scalar(0))
         check(_lib.load().bmg_restriction(self.ptr, arr), "bmg_restriction")
 
+    def _named_list(self, fields):
+        items = list(fields.items()) if isinstance(fields, dict) else list(fields)
+        for name, f in items:
+            if not isinstance(f, Field):
+                raise TypeError("dump/restore take cell fields (%s)" % name)
+        arr = (bmg_scalar * (len(items) + 1))(*[bmg_scalar(f.handle) for _, f in items],
+                                              bmg_scalar(0))
+        names = (ctypes.c_char_p * max(1, len(items)))(*[n.encode() for n, _ in items])
+        return arr, names
+
+    def dump(self, file, fields, t=0.0, i=0):
+        """``dump (file, list)`` (output.h:1138-1171): fields is a dict (or
+        list of pairs) name -> cell field; t and i go into the header."""
+        arr, names = self._named_list(fields)
+        check(_lib.load().bmg_dump(self.ptr, os.fsencode(file), arr, names, float(t), int(i)),
+              "bmg_dump")
+
+    def restore(self, file, fields):
+        """``restore (file, list)`` (output.h:1220-1400): fills the fields
+        whose names the file holds; returns the header's (t, i)."""
+        arr, names = self._named_list(fields)
+        t, i = ctypes.c_double(0.0), ctypes.c_int(0)
+        check(_lib.load().bmg_restore(self.ptr, os.fsencode(file), arr, names,
+                                      ctypes.byref(t), ctypes.byref(i)), "bmg_restore")
+        # the file's origin and size now hold (output.h:1325-1326)
+        with open(file, "rb") as fp:
+            head = fp.read(56)
+            nlen, version = ctypes.c_long.from_buffer_copy(head, 8).value, \
+                ctypes.c_int.from_buffer_copy(head, 28).value
+            if version != 161020:
+                for _ in range(nlen):
+                    fp.seek(ctypes.c_uint.from_buffer_copy(fp.read(4)).value, 1)
+            o = np.frombuffer(fp.read(32), dtype=np.float64)
+        self.origin, self.L0 = (float(o[0]), float(o[1]), float(o[2])), float(o[3])
+        return t.value, i.value
+
     def counters(self):
         c = _lib.bmg_counters()
         check(_lib.load().bmg_get_counters(self.ptr, ctypes.byref(c)), "bmg_get_counters")
@@ -435,6 +472,16 @@ class TreeGrid(Grid):
         if r < 0:
             check(r, "bmg_tree_refine")
         return r
+
+    def restore(self, file, fields):
+        """``restore (file, list)`` on a tree: init_grid (1), then the file's
+        refinement (output.h:1237-1242, 1357-1358)."""
+        if not self._has_tree():
+            self.refine(lambda l, x, y: False)
+        return super().restore(file, fields)
+
+    def _has_tree(self):
+        return _lib.load().bmg_tree_info(self.ptr, None, None) == _lib.OK
 
     def info(self):
         d = ctypes.c_int()

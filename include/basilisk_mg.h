@@ -248,6 +248,31 @@ int bmg_tree_flags (const bmg_grid * grid, int level, unsigned char * flags);
 int bmg_bc_level (bmg_grid * grid, bmg_scalar s, int side, int type, int level,
                   const double * values, int memory);
 
+/* ---- snapshots: dump () and restore () (output.h:1043-1400) ---------- */
+
+/* dump (file, list) (output.h:1138-1171): writes the fields of list (ends
+   with .i = 0), named by names[], in the reference's binary format
+   (dump_version 170901): header {t, len, i, depth, npe = 1, version, n},
+   the names with "size" first, {X0, Y0, Z0, L0}, then every cell of
+   foreach_cell () with its flags (leaf = 2), its subtree's cell count and
+   the values.  A uniform grid writes all its levels (its leaves are the
+   finest level); a tree grid its active cells.  t and iter go into the
+   header. */
+int bmg_dump (bmg_grid * grid, const char * file, const bmg_scalar * list,
+              const char * const * names, double t, int iter);
+/* restore (file, list) (output.h:1220-1400): reads a file of the format
+   above (or the older, unnamed 161020 one, whose columns must be list's
+   fields in order).  Columns whose name matches names[k] go to list[k];
+   the others are skipped.  The origin and size of the file are applied.
+   A tree grid, or any grid given a file that holds a tree, is rebuilt
+   from init_grid (1) by refining the cells the file holds refined (as
+   refine_cell does in restore); a uniform grid takes a uniform file of
+   its own depth.  Fields that are not listed keep their values (the
+   reference resets them to 0; here the caller owns them).  *t and *iter
+   (when not NULL) receive the header's time and iteration. */
+int bmg_restore (bmg_grid * grid, const char * file, const bmg_scalar * list,
+                 const char * const * names, double * t, int * iter);
+
 /* ---- differentiation ----------------------------------------------- */
 
 /* Gradients of a loss l(a) with respect to the coefficients of the solve
