@@ -171,6 +171,71 @@ __device__ __forceinline__ void put_quad (T * a0, T * a1, int off, const Quad<T>
 template <typename T> struct Vec4;
 template <> struct Vec4<float> { typedef float4 type; };
 
+/* One colour pass of an FP32 tile that lies inside the domain, four cells
+   of colour C per thread.  Everything that does not change between passes
+   is hoisted by the caller: the column offset o of the thread's colour
+   cells (the same in every pass, since the row advances by one per pass
+   while the colour alternates) and the thread's quad m0.  With C a
+   template parameter every array offset is a constant, so each operand is
+   one 16-byte shared load from one base address. */
+template <int C, bool LAM, int W, int M, int MY>
+__device__ __forceinline__ void tile_pass4 (float * __restrict__ smb, int k, int pr, int m0, int o,
+                                            float D2, float lamc)
+{
+  constexpr int WM = W*M, WX = (W + 1)*M, WY = W*MY;
+  constexpr int OR = 2*WM, OX = 4*WM, OY = OX + 2*WX, OL = OY + 2*WY;
+  constexpr int CO = C ^ 1;
+  const int p = k + 1 + pr;
+  if (p >= W - k - 1) return;
+  const int ci = p*M + m0, cy = p*MY + m0;
+  const float * __restrict__ A = smb + CO*WM + ci;             /* the other colour */
+  const float4 up = *(const float4 *) (A - M), dn = *(const float4 *) (A + M);
+  const float4 mid = *(const float4 *) A;
+  const float4 rr = *(const float4 *) (smb + OR + C*WM + ci);
+  const float4 xl = *(const float4 *) (smb + OX + C*WX + ci);
+  const float4 xu = *(const float4 *) (smb + OX + CO*WX + ci + M);
+  const float4 yl = *(const float4 *) (smb + OY + C*WY + cy);
+  const float4 y4 = *(const float4 *) (smb + OY + CO*WY + cy);
+  float4 lv;
+  if (LAM) lv = *(const float4 *) (smb + OL + C*WM + ci);
+  else lv = make_float4 (lamc, lamc, lamc, lamc);
+  /* left / right neighbours and right faces of the four cells */
+  float v[5], yr[4];
+  if (o == 0) {
+    v[0] = A[-1]; v[1] = mid.x; v[2] = mid.y; v[3] = mid.z; v[4] = mid.w;
+    yr[0] = y4.x; yr[1] = y4.y; yr[2] = y4.z; yr[3] = y4.w;
+  }
+  else {
+    v[0] = mid.x; v[1] = mid.y; v[2] = mid.z; v[3] = mid.w; v[4] = A[4];
+    yr[0] = y4.y; yr[1] = y4.z; yr[2] = y4.w; yr[3] = smb[OY + CO*WY + cy + 4];
+  }
+  const float rv[4] = {rr.x, rr.y, rr.z, rr.w}, lvv[4] = {lv.x, lv.y, lv.z, lv.w};
+  const float xlv[4] = {xl.x, xl.y, xl.z, xl.w}, xuv[4] = {xu.x, xu.y, xu.z, xu.w};
+  const float ylv[4] = {yl.x, yl.y, yl.z, yl.w};
+  const float upv[4] = {up.x, up.y, up.z, up.w}, dnv[4] = {dn.x, dn.y, dn.z, dn.w};
+  float out[4];
+#pragma unroll
+  for (int e = 0; e < 4; e++) {
+    /* relax_value (poisson.h:303-319) in FP32 with fused multiply-adds */
+    float nn = (-D2)*rv[e], d = (-lvv[e])*D2;
+    nn = fmaf (xlv[e], upv[e], fmaf (xuv[e], dnv[e], nn));
+    nn = fmaf (ylv[e], v[e], fmaf (yr[e], v[e + 1], nn));
+    d += xuv[e] + xlv[e];
+    d += yr[e] + ylv[e];
+    out[e] = __fdividef (nn, d);
+  }
+  /* the valid columns of colour C shrink by one cell per pass */
+  const int mlo = (k + 2 - o) >> 1, mhi = (W - k - o) >> 1;
+  float * __restrict__ a = smb + C*WM + ci;
+  if (m0 >= mlo && m0 + 4 <= mhi)
+    *(float4 *) a = make_float4 (out[0], out[1], out[2], out[3]);
+  else {
+#pragma unroll
+    for (int e = 0; e < 4; e++)
+      if (m0 + e >= mlo && m0 + e < mhi) a[e] = out[e];
+  }
+}
+
 template <typename T, int TS, int S, bool LAM, int BX, int BY, int CPT, int MINB>
 __global__ void __launch_bounds__ (BX*BY, MINB)
 k_relax_tile2d (bmg_geom g, T * __restrict__ out, const T * __restrict__ in,
@@ -305,7 +370,20 @@ k_relax_tile2d (bmg_geom g, T * __restrict__ out, const T * __restrict__ in,
   __syncthreads ();
 
   const T D2 = Delta*Delta;
-  for (int sw = 0; sw < nsweeps; sw++)
+  if constexpr (CPT == 4) {
+    if (inner) {
+      /* column offset of the thread's cells: (c - base - p) & 1 with
+         p = k + 1 + pr and c = k & 1, the same in every pass */
+      const int o = (base + 1 + pr) & 1, m0 = 4*tx;
+      for (int sw = 0; sw < nsweeps; sw++) {
+        tile_pass4<0, LAM, W, M, MY> (smb, 2*sw, pr, m0, o, D2, lam.c);
+        __syncthreads ();
+        tile_pass4<1, LAM, W, M, MY> (smb, 2*sw + 1, pr, m0, o, D2, lam.c);
+        __syncthreads ();
+      }
+    }
+  }
+  for (int sw = 0; sw < ((CPT == 4 && inner) ? 0 : nsweeps); sw++)
 #pragma unroll
     for (int c = 0; c < 2; c++) {
       const int k = 2*sw + c;
@@ -752,6 +830,68 @@ __device__ __forceinline__ void bot_sweeps2d (const bmg_geom g, T * a, const T *
     }
 }
 
+/* all nrelax sweeps of one FP32 2D level whose cells of one colour number
+   at most 2 nt: each thread keeps its (up to two per colour) cells'
+   coefficients in registers, divided by the diagonal once per level, so a
+   pass reads only the four neighbours of each cell from shared memory and
+   needs no division: a = beta + sum of w a_neighbour with w = alpha/d and
+   beta = -Delta^2 b/d, the same relaxation as relax_value
+   (poisson.h:303-319) up to FP32 rounding.  The pass is bound by the
+   shared-memory bandwidth of the one SM, which this cuts from nine operands
+   per cell to four. */
+__device__ __forceinline__ void bot_sweeps2d_reg (const bmg_geom g, float * a, const float * b,
+                                                  const float * ax, const float * ay, float axc,
+                                                  float ayc, const float * lam, float lamc,
+                                                  float D2, const BCH bc, int nrelax, int nt,
+                                                  bool small)
+{
+  const int n = g.n, P = g.P, nh = n >> 1, total = n*nh;
+  const int lh = 30 - __clz (n);              /* log2 (n) - 1 */
+  int ij[2][2];                               /* i << 16 | j, or -1: no cell */
+  float wx0[2][2], wx1[2][2], wy0[2][2], wy1[2][2], beta[2][2];
+#pragma unroll
+  for (int c = 0; c < 2; c++)
+#pragma unroll
+    for (int k = 0; k < 2; k++) {
+      const int q = threadIdx.x + k*nt;
+      const int i = q >> lh, j = 2*(q & (nh - 1)) + ((c + i) & 1);
+      ij[c][k] = q < total ? (i << 16) | j : -1;
+      wx0[c][k] = wx1[c][k] = wy0[c][k] = wy1[c][k] = beta[c][k] = 0.f;
+      if (q < total) {
+        const int e = (i + 1)*P + 1 + j;
+        const float x0 = ax ? ax[e] : axc, x1 = ax ? ax[e + P] : axc;
+        const float y0 = ay ? ay[e] : ayc, y1 = ay ? ay[e + 1] : ayc;
+        float d = (-(lam ? lam[e] : lamc))*D2;
+        d += x1 + x0;
+        d += y1 + y0;
+        const float inv = 1.f/d;
+        wx0[c][k] = x0*inv; wx1[c][k] = x1*inv; wy0[c][k] = y0*inv; wy1[c][k] = y1*inv;
+        beta[c][k] = ((-D2)*b[e])*inv;
+      }
+    }
+  for (int sw = 0; sw < nrelax; sw++)
+#pragma unroll
+    for (int c = 0; c < 2; c++) {
+      float v[2];
+      int e[2];
+#pragma unroll
+      for (int k = 0; k < 2; k++) {
+        const int t = ij[c][k] < 0 ? 0 : ij[c][k];
+        e[k] = ((t >> 16) + 1)*P + 1 + (t & 0xffff);
+        v[k] = fmaf (wy0[c][k], a[e[k] - 1], fmaf (wy1[c][k], a[e[k] + 1],
+               fmaf (wx0[c][k], a[e[k] - P], fmaf (wx1[c][k], a[e[k] + P], beta[c][k]))));
+      }
+#pragma unroll
+      for (int k = 0; k < 2; k++)
+        if (ij[c][k] >= 0) {
+          a[e[k]] = v[k];
+          ghosts_homog_2d<float> (a, g, ij[c][k] >> 16, ij[c][k] & 0xffff, v[k], bc);
+        }
+      if (small) __syncwarp ();
+      else __syncthreads ();
+    }
+}
+
 template <typename T>
 __device__ __forceinline__ void bot_level2d (const bmg_geom g, void * dav, const void * resv,
                                              const void * axv, const void * ayv, double axc,
@@ -763,6 +903,15 @@ __device__ __forceinline__ void bot_level2d (const bmg_geom g, void * dav, const
   const T * b = (const T *) resv, * ax = (const T *) axv, * ay = (const T *) ayv,
     * lam = (const T *) lamv;
   const T D2 = (T) Delta*(T) Delta;
+  if (sizeof (T) == 4 && g.n >= 2 && g.n*(g.n >> 1) <= 2*nt) {
+    float * af = (float *) dav;
+    const float * bf = (const float *) resv, * axf = (const float *) axv,
+      * ayf = (const float *) ayv, * lamf = (const float *) lamv;
+    const float D2f = (float) Delta*(float) Delta;
+    bot_sweeps2d_reg (g, af, bf, axf, ayf, (float) axc, (float) ayc, lamf, (float) lamc, D2f, bc,
+                      nrelax, nt, small);
+    return;
+  }
   if (ax && lam)
     bot_sweeps2d<T, true, true> (g, a, b, ax, ay, (T) axc, (T) ayc, lam, (T) lamc, D2, bc, nrelax, nt, small);
   else if (ax)
@@ -911,20 +1060,23 @@ int launch_tile (bmg_geom g, void * out, const void * in, const void * res,
 
 extern "C" {
 
-int bmg_tile_sweeps (int st)
+int bmg_tile_sweeps (int st, int n)
 {
-  return st == BMG_ST_F64 ? 4 : 4;
+  (void) st; (void) n;
+  return 4;
 }
 
 int bmg_launch_relax_tile (int dim, int st, bmg_geom g, void * out, const void * in,
                            const void * res, const bmg_coef * alpha, bmg_coef lambda,
                            double Delta, const bmg_bcdesc * bc, int nsweeps, cudaStream_t s)
 {
-  if (dim != 2 || nsweeps < 1 || nsweeps > bmg_tile_sweeps (st)) return (int) cudaErrorInvalidValue;
+  if (dim != 2 || nsweeps < 1 || nsweeps > bmg_tile_sweeps (st, g.n)) return (int) cudaErrorInvalidValue;
   BCH h = bch_of (bc);
   int e;
   /* small levels: 16 x 16 tiles (more CTAs, a shorter critical path per
-     CTA); large levels: big tiles (less halo recomputation) */
+     CTA); large levels: big tiles (less halo recomputation).  A deeper halo
+     on the small levels (twelve sweeps per launch) measured slower: the
+     redundant halo work outweighs the saved launches. */
   const bool small = g.n <= BMG_SMALL_TILE_N;
   if (st == BMG_ST_F64)
     e = small ? launch_tile<double, 16, 4, 8, 32> (g, out, in, res, alpha, lambda, Delta, h, nsweeps, s)

@@ -832,7 +832,7 @@ static int cycle_launches (bmg_grid * g, field_t * a, const levels_t * lv, const
     if (timed) CK (record_event (g->evr0, s));
     if (g->relax == BMG_RELAX_RBGS && dim == 2) {
       /* several complete red-black sweeps per launch, ping-pong buffers */
-      const int S = bmg_tile_sweeps (st);
+      const int S = bmg_tile_sweeps (st, gl.n);
       for (int done = 0; done < nrelax; ) {
         const int k = nrelax - done < S ? nrelax - done : S;
         CL (bmg_launch_relax_tile (dim, st, gl, oth[l], cur[l], lv->res[l], al, la,

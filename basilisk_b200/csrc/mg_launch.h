@@ -113,7 +113,7 @@ int bmg_launch_adjoint_cells (int dim, bmg_geom g, const double * mu, const doub
 int bmg_launch_face_wrap (int dim, bmg_geom g, int face_dim, double * f, cudaStream_t s);
 
 /* fused red-black relaxation (mg_fused.cu) */
-int bmg_tile_sweeps (int st);   /* sweeps one tile launch can do */
+int bmg_tile_sweeps (int st, int n);   /* sweeps one tile launch can do on an n x n level */
 int bmg_launch_relax_tile (int dim, int st, bmg_geom g, void * out, const void * in,
                            const void * res, const bmg_coef * alpha, bmg_coef lambda,
                            double Delta, const bmg_bcdesc * bc, int nsweeps, cudaStream_t s);
