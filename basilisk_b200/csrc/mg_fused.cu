@@ -86,6 +86,20 @@ __device__ __forceinline__ void cp_async_wait_all ()
   asm volatile ("cp.async.wait_group 0;\n" ::: "memory");
 }
 
+/* programmatic dependent launch (sm_90+): with the launch attribute set,
+   a dependent grid may start before this one ends; wait () blocks until
+   the preceding grid has completed and its writes are visible, and is a
+   no-op in a grid launched without the attribute */
+__device__ __forceinline__ void grid_dependency_wait ()
+{
+  asm volatile ("griddepcontrol.wait;" ::: "memory");
+}
+
+__device__ __forceinline__ void grid_dependents_launch ()
+{
+  asm volatile ("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 template <typename T, int TS, int S>
 struct TileShape {
   static constexpr int H = 2*S;        /* halo: one cell per colour pass */
@@ -268,6 +282,9 @@ k_relax_tile2d (bmg_geom g, T * __restrict__ out, const T * __restrict__ in,
   const int base = (i0 + j0) & 1;                             /* colour of (0,0) */
   /* the whole staged region inside the domain: no cell checks needed */
   const bool inner = i0 >= 0 && i0 + W <= n && j0 >= 0 && j0 + W <= n;
+  /* the next launch may start staging its coefficients now: it waits for
+     this grid before it reads the iterate this grid writes */
+  grid_dependents_launch ();
 
   if (inner) {
     /* the staged region lies inside the domain: 16-byte loads of four
@@ -279,14 +296,13 @@ k_relax_tile2d (bmg_geom g, T * __restrict__ out, const T * __restrict__ in,
       const int p = idx/QW, k = idx - p*QW, q = 4*k;
       const int c0 = (base + p + q) & 1;
       const long long id = cidx<2> (g, i0 + p, j0 + q, 0);
-      const Quad<T> va = load_quad (in + id), vr = load_quad (res + id);
+      const Quad<T> vr = load_quad (res + id);
       Quad<T> vl, vx, vy;
       if (LAM) vl = load_quad (lam.p + id);
       if (ax.p) vx = load_quad (ax.p + id);
       else vx.x = vx.y = vx.z = vx.w = ax.c;
       if (ay.p) vy = load_quad (ay.p + id);
       else vy.x = vy.y = vy.z = vy.w = ay.c;
-      put_quad (sa(c0), sa(c0 ^ 1), p*M + 2*k, va);
       put_quad (sr(c0), sr(c0 ^ 1), p*M + 2*k, vr);
       if (LAM) put_quad (sl(c0), sl(c0 ^ 1), p*M + 2*k, vl);
       put_quad (sx(c0), sx(c0 ^ 1), p*M + 2*k, vx);
@@ -308,6 +324,14 @@ k_relax_tile2d (bmg_geom g, T * __restrict__ out, const T * __restrict__ in,
         sy(c)[p*MY + W/2] = ay.p ? ay.p[cidx<2> (g, i0 + p, fj, 0)] : ay.c;
       }
     }
+    /* the iterate is the previous launch's output */
+    grid_dependency_wait ();
+    for (int idx = tid; idx < W*QW; idx += nth) {
+      const int p = idx/QW, k = idx - p*QW, q = 4*k;
+      const int c0 = (base + p + q) & 1;
+      const Quad<T> va = load_quad (in + cidx<2> (g, i0 + p, j0 + q, 0));
+      put_quad (sa(c0), sa(c0 ^ 1), p*M + 2*k, va);
+    }
   }
   else {
   /* stage cells and faces with asynchronous copies (zero fill outside) */
@@ -317,7 +341,6 @@ k_relax_tile2d (bmg_geom g, T * __restrict__ out, const T * __restrict__ in,
     const int ri = real_index (i0 + p, n, px), rj = real_index (j0 + q, n, py);
     const bool ok = ri >= 0 && rj >= 0;
     const long long id = ok ? cidx<2> (g, ri, rj, 0) : 0;
-    cp_async_elem (&sa(c)[p*M + m], in + id, ok);
     cp_async_elem (&sr(c)[p*M + m], res + id, ok);
     if (LAM) cp_async_elem (&sl(c)[p*M + m], lam.p + id, ok);
   }
@@ -338,6 +361,14 @@ k_relax_tile2d (bmg_geom g, T * __restrict__ out, const T * __restrict__ in,
     const bool ok = ri >= 0 && fj >= 0;
     if (ay.p) cp_async_elem (&sy(c)[p*MY + (q >> 1)], ay.p + (ok ? cidx<2> (g, ri, fj, 0) : 0), ok);
     else sy(c)[p*MY + (q >> 1)] = ok ? ay.c : T(0);
+  }
+  grid_dependency_wait ();
+  for (int idx = tid; idx < W*W; idx += nth) {
+    const int p = idx/W, q = idx - p*W;
+    const int c = (base + p + q) & 1, m = q >> 1;
+    const int ri = real_index (i0 + p, n, px), rj = real_index (j0 + q, n, py);
+    const bool ok = ri >= 0 && rj >= 0;
+    cp_async_elem (&sa(c)[p*M + m], in + (ok ? cidx<2> (g, ri, rj, 0) : 0), ok);
   }
   }
   cp_async_wait_all ();
@@ -1039,11 +1070,23 @@ int launch_tile_v (bmg_geom g, void * out, const void * in, const void * res,
     if (e != cudaSuccess) return (int) e;
     configured[dev] = 1;
   }
-  dim3 grid ((g.n + TS - 1)/TS, (g.n + TS - 1)/TS, 1);
-  k_relax_tile2d<T, TS, S, LAM, BX, BY, CPT, MINB><<<grid, dim3 (BX, BY, 1), bytes, s>>>
-    (g, (T *) out, (const T *) in, (const T *) res, coef_of<T> (alpha[0]), coef_of<T> (alpha[1]),
-     coef_of<T> (lambda), (T) Delta, h, nsweeps);
-  return 0;
+  cudaLaunchConfig_t cfg;
+  memset (&cfg, 0, sizeof cfg);
+  cfg.gridDim = dim3 ((g.n + TS - 1)/TS, (g.n + TS - 1)/TS, 1);
+  cfg.blockDim = dim3 (BX, BY, 1);
+  cfg.dynamicSmemBytes = bytes;
+  cfg.stream = s;
+  /* programmatic dependent launch: the kernel stages res and alpha before
+     it waits for the preceding grid, which wrote the iterate it reads */
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return (int) cudaLaunchKernelEx (&cfg, k_relax_tile2d<T, TS, S, LAM, BX, BY, CPT, MINB>, g, (T *) out,
+                                   (const T *) in, (const T *) res, coef_of<T> (alpha[0]),
+                                   coef_of<T> (alpha[1]), coef_of<T> (lambda), (T) Delta, h,
+                                   nsweeps);
 }
 
 template <typename T, int TS, int S, int BX, int BY, int CPT = 2, int MINB = 1>

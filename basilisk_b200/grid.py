@@ -61,11 +61,12 @@ class Field:
         else:
             if _is_torch(values):
                 values = values.detach().cpu().numpy()
-            v = np.ascontiguousarray(values, dtype=np.float64)
-            if v.shape != shape:
-                if v.ndim != 0:
-                    raise ValueError("expected shape %s, got %s" % (shape, v.shape))
+            v = np.asarray(values, dtype=np.float64)
+            if v.ndim == 0:
                 v = np.full(shape, float(v))
+            v = np.ascontiguousarray(v)
+            if v.shape != shape:
+                raise ValueError("expected shape %s, got %s" % (shape, v.shape))
             check(L.bmg_field_set_level(g.ptr, self.scalar, lvl, v.ctypes.data, v.size,
                                         _lib.HOST), "bmg_field_set")
         return self
