@@ -861,41 +861,45 @@ __device__ __forceinline__ void bot_sweeps2d (const bmg_geom g, T * a, const T *
     }
 }
 
-/* all nrelax sweeps of one FP32 2D level whose cells of one colour number
-   at most 2 nt: each thread keeps its (up to two per colour) cells'
-   coefficients in registers, divided by the diagonal once per level, so a
-   pass reads only the four neighbours of each cell from shared memory and
-   needs no division: a = beta + sum of w a_neighbour with w = alpha/d and
-   beta = -Delta^2 b/d, the same relaxation as relax_value
-   (poisson.h:303-319) up to FP32 rounding.  The pass is bound by the
+/* all nrelax sweeps of one 2D level of the mixed form whose cells of one
+   colour number at most 2 nt: each thread keeps its (up to two per colour)
+   cells' coefficients in registers, divided by the diagonal once per
+   level, so a pass reads only the four neighbours of each cell from shared
+   memory and needs no division: a = beta + sum of w a_neighbour with
+   w = alpha/d and beta = -Delta^2 b/d, the relaxation of relax_value
+   (poisson.h:303-319) up to rounding.  The pass is bound by the
    shared-memory bandwidth of the one SM, which this cuts from nine operands
    per cell to four. */
-__device__ __forceinline__ void bot_sweeps2d_reg (const bmg_geom g, float * a, const float * b,
-                                                  const float * ax, const float * ay, float axc,
-                                                  float ayc, const float * lam, float lamc,
-                                                  float D2, const BCH bc, int nrelax, int nt,
+__device__ __forceinline__ float fma_t (float a, float b, float c) { return fmaf (a, b, c); }
+__device__ __forceinline__ double fma_t (double a, double b, double c) { return fma (a, b, c); }
+
+template <typename T, int K>
+__device__ __forceinline__ void bot_sweeps2d_reg (const bmg_geom g, T * a, const T * b,
+                                                  const T * ax, const T * ay, T axc,
+                                                  T ayc, const T * lam, T lamc,
+                                                  T D2, const BCH bc, int nrelax, int nt,
                                                   bool small)
 {
   const int n = g.n, P = g.P, nh = n >> 1, total = n*nh;
   const int lh = 30 - __clz (n);              /* log2 (n) - 1 */
-  int ij[2][2];                               /* i << 16 | j, or -1: no cell */
-  float wx0[2][2], wx1[2][2], wy0[2][2], wy1[2][2], beta[2][2];
+  int ij[2][K];                               /* i << 16 | j, or -1: no cell */
+  T wx0[2][K], wx1[2][K], wy0[2][K], wy1[2][K], beta[2][K];
 #pragma unroll
   for (int c = 0; c < 2; c++)
 #pragma unroll
-    for (int k = 0; k < 2; k++) {
+    for (int k = 0; k < K; k++) {
       const int q = threadIdx.x + k*nt;
       const int i = q >> lh, j = 2*(q & (nh - 1)) + ((c + i) & 1);
       ij[c][k] = q < total ? (i << 16) | j : -1;
-      wx0[c][k] = wx1[c][k] = wy0[c][k] = wy1[c][k] = beta[c][k] = 0.f;
+      wx0[c][k] = wx1[c][k] = wy0[c][k] = wy1[c][k] = beta[c][k] = T(0);
       if (q < total) {
         const int e = (i + 1)*P + 1 + j;
-        const float x0 = ax ? ax[e] : axc, x1 = ax ? ax[e + P] : axc;
-        const float y0 = ay ? ay[e] : ayc, y1 = ay ? ay[e + 1] : ayc;
-        float d = (-(lam ? lam[e] : lamc))*D2;
+        const T x0 = ax ? ax[e] : axc, x1 = ax ? ax[e + P] : axc;
+        const T y0 = ay ? ay[e] : ayc, y1 = ay ? ay[e + 1] : ayc;
+        T d = (-(lam ? lam[e] : lamc))*D2;
         d += x1 + x0;
         d += y1 + y0;
-        const float inv = 1.f/d;
+        const T inv = T(1)/d;
         wx0[c][k] = x0*inv; wx1[c][k] = x1*inv; wy0[c][k] = y0*inv; wy1[c][k] = y1*inv;
         beta[c][k] = ((-D2)*b[e])*inv;
       }
@@ -903,20 +907,20 @@ __device__ __forceinline__ void bot_sweeps2d_reg (const bmg_geom g, float * a, c
   for (int sw = 0; sw < nrelax; sw++)
 #pragma unroll
     for (int c = 0; c < 2; c++) {
-      float v[2];
-      int e[2];
+      T v[K];
+      int e[K];
 #pragma unroll
-      for (int k = 0; k < 2; k++) {
+      for (int k = 0; k < K; k++) {
         const int t = ij[c][k] < 0 ? 0 : ij[c][k];
         e[k] = ((t >> 16) + 1)*P + 1 + (t & 0xffff);
-        v[k] = fmaf (wy0[c][k], a[e[k] - 1], fmaf (wy1[c][k], a[e[k] + 1],
-               fmaf (wx0[c][k], a[e[k] - P], fmaf (wx1[c][k], a[e[k] + P], beta[c][k]))));
+        v[k] = fma_t (wy0[c][k], a[e[k] - 1], fma_t (wy1[c][k], a[e[k] + 1],
+               fma_t (wx0[c][k], a[e[k] - P], fma_t (wx1[c][k], a[e[k] + P], beta[c][k]))));
       }
 #pragma unroll
-      for (int k = 0; k < 2; k++)
+      for (int k = 0; k < K; k++)
         if (ij[c][k] >= 0) {
           a[e[k]] = v[k];
-          ghosts_homog_2d<float> (a, g, ij[c][k] >> 16, ij[c][k] & 0xffff, v[k], bc);
+          ghosts_homog_2d<T> (a, g, ij[c][k] >> 16, ij[c][k] & 0xffff, v[k], bc);
         }
       if (small) __syncwarp ();
       else __syncthreads ();
@@ -928,19 +932,16 @@ __device__ __forceinline__ void bot_level2d (const bmg_geom g, void * dav, const
                                              const void * axv, const void * ayv, double axc,
                                              double ayc, const void * lamv, double lamc,
                                              double Delta, const BCH bc, int nrelax, int nt,
-                                             bool small)
+                                             bool small, int fast)
 {
   T * a = (T *) dav;
   const T * b = (const T *) resv, * ax = (const T *) axv, * ay = (const T *) ayv,
     * lam = (const T *) lamv;
   const T D2 = (T) Delta*(T) Delta;
-  if (sizeof (T) == 4 && g.n >= 2 && g.n*(g.n >> 1) <= 2*nt) {
-    float * af = (float *) dav;
-    const float * bf = (const float *) resv, * axf = (const float *) axv,
-      * ayf = (const float *) ayv, * lamf = (const float *) lamv;
-    const float D2f = (float) Delta*(float) Delta;
-    bot_sweeps2d_reg (g, af, bf, axf, ayf, (float) axc, (float) ayc, lamf, (float) lamc, D2f, bc,
-                      nrelax, nt, small);
+  /* two cells per colour per thread in FP32, one in FP64 (registers) */
+  constexpr int K = sizeof (T) == 4 ? 2 : 1;
+  if (fast && g.n >= 2 && g.n*(g.n >> 1) <= K*nt) {
+    bot_sweeps2d_reg<T, K> (g, a, b, ax, ay, (T) axc, (T) ayc, lam, (T) lamc, D2, bc, nrelax, nt, small);
     return;
   }
   if (ax && lam)
@@ -1029,9 +1030,9 @@ __global__ void __launch_bounds__ (1024, 1) k_bottom (const __grid_constant__ Bo
       const double axc = L.alpha[0].c, ayc = L.alpha[1].c, lamc = L.lambda.c, Delta = L.Delta;
       if (!small || threadIdx.x < 32) {
         if (st == BMG_ST_F64)
-          bot_level2d<double> (gs, da, res, al[0], al[1], axc, ayc, lam, lamc, Delta, bc, nrelax, nt, small);
+          bot_level2d<double> (gs, da, res, al[0], al[1], axc, ayc, lam, lamc, Delta, bc, nrelax, nt, small, L.fast);
         else
-          bot_level2d<float> (gs, da, res, al[0], al[1], axc, ayc, lam, lamc, Delta, bc, nrelax, nt, small);
+          bot_level2d<float> (gs, da, res, al[0], al[1], axc, ayc, lam, lamc, Delta, bc, nrelax, nt, small, L.fast);
       }
     }
     else if (!small || threadIdx.x < 32)

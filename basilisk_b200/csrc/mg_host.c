@@ -754,6 +754,7 @@ static int bottom_top (const bmg_grid * g, const levels_t * lv, const coefs_t * 
       b->alpha[d] = b->st == BMG_ST_F64 ? c->alpha64[l][d] : c->alpha32[l][d];
     b->lambda = b->st == BMG_ST_F64 ? c->lambda64[l] : c->lambda32[l];
     b->Delta = delta_of (g, l);
+    b->fast = g->precision == BMG_MIXED;
     if (l > minlevel && bmg_bottom_smem (g->dim, bl, l - minlevel + 1) > BMG_BOTTOM_SMEM) break;
     top = l;
   }

@@ -127,7 +127,8 @@ typedef struct {
   bmg_coef lambda;
   double Delta;
   int st;
-  int pad_;
+  int fast;     /* relax from weights divided by the diagonal once per level
+                   (not in the reference's evaluation order: mixed form only) */
 } bmg_bottom_level;
 
 /* levels lv[0..nlev-1] (coarse to fine): restriction of res (from the level
