@@ -567,6 +567,260 @@ k_relax_tile2d (bmg_geom g, T * __restrict__ out, const T * __restrict__ in,
 }
 
 /* ---------------------------------------------------------------- */
+/* FP32 tiles with register-resident weights                         */
+/* ---------------------------------------------------------------- */
+
+/* The FP32 red-black sweeps of the mixed form on large 2D levels, S per
+   launch on TS x TS tiles staged with a 2S halo, as k_relax_tile2d, but
+   with the roles of registers and shared memory swapped: each of the 512
+   threads owns eight cells of the staged W x W region for the whole launch
+   (one row, four cells of each colour), reads their coefficients from
+   global memory once and divides them by the diagonal,
+
+     a = beta + w_xl a[-1,0] + w_xu a[1,0] + w_yl a[0,-1] + w_yr a[0,1],
+     w = alpha/d,  beta = -Delta^2 res/d,  d = sum of the four alpha - lambda Delta^2,
+
+   the relaxation of relax_value (poisson.h:303-319) up to FP32 rounding.
+   Only the iterate lives in shared memory (16 KB, split by colour), so a
+   colour pass reads four operands per cell instead of nine and issues four
+   fused multiply-adds per cell instead of a division and eleven
+   operations: the shared-memory pipe, which bounds k_relax_tile2d, carries
+   less than half the traffic. */
+namespace tw {
+constexpr int TS = 48, S = 4, H = 2*S, W = TS + 2*H, M = W/2, WM = W*M, BX = 8, BY = 64;
+static_assert (W == 8*BX && W - 2 <= BY && BY % 8 == 0, "one row of eight cells per thread");
+}
+
+template <bool LAM>
+__global__ void __launch_bounds__ (tw::BX*tw::BY, 2)
+k_relax_tile2d_w (bmg_geom g, float * __restrict__ out, const float * __restrict__ in,
+                  const float * __restrict__ res, Coef<float> ax, Coef<float> ay, Coef<float> lam,
+                  float Delta, BCH bc, int nsweeps)
+{
+  using namespace tw;
+  __shared__ __align__ (16) float sa[2*WM];     /* colour c of staged cell (p, q) at c*WM + p*M + q/2 */
+  const int n = g.n, tx = threadIdx.x, ty = threadIdx.y, tid = ty*BX + tx, nth = BX*BY;
+  constexpr int RW = 32/BX;                     /* rows per warp, all of one parity */
+  const int p = 2*RW*(ty/(2*RW)) + 2*(ty % RW) + ((ty/RW) & 1);
+  const int i0 = blockIdx.y*TS - H, j0 = blockIdx.x*TS - H;
+  const int px = bc.periodic[0], py = bc.periodic[1];
+  const int base = (i0 + j0) & 1;
+  const bool inner = i0 >= 0 && i0 + W <= n && j0 >= 0 && j0 + W <= n;
+  const int q0 = 8*tx, m0 = 4*tx, gi = i0 + p;
+  const float D2 = Delta*Delta;
+  grid_dependents_launch ();
+
+  /* the coefficients of the thread's eight columns q0 .. q0 + 7 of row p
+     (x faces below and above, y faces left of each column and right of the
+     last), res and lambda */
+  float r8[8], xl8[8], xu8[8], yl8[9], l8[8];
+  if (inner) {
+    const long long id = cidx<2> (g, gi, j0 + q0, 0);
+    const Quad<float> r0 = load_quad (res + id), r1 = load_quad (res + id + 4);
+    r8[0] = r0.x; r8[1] = r0.y; r8[2] = r0.z; r8[3] = r0.w;
+    r8[4] = r1.x; r8[5] = r1.y; r8[6] = r1.z; r8[7] = r1.w;
+    if (ax.p) {
+      const Quad<float> a0 = load_quad (ax.p + id), a1 = load_quad (ax.p + id + 4);
+      const Quad<float> b0 = load_quad (ax.p + id + g.P), b1 = load_quad (ax.p + id + g.P + 4);
+      xl8[0] = a0.x; xl8[1] = a0.y; xl8[2] = a0.z; xl8[3] = a0.w;
+      xl8[4] = a1.x; xl8[5] = a1.y; xl8[6] = a1.z; xl8[7] = a1.w;
+      xu8[0] = b0.x; xu8[1] = b0.y; xu8[2] = b0.z; xu8[3] = b0.w;
+      xu8[4] = b1.x; xu8[5] = b1.y; xu8[6] = b1.z; xu8[7] = b1.w;
+    }
+    else
+#pragma unroll
+      for (int q = 0; q < 8; q++) xl8[q] = xu8[q] = ax.c;
+    if (ay.p) {
+      const Quad<float> a0 = load_quad (ay.p + id), a1 = load_quad (ay.p + id + 4);
+      yl8[0] = a0.x; yl8[1] = a0.y; yl8[2] = a0.z; yl8[3] = a0.w;
+      yl8[4] = a1.x; yl8[5] = a1.y; yl8[6] = a1.z; yl8[7] = a1.w;
+      yl8[8] = ay.p[id + 8];
+    }
+    else
+#pragma unroll
+      for (int q = 0; q < 9; q++) yl8[q] = ay.c;
+    if (LAM) {
+      const Quad<float> a0 = load_quad (lam.p + id), a1 = load_quad (lam.p + id + 4);
+      l8[0] = a0.x; l8[1] = a0.y; l8[2] = a0.z; l8[3] = a0.w;
+      l8[4] = a1.x; l8[5] = a1.y; l8[6] = a1.z; l8[7] = a1.w;
+    }
+  }
+  else {
+    /* outside the domain: zero, or the periodic image */
+    const int ri = real_index (gi, n, px);
+    const int flo = real_face (gi, n, px), fhi = real_face (gi + 1, n, px);
+#pragma unroll
+    for (int q = 0; q < 9; q++) {
+      const int rj = real_index (j0 + q0 + q, n, py), fj = real_face (j0 + q0 + q, n, py);
+      yl8[q] = ri >= 0 && fj >= 0 ? ay.at (cidx<2> (g, ri, fj, 0)) : 0.f;
+      if (q == 8) break;
+      const bool ok = ri >= 0 && rj >= 0;
+      r8[q] = ok ? res[cidx<2> (g, ri, rj, 0)] : 0.f;
+      xl8[q] = flo >= 0 && rj >= 0 ? ax.at (cidx<2> (g, flo, rj, 0)) : 0.f;
+      xu8[q] = fhi >= 0 && rj >= 0 ? ax.at (cidx<2> (g, fhi, rj, 0)) : 0.f;
+      if (LAM) l8[q] = ok ? lam.p[cidx<2> (g, ri, rj, 0)] : 0.f;
+    }
+  }
+  /* weights of cell e of colour c: column 2e + o_c of the eight */
+  float wxl[2][4], wxu[2][4], wyl[2][4], wyr[2][4], be[2][4];
+  unsigned valid = 0;                           /* bit 4c + e: a cell that is updated */
+  const bool rowok = px || (unsigned) gi < (unsigned) n;
+#pragma unroll
+  for (int c = 0; c < 2; c++)
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+      /* column 2e or 2e + 1 (selects with constant indices: a runtime
+         index would put the arrays in local memory) */
+      const bool odd = (c ^ base ^ p) & 1;
+      const int q = 2*e + (odd ? 1 : 0);
+      const float xl = odd ? xl8[2*e + 1] : xl8[2*e], xu = odd ? xu8[2*e + 1] : xu8[2*e];
+      const float yl = odd ? yl8[2*e + 1] : yl8[2*e], yr = odd ? yl8[2*e + 2] : yl8[2*e + 1];
+      const float rv = odd ? r8[2*e + 1] : r8[2*e];
+      const float lv = LAM ? (odd ? l8[2*e + 1] : l8[2*e]) : lam.c;
+      const bool ok = rowok && (py || (unsigned) (j0 + q0 + q) < (unsigned) n);
+      float d = (-lv)*D2;
+      d += xu + xl;
+      d += yr + yl;
+      const float inv = ok ? 1.f/d : 0.f;
+      wxl[c][e] = xl*inv; wxu[c][e] = xu*inv;
+      wyl[c][e] = yl*inv; wyr[c][e] = yr*inv;
+      be[c][e] = ((-D2)*rv)*inv;
+      valid |= (ok ? 1u : 0u) << (4*c + e);
+    }
+
+  /* the iterate is the previous launch's output */
+  grid_dependency_wait ();
+  const int cq = (base + p) & 1;                /* colour of the even columns */
+  if (inner) {
+    const long long id = cidx<2> (g, gi, j0 + q0, 0);
+    const Quad<float> va = load_quad (in + id), vb = load_quad (in + id + 4);
+    put_quad (sa + cq*WM, sa + (cq ^ 1)*WM, p*M + m0, va);
+    put_quad (sa + cq*WM, sa + (cq ^ 1)*WM, p*M + m0 + 2, vb);
+  }
+  else {
+    const int ri = real_index (gi, n, px);
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+      const int rj = real_index (j0 + q0 + q, n, py);
+      sa[((cq + q) & 1)*WM + p*M + ((q0 + q) >> 1)] =
+        ri >= 0 && rj >= 0 ? in[cidx<2> (g, ri, rj, 0)] : 0.f;
+    }
+  }
+  __syncthreads ();
+
+  /* box ghosts (global -1 and n) of the staged region: ghost = factor x
+     mirror */
+  const int glo_i = px ? -1 : -1 - i0, ghi_i = px ? -1 : n - i0;
+  const int glo_j = py ? -1 : -1 - j0, ghi_j = py ? -1 : n - j0;
+  const bool has_ghosts = !inner &&
+    ((glo_i >= 0 && glo_i < W) || (ghi_i >= 0 && ghi_i < W) ||
+     (glo_j >= 0 && glo_j < W) || (ghi_j >= 0 && ghi_j < W));
+  auto refresh = [&] () {
+    for (int t = tid; t < 4*W; t += nth) {
+      const int line = t/W, u = t - line*W;
+      int pp, q, pm, qm, f;
+      if (line == 0) { pp = glo_i; q = u; pm = pp + 1; qm = q; f = bc.fac[1]; }
+      else if (line == 1) { pp = ghi_i; q = u; pm = pp - 1; qm = q; f = bc.fac[0]; }
+      else if (line == 2) { pp = u; q = glo_j; pm = pp; qm = q + 1; f = bc.fac[3]; }
+      else { pp = u; q = ghi_j; pm = pp; qm = q - 1; f = bc.fac[2]; }
+      if (pp < 0 || pp >= W || q < 0 || q >= W || pm < 0 || pm >= W || qm < 0 || qm >= W)
+        continue;
+      if (line < 2 ? real_index (j0 + q, n, py) < 0 : real_index (i0 + pp, n, px) < 0)
+        continue;
+      const int c = (base + pp + q) & 1;
+      sa[c*WM + pp*M + (q >> 1)] = sa[(c ^ 1)*WM + pm*M + (qm >> 1)]*float(f);
+    }
+  };
+  if (has_ghosts) {
+    refresh ();
+    __syncthreads ();
+  }
+
+  for (int sw = 0; sw < nsweeps; sw++)
+#pragma unroll
+    for (int c = 0; c < 2; c++) {
+      const int k = 2*sw + c;
+      if (p >= k + 1 && p < W - k - 1) {
+        const int o = (c ^ base ^ p) & 1;
+        const float * A = sa + (c ^ 1)*WM + p*M + m0;      /* the other colour */
+        const float4 up = *(const float4 *) (A - M), dn = *(const float4 *) (A + M);
+        const float4 mid = *(const float4 *) A;
+        float v[5];
+        if (o == 0) { v[0] = A[-1]; v[1] = mid.x; v[2] = mid.y; v[3] = mid.z; v[4] = mid.w; }
+        else { v[0] = mid.x; v[1] = mid.y; v[2] = mid.z; v[3] = mid.w; v[4] = A[4]; }
+        const float upv[4] = {up.x, up.y, up.z, up.w}, dnv[4] = {dn.x, dn.y, dn.z, dn.w};
+        float nv[4];
+#pragma unroll
+        for (int e = 0; e < 4; e++)
+          nv[e] = fmaf (wyr[c][e], v[e + 1], fmaf (wyl[c][e], v[e],
+                  fmaf (wxu[c][e], dnv[e], fmaf (wxl[c][e], upv[e], be[c][e]))));
+        /* the valid columns of colour c shrink by one cell per pass */
+        const int mlo = (k + 2 - o) >> 1, mhi = (W - k - o) >> 1;
+        float * a = sa + c*WM + p*M + m0;
+        const unsigned vc = (valid >> (4*c)) & 15u;
+        if (vc == 15u && m0 >= mlo && m0 + 4 <= mhi)
+          *(float4 *) a = make_float4 (nv[0], nv[1], nv[2], nv[3]);
+        else {
+#pragma unroll
+          for (int e = 0; e < 4; e++)
+            if (((vc >> e) & 1u) && m0 + e >= mlo && m0 + e < mhi) a[e] = nv[e];
+        }
+      }
+      __syncthreads ();
+      if (has_ghosts) {
+        refresh ();
+        __syncthreads ();
+      }
+    }
+
+  /* the tile interior back, with its ghost images */
+  if (inner) {
+    constexpr int QT = TS/4;
+    for (int idx = tid; idx < TS*QT; idx += nth) {
+      const int rr = idx/QT, k = idx - rr*QT;
+      const int pp = rr + H, q = H + 4*k, c0 = (base + pp + q) & 1, m = q >> 1;
+      Quad<float> v;
+      v.x = sa[c0*WM + pp*M + m]; v.z = sa[c0*WM + pp*M + m + 1];
+      v.y = sa[(c0 ^ 1)*WM + pp*M + m]; v.w = sa[(c0 ^ 1)*WM + pp*M + m + 1];
+      store_quad (out + cidx<2> (g, blockIdx.y*TS + rr, blockIdx.x*TS + 4*k, 0), v);
+    }
+    return;
+  }
+  for (int idx = tid; idx < TS*TS; idx += nth) {
+    const int rr = idx/TS, s = idx - rr*TS;
+    const int oi = blockIdx.y*TS + rr, oj = blockIdx.x*TS + s;
+    if (oi >= n || oj >= n) continue;
+    const int pp = rr + H, q = s + H;
+    const float v = sa[((base + pp + q) & 1)*WM + pp*M + (q >> 1)];
+    out[cidx<2> (g, oi, oj, 0)] = v;
+    ghosts_homog<2, float> (out, g, oi, oj, 0, v, bc);
+  }
+}
+
+template <bool LAM>
+int launch_tile_w (bmg_geom g, void * out, const void * in, const void * res,
+                   const bmg_coef * alpha, bmg_coef lambda, double Delta, BCH h, int nsweeps,
+                   cudaStream_t s)
+{
+  using namespace tw;
+  cudaLaunchConfig_t cfg;
+  memset (&cfg, 0, sizeof cfg);
+  cfg.gridDim = dim3 ((g.n + TS - 1)/TS, (g.n + TS - 1)/TS, 1);
+  cfg.blockDim = dim3 (BX, BY, 1);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return (int) cudaLaunchKernelEx (&cfg, k_relax_tile2d_w<LAM>, g, (float *) out, (const float *) in,
+                                   (const float *) res, coef_of<float> (alpha[0]),
+                                   coef_of<float> (alpha[1]), coef_of<float> (lambda),
+                                   (float) Delta, h, nsweeps);
+}
+
+/* ---------------------------------------------------------------- */
 /* single-CTA bottom of the cycle                                    */
 /* ---------------------------------------------------------------- */
 
@@ -1127,7 +1381,8 @@ int bmg_launch_relax_tile (int dim, int st, bmg_geom g, void * out, const void *
       : launch_tile<double, 40, 4, 16, 64> (g, out, in, res, alpha, lambda, Delta, h, nsweeps, s);
   else
     e = small ? launch_tile<float, 16, 4, 8, 32> (g, out, in, res, alpha, lambda, Delta, h, nsweeps, s)
-      : launch_tile<float, 48, 4, 8, 64, 4, 3> (g, out, in, res, alpha, lambda, Delta, h, nsweeps, s);
+      : lambda.p ? launch_tile_w<true> (g, out, in, res, alpha, lambda, Delta, h, nsweeps, s)
+      : launch_tile_w<false> (g, out, in, res, alpha, lambda, Delta, h, nsweeps, s);
   if (e) return e;
   cudaError_t r = cudaGetLastError ();
   return r == cudaSuccess ? 0 : (int) r;

@@ -87,6 +87,28 @@ def test_rbgs_large_levels_bit_exact(case):
     assert_same(ost, gst, og.get_a(), a.get(), prob["b"])
 
 
+@pytest.mark.parametrize("case", range(len(LARGE)))
+def test_mixed_large_levels(case):
+    """The mixed form on the same large levels (FP32 tiles with
+    register-resident weights on levels of 512^2 and more: domain edges,
+    periodic wrap, constant and stored alpha and lambda): it converges to
+    the tolerance in about the oracle's number of cycles, to the oracle's
+    solution within the tolerance-implied bound."""
+    dim, depth, per, bc, al, lam = LARGE[case]
+    rng = np.random.default_rng(300 + case)
+    prob = random_problem(dim, depth, rng, periodic=per, bc=bc, alpha=al, lam=lam)
+    og = oracle_grid(prob, relax=RELAX["rbgs"])
+    ost = og.poisson(tolerance=1e-7)
+    g, a, b, alpha, lamf = gpu_grid(prob, relax="rbgs", precision="mixed")
+    gst = g.poisson(a, b, alpha=alpha, lambda_=lamf, tolerance=1e-7)
+    assert gst["resa"] <= 1e-7, gst
+    assert gst["i"] <= 1.25 * ost["i"] + 1, (gst, ost)
+    ref, got = og.get_a(), a.get()
+    if per and lam is None:          # defined up to a constant
+        ref, got = ref - ref.mean(), got - got.mean()
+    assert np.abs(got - ref).max() <= 1e-4 * max(1.0, np.abs(ref).max())
+
+
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_two_phase_rbgs(precision):
     """The two-phase recipe at 256^2 on the red-black path: bit-identical in
