@@ -661,6 +661,25 @@ k_relax_tile2d_w (bmg_geom g, float * __restrict__ out, const float * __restrict
       if (LAM) l8[q] = ok ? lam.p[cidx<2> (g, ri, rj, 0)] : 0.f;
     }
   }
+  /* the iterate is the previous launch's output: its loads are issued
+     before the weights are computed, so that both round trips overlap */
+  grid_dependency_wait ();
+  const int cq = (base + p) & 1;                /* colour of the even columns */
+  if (inner) {
+    const long long id = cidx<2> (g, gi, j0 + q0, 0);
+    const Quad<float> va = load_quad (in + id), vb = load_quad (in + id + 4);
+    put_quad (sa + cq*WM, sa + (cq ^ 1)*WM, p*M + m0, va);
+    put_quad (sa + cq*WM, sa + (cq ^ 1)*WM, p*M + m0 + 2, vb);
+  }
+  else {
+    const int ri = real_index (gi, n, px);
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+      const int rj = real_index (j0 + q0 + q, n, py);
+      sa[((cq + q) & 1)*WM + p*M + ((q0 + q) >> 1)] =
+        ri >= 0 && rj >= 0 ? in[cidx<2> (g, ri, rj, 0)] : 0.f;
+    }
+  }
   /* weights of cell e of colour c: column 2e + o_c of the eight */
   float wxl[2][4], wxu[2][4], wyl[2][4], wyr[2][4], be[2][4];
   unsigned valid = 0;                           /* bit 4c + e: a cell that is updated */
@@ -681,31 +700,13 @@ k_relax_tile2d_w (bmg_geom g, float * __restrict__ out, const float * __restrict
       float d = (-lv)*D2;
       d += xu + xl;
       d += yr + yl;
-      const float inv = ok ? 1.f/d : 0.f;
+      const float inv = ok ? __fdividef (1.f, d) : 0.f;
       wxl[c][e] = xl*inv; wxu[c][e] = xu*inv;
       wyl[c][e] = yl*inv; wyr[c][e] = yr*inv;
       be[c][e] = ((-D2)*rv)*inv;
       valid |= (ok ? 1u : 0u) << (4*c + e);
     }
 
-  /* the iterate is the previous launch's output */
-  grid_dependency_wait ();
-  const int cq = (base + p) & 1;                /* colour of the even columns */
-  if (inner) {
-    const long long id = cidx<2> (g, gi, j0 + q0, 0);
-    const Quad<float> va = load_quad (in + id), vb = load_quad (in + id + 4);
-    put_quad (sa + cq*WM, sa + (cq ^ 1)*WM, p*M + m0, va);
-    put_quad (sa + cq*WM, sa + (cq ^ 1)*WM, p*M + m0 + 2, vb);
-  }
-  else {
-    const int ri = real_index (gi, n, px);
-#pragma unroll
-    for (int q = 0; q < 8; q++) {
-      const int rj = real_index (j0 + q0 + q, n, py);
-      sa[((cq + q) & 1)*WM + p*M + ((q0 + q) >> 1)] =
-        ri >= 0 && rj >= 0 ? in[cidx<2> (g, ri, rj, 0)] : 0.f;
-    }
-  }
   __syncthreads ();
 
   /* box ghosts (global -1 and n) of the staged region: ghost = factor x
