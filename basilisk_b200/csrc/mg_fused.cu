@@ -591,6 +591,36 @@ constexpr int TS = 48, S = 4, H = 2*S, W = TS + 2*H, M = W/2, WM = W*M, BX = 8, 
 static_assert (W == 8*BX && W - 2 <= BY && BY % 8 == 0, "one row of eight cells per thread");
 }
 
+/* shared-memory accesses by 32-bit byte address plus a constant offset
+   (volatile: kept in program order with the barriers) */
+template <int OFF>
+__device__ __forceinline__ float4 lds_f4 (unsigned a)
+{
+  float4 v;
+  asm volatile ("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4+%5];"
+                : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "r"(a), "n"(OFF));
+  return v;
+}
+
+template <int OFF>
+__device__ __forceinline__ float lds_f1 (unsigned a)
+{
+  float v;
+  asm volatile ("ld.shared.f32 %0, [%1+%2];" : "=f"(v) : "r"(a), "n"(OFF));
+  return v;
+}
+
+__device__ __forceinline__ void sts_f4 (unsigned a, float4 v)
+{
+  asm volatile ("st.shared.v4.f32 [%0], {%1, %2, %3, %4};"
+                :: "r"(a), "f"(v.x), "f"(v.y), "f"(v.z), "f"(v.w) : "memory");
+}
+
+__device__ __forceinline__ void sts_f1 (unsigned a, float v)
+{
+  asm volatile ("st.shared.f32 [%0], %1;" :: "r"(a), "f"(v) : "memory");
+}
+
 template <bool LAM>
 __global__ void __launch_bounds__ (tw::BX*tw::BY, 2)
 k_relax_tile2d_w (bmg_geom g, float * __restrict__ out, const float * __restrict__ in,
@@ -737,34 +767,43 @@ k_relax_tile2d_w (bmg_geom g, float * __restrict__ out, const float * __restrict
     __syncthreads ();
   }
 
+  /* the colour passes.  Rows shrink by one per pass (whole warps drop out);
+     columns do not: a cell next to the staged region's edge may be updated
+     from stale neighbours, but staleness moves inward by one cell per pass
+     and never reaches the TS x TS interior after 2S passes, so only cells
+     outside the domain (box ghosts, refreshed from their mirrors) are
+     masked.  Shared memory is addressed by 32-bit byte offsets with the
+     row offsets as immediates. */
+  const unsigned sbase = (unsigned) __cvta_generic_to_shared (sa);
+  const int o0 = (base ^ p) & 1;               /* column offset of colour 0 in row p */
   for (int sw = 0; sw < nsweeps; sw++)
 #pragma unroll
     for (int c = 0; c < 2; c++) {
       const int k = 2*sw + c;
       if (p >= k + 1 && p < W - k - 1) {
-        const int o = (c ^ base ^ p) & 1;
-        const float * A = sa + (c ^ 1)*WM + p*M + m0;      /* the other colour */
-        const float4 up = *(const float4 *) (A - M), dn = *(const float4 *) (A + M);
-        const float4 mid = *(const float4 *) A;
+        const int o = o0 ^ c;
+        /* the other colour's quad at rows p - 1, p, p + 1 and its left or
+           right neighbour in row p */
+        const unsigned aup = sbase + 4u*((c ^ 1)*WM + (p - 1)*M + m0);
+        const float4 up = lds_f4<0> (aup), mid = lds_f4<4*M> (aup), dn = lds_f4<8*M> (aup);
         float v[5];
-        if (o == 0) { v[0] = A[-1]; v[1] = mid.x; v[2] = mid.y; v[3] = mid.z; v[4] = mid.w; }
-        else { v[0] = mid.x; v[1] = mid.y; v[2] = mid.z; v[3] = mid.w; v[4] = A[4]; }
+        if (o == 0) { v[0] = lds_f1<4*M - 4> (aup); v[1] = mid.x; v[2] = mid.y; v[3] = mid.z; v[4] = mid.w; }
+        else { v[0] = mid.x; v[1] = mid.y; v[2] = mid.z; v[3] = mid.w; v[4] = lds_f1<4*M + 16> (aup); }
         const float upv[4] = {up.x, up.y, up.z, up.w}, dnv[4] = {dn.x, dn.y, dn.z, dn.w};
         float nv[4];
 #pragma unroll
         for (int e = 0; e < 4; e++)
           nv[e] = fmaf (wyr[c][e], v[e + 1], fmaf (wyl[c][e], v[e],
                   fmaf (wxu[c][e], dnv[e], fmaf (wxl[c][e], upv[e], be[c][e]))));
-        /* the valid columns of colour c shrink by one cell per pass */
-        const int mlo = (k + 2 - o) >> 1, mhi = (W - k - o) >> 1;
-        float * a = sa + c*WM + p*M + m0;
+        const unsigned aw = sbase + 4u*(c*WM + p*M + m0);
         const unsigned vc = (valid >> (4*c)) & 15u;
-        if (vc == 15u && m0 >= mlo && m0 + 4 <= mhi)
-          *(float4 *) a = make_float4 (nv[0], nv[1], nv[2], nv[3]);
+        if (vc == 15u)
+          sts_f4 (aw, make_float4 (nv[0], nv[1], nv[2], nv[3]));
         else {
-#pragma unroll
-          for (int e = 0; e < 4; e++)
-            if (((vc >> e) & 1u) && m0 + e >= mlo && m0 + e < mhi) a[e] = nv[e];
+          if (vc & 1u) sts_f1 (aw, nv[0]);
+          if (vc & 2u) sts_f1 (aw + 4, nv[1]);
+          if (vc & 4u) sts_f1 (aw + 8, nv[2]);
+          if (vc & 8u) sts_f1 (aw + 12, nv[3]);
         }
       }
       __syncthreads ();
