@@ -867,6 +867,10 @@ int launch_tile_w (bmg_geom g, void * out, const void * in, const void * res,
 typedef bmg_bottom_level BotLevel;
 
 #define BOT_MAXLEVELS 14
+/* threads of the bottom CTA: 512 leaves each up to 128 registers, enough
+   for the register-resident weights of four cells per colour without
+   spilling */
+#define BOT_THREADS 512
 /* levels up to this size use the small relaxation tiles */
 #define BMG_SMALL_TILE_N 256
 /* staged levels up to this many padded cells are relaxed by one warp */
@@ -1156,7 +1160,7 @@ __device__ __forceinline__ void bot_sweeps2d (const bmg_geom g, T * a, const T *
 }
 
 /* all nrelax sweeps of one 2D level of the mixed form whose cells of one
-   colour number at most 2 nt: each thread keeps its (up to two per colour)
+   colour number at most K nt: each thread keeps its (up to K per colour)
    cells' coefficients in registers, divided by the diagonal once per
    level, so a pass reads only the four neighbours of each cell from shared
    memory and needs no division: a = beta + sum of w a_neighbour with
@@ -1177,6 +1181,11 @@ __device__ __forceinline__ void bot_sweeps2d_reg (const bmg_geom g, T * a, const
   const int n = g.n, P = g.P, nh = n >> 1, total = n*nh;
   const int lh = 30 - __clz (n);              /* log2 (n) - 1 */
   int ij[2][K];                               /* i << 16 | j, or -1: no cell */
+  /* the ghost images of a boundary cell (ghosts_homog_2d, with the box
+     factors +-1 as signs): bits 0/1 a column / row ghost, bits 2/3 their
+     signs, bits 8-15 the column offset, bits 16-31 the row offset in
+     elements; 0 for an interior cell */
+  int gw[2][K];
   T wx0[2][K], wx1[2][K], wy0[2][K], wy1[2][K], beta[2][K];
 #pragma unroll
   for (int c = 0; c < 2; c++)
@@ -1185,6 +1194,18 @@ __device__ __forceinline__ void bot_sweeps2d_reg (const bmg_geom g, T * a, const
       const int q = threadIdx.x + k*nt;
       const int i = q >> lh, j = 2*(q & (nh - 1)) + ((c + i) & 1);
       ij[c][k] = q < total ? (i << 16) | j : -1;
+      {
+        int w = 0;
+        if (q < total && (i == 0 || i == n - 1 || j == 0 || j == n - 1)) {
+          int ro = 0, co = 0, si = 0, sj = 0;
+          if (i == 0) { ro = (bc.periodic[0] ? n : -1)*P; si = bc.periodic[0] ? 0 : bc.fac[1] < 0; }
+          else if (i == n - 1) { ro = (bc.periodic[0] ? -n : 1)*P; si = bc.periodic[0] ? 0 : bc.fac[0] < 0; }
+          if (j == 0) { co = bc.periodic[1] ? n : -1; sj = bc.periodic[1] ? 0 : bc.fac[3] < 0; }
+          else if (j == n - 1) { co = bc.periodic[1] ? -n : 1; sj = bc.periodic[1] ? 0 : bc.fac[2] < 0; }
+          w = (ro << 16) | ((co & 0xff) << 8) | (si << 3) | (sj << 2) | (ro ? 2 : 0) | (co ? 1 : 0);
+        }
+        gw[c][k] = w;
+      }
       wx0[c][k] = wx1[c][k] = wy0[c][k] = wy1[c][k] = beta[c][k] = T(0);
       if (q < total) {
         const int e = (i + 1)*P + 1 + j;
@@ -1214,7 +1235,14 @@ __device__ __forceinline__ void bot_sweeps2d_reg (const bmg_geom g, T * a, const
       for (int k = 0; k < K; k++)
         if (ij[c][k] >= 0) {
           a[e[k]] = v[k];
-          ghosts_homog_2d<T> (a, g, ij[c][k] >> 16, ij[c][k] & 0xffff, v[k], bc);
+          const int w = gw[c][k];
+          if (w) {
+            const int ro = w >> 16, co = (signed char) ((w >> 8) & 0xff);
+            const T vi = (w & 8) ? -v[k] : v[k], vj = (w & 4) ? -v[k] : v[k];
+            if (w & 2) a[e[k] + ro] = vi;
+            if (w & 1) a[e[k] + co] = vj;
+            if ((w & 3) == 3) a[e[k] + ro + co] = (w & 4) ? -vi : vi;
+          }
         }
       if (small) __syncwarp ();
       else __syncthreads ();
@@ -1232,8 +1260,8 @@ __device__ __forceinline__ void bot_level2d (const bmg_geom g, void * dav, const
   const T * b = (const T *) resv, * ax = (const T *) axv, * ay = (const T *) ayv,
     * lam = (const T *) lamv;
   const T D2 = (T) Delta*(T) Delta;
-  /* two cells per colour per thread in FP32, one in FP64 (registers) */
-  constexpr int K = sizeof (T) == 4 ? 2 : 1;
+  /* four cells per colour per thread in FP32, two in FP64 (registers) */
+  constexpr int K = sizeof (T) == 4 ? 4 : 2;
   if (fast && g.n >= 2 && g.n*(g.n >> 1) <= K*nt) {
     bot_sweeps2d_reg<T, K> (g, a, b, ax, ay, (T) axc, (T) ayc, lam, (T) lamc, D2, bc, nrelax, nt, small);
     return;
@@ -1269,7 +1297,7 @@ __device__ __forceinline__ void bot_prolong_st (int stc, const bmg_geom & gc, co
 }
 
 template <int DIM>
-__global__ void __launch_bounds__ (1024, 1) k_bottom (const __grid_constant__ BotParams P)
+__global__ void __launch_bounds__ (BOT_THREADS, 1) k_bottom (const __grid_constant__ BotParams P)
 {
   extern __shared__ __align__ (16) unsigned char bsm[];
   const BCH bc = P.bc;
@@ -1484,9 +1512,9 @@ int bmg_launch_bottom (int dim, const bmg_bottom_level * lv, int nlev, bmg_geom 
     if (e != cudaSuccess) return (int) e;
     configured[dev][dim - 1] = 1;
   }
-  if (dim == 1) k_bottom<1><<<1, 1024, bytes, s>>> (P);
-  else if (dim == 2) k_bottom<2><<<1, 1024, bytes, s>>> (P);
-  else k_bottom<3><<<1, 1024, bytes, s>>> (P);
+  if (dim == 1) k_bottom<1><<<1, BOT_THREADS, bytes, s>>> (P);
+  else if (dim == 2) k_bottom<2><<<1, BOT_THREADS, bytes, s>>> (P);
+  else k_bottom<3><<<1, BOT_THREADS, bytes, s>>> (P);
   cudaError_t r = cudaGetLastError ();
   return r == cudaSuccess ? 0 : (int) r;
 }
