@@ -32,6 +32,7 @@
  * a C build of the same expressions.
  */
 #include <cuda_runtime.h>
+#include <math.h>
 #include <stdint.h>
 #include <stdio.h>
 #include "mg_launch.h"
@@ -202,7 +203,16 @@ __device__ __forceinline__ void block_max_atomic (double m, unsigned long long *
   }
 }
 
-template <int DIM, typename TR>
+/* x/Delta; when Delta is a power of two (L0 = 1, Delta = 2^-l) the
+   division is an exact scaling and x*(1/Delta) is the same double, at a
+   fraction of the cost of the IEEE division */
+template <bool POW2>
+__device__ __forceinline__ double over_delta (double x, double Delta, double rDelta)
+{
+  return POW2 ? x*rDelta : x/Delta;
+}
+
+template <int DIM, typename TR, bool POW2>
 __global__ void k_residual (bmg_geom g, bmg_geom gr, const double * __restrict__ a,
                             const double * __restrict__ b, Coef<double> ax,
                             Coef<double> ay, Coef<double> az, Coef<double> lam,
@@ -211,21 +221,25 @@ __global__ void k_residual (bmg_geom g, bmg_geom gr, const double * __restrict__
 {
   int i, j, k;
   double m = 0.;
+  const double rD = 1./Delta;
   if (cell_of_thread<DIM> (g.n, i, j, k)) {
     const long long id = cidx<DIM> (g, i, j, k);
     const double ac = a[id];
     double r = b[id] - lam.at (id)*ac;
     {
       long long s = cstride<DIM> (g, 0);
-      r += (ax.at (id)*((ac - a[id - s])/Delta) - ax.at (id + s)*((a[id + s] - ac)/Delta))/Delta;
+      r += over_delta<POW2> (ax.at (id)*over_delta<POW2> (ac - a[id - s], Delta, rD) -
+                             ax.at (id + s)*over_delta<POW2> (a[id + s] - ac, Delta, rD), Delta, rD);
     }
     if (DIM > 1) {
       long long s = cstride<DIM> (g, 1);
-      r += (ay.at (id)*((ac - a[id - s])/Delta) - ay.at (id + s)*((a[id + s] - ac)/Delta))/Delta;
+      r += over_delta<POW2> (ay.at (id)*over_delta<POW2> (ac - a[id - s], Delta, rD) -
+                             ay.at (id + s)*over_delta<POW2> (a[id + s] - ac, Delta, rD), Delta, rD);
     }
     if (DIM > 2) {
       long long s = cstride<DIM> (g, 2);
-      r += (az.at (id)*((ac - a[id - s])/Delta) - az.at (id + s)*((a[id + s] - ac)/Delta))/Delta;
+      r += over_delta<POW2> (az.at (id)*over_delta<POW2> (ac - a[id - s], Delta, rD) -
+                             az.at (id + s)*over_delta<POW2> (a[id + s] - ac, Delta, rD), Delta, rD);
     }
     res[cidx<DIM> (gr, i, j, k)] = (TR) r;
     m = fabs (r);
@@ -491,10 +505,16 @@ void residual_dim (int st, bmg_geom g, bmg_geom gr, const double * a, const doub
   Coef<double> ax = coef_of<double> (alpha[0]), ay = coef_of<double> (alpha[1]),
     az = coef_of<double> (alpha[2]), lam = coef_of<double> (lambda);
   dim3 gb = grid_shape<DIM> (g.n), bb = block_shape<DIM> ();
-  if (st == BMG_ST_F64)
-    k_residual<DIM, double><<<gb, bb, 0, s>>> (g, gr, a, b, ax, ay, az, lam, Delta, (double *) res, maxres);
-  else
-    k_residual<DIM, float><<<gb, bb, 0, s>>> (g, gr, a, b, ax, ay, az, lam, Delta, (float *) res, maxres);
+  int ex;
+  const bool pow2 = Delta > 0. && frexp (Delta, &ex) == 0.5 && ex > -1000 && ex < 1000;
+  if (st == BMG_ST_F64) {
+    if (pow2) k_residual<DIM, double, true><<<gb, bb, 0, s>>> (g, gr, a, b, ax, ay, az, lam, Delta, (double *) res, maxres);
+    else k_residual<DIM, double, false><<<gb, bb, 0, s>>> (g, gr, a, b, ax, ay, az, lam, Delta, (double *) res, maxres);
+  }
+  else {
+    if (pow2) k_residual<DIM, float, true><<<gb, bb, 0, s>>> (g, gr, a, b, ax, ay, az, lam, Delta, (float *) res, maxres);
+    else k_residual<DIM, float, false><<<gb, bb, 0, s>>> (g, gr, a, b, ax, ay, az, lam, Delta, (float *) res, maxres);
+  }
 }
 
 template <int DIM>

@@ -68,6 +68,20 @@ def test_poisson_bit_exact(case, relax):
     assert_same(ost, gst, og.get_a(), a.get(), prob["b"])
 
 
+@pytest.mark.parametrize("L0", [1.0, 3.0, 0.25])
+def test_domain_size_bit_exact(L0):
+    """Delta = L0/2^l: a power of two (the residual scales by 1/Delta
+    exactly) or not (it divides, in the reference's order); both
+    bit-identical to the oracle."""
+    rng = np.random.default_rng(17)
+    prob = random_problem(2, 6, rng, bc={s: ("dirichlet", 0.0) for s in range(4)}, alpha="field")
+    og = oracle_grid(prob, relax=RELAX["rbgs"], L0=L0)
+    ost = og.poisson(tolerance=1e-7)
+    g, a, b, alpha, lam = gpu_grid(prob, relax="rbgs", L0=L0)
+    gst = g.poisson(a, b, alpha=alpha, lambda_=lam, tolerance=1e-7)
+    assert_same(ost, gst, og.get_a(), a.get(), prob["b"])
+
+
 LARGE = [
     # larger 2D levels: several shared-memory tiles per level, tile edges,
     # lambda staged in shared memory, periodic halos wrapping across tiles
