@@ -990,7 +990,10 @@ static int solve (bmg_grid * g, field_t * a, field_t * b, coefs_t * c, int nrela
   if (minlevel < 0) minlevel = 0;
   if (mixed) { r = convert_coefs (g, c); if (r) return r; }
 
+  /* zeroed: the struct is part of the graph cache key (memcmp), so the
+     entries of levels above the depth must not be stack garbage */
   levels_t lv;
+  memset (&lv, 0, sizeof lv);
   for (int l = 0; l <= L; l++) {
     int st = (mixed && l != minlevel) ? BMG_ST_F32 : BMG_ST_F64;
     lv.st[l] = st;
@@ -1281,6 +1284,7 @@ void mg_cycle (bmg_scalar * al, bmg_scalar * resl, bmg_scalar * dal,
   minlevel = minlevel < maxlevel ? minlevel : maxlevel;   /* poisson.h:48 */
   if (minlevel < 0) minlevel = 0;
   levels_t lv;
+  memset (&lv, 0, sizeof lv);
   for (int l = 0; l <= g->depth; l++) {
     lv.st[l] = BMG_ST_F64;
     lv.da[l] = da->lv[l];
