@@ -61,6 +61,13 @@ class ClockSampler:
         self.device_index = device_index
         self.proc = None
         self.lines = []
+        self.t0 = self.t1 = None
+
+    def window(self, t0, t1):
+        """Keep only the samples read between t0 and t1 (time.monotonic()):
+        the sampler is started before the warm-up, so that nvidia-smi's own
+        start-up does not fall inside the timed region."""
+        self.t0, self.t1 = t0, t1
 
     def start(self):
         try:
@@ -75,7 +82,7 @@ class ClockSampler:
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.monotonic(), line.strip()))
 
     def stop(self):
         if not self.proc:
@@ -88,7 +95,11 @@ class ClockSampler:
         self.t.join(timeout=2)
         sm, smax, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in self.lines:
+        lines = [l for t, l in self.lines
+                 if self.t0 is None or self.t0 <= t <= self.t1 + 0.25]
+        if not lines:
+            lines = [l for _, l in self.lines[-1:]]
+        for line in lines:
             f = [x.strip() for x in line.split(",")]
             if len(f) < 9:
                 continue
@@ -161,7 +172,7 @@ def flush_l2(buf):
     buf.zero_()
 
 
-def time_steps(solver, steps, warmup, ws, flush):
+def time_steps(solver, steps, warmup, ws, flush, clocks=None):
     import torch
     for _ in range(warmup):
         solver.step()
@@ -169,6 +180,7 @@ def time_steps(solver, steps, warmup, ws, flush):
     barrier(ws)
     solver.g.reset_counters()
     times, stats = [], None
+    t_begin = time.monotonic()
     for _ in range(steps):
         flush_l2(flush)
         torch.cuda.synchronize()
@@ -178,6 +190,8 @@ def time_steps(solver, steps, warmup, ws, flush):
         e1.record()
         torch.cuda.synchronize()
         times.append(e0.elapsed_time(e1))
+    if clocks is not None:
+        clocks.window(t_begin, time.monotonic())
     barrier(ws)
     return times, stats, solver.g.counters()
 
@@ -376,6 +390,7 @@ def run_workload(args, ws, rank, local):
                   "relax": "red-black Gauss-Seidel",
                   "parallelism": "replicas" if ws > 1 else "1 gpu"}
     g.set_timing(True)
+    clocks.start()
     for _ in range(args.warmup):
         reset()
         solve()
@@ -383,7 +398,7 @@ def run_workload(args, ws, rank, local):
     barrier(ws)
     g.reset_counters()
     times, st = [], None
-    clocks.start()
+    t_begin = time.monotonic()
     for _ in range(args.steps):
         flush_l2(flush)
         reset()
@@ -394,6 +409,7 @@ def run_workload(args, ws, rank, local):
         e1.record()
         torch.cuda.synchronize()
         times.append(e0.elapsed_time(e1))
+    clocks.window(t_begin, time.monotonic())
     clk = clocks.stop()
     barrier(ws)
     c = g.counters()
@@ -514,7 +530,7 @@ def main():
     smx = Solver(prob, "mixed")
     clocks = ClockSampler(local)
     clocks.start()
-    tmx, stmx, cmx = time_steps(smx, args.steps, args.warmup, ws, flush)
+    tmx, stmx, cmx = time_steps(smx, args.steps, args.warmup, ws, flush, clocks)
     clk = clocks.stop()
     amx = smx.a.get()
 
