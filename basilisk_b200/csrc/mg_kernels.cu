@@ -99,6 +99,39 @@ __global__ void k_prolong (bmg_geom gc, bmg_geom gf, const TC * __restrict__ s,
   ghosts_homog<DIM, TF> (f, gf, i, j, k, w, bc);
 }
 
+/* the 2D bilinear prolongation by coarse cell: one thread reads the 3 x 3
+   coarse neighbourhood (ghosts included) once and writes the four children,
+   each with k_prolong's expression and order (bit-identical) */
+template <typename TC, typename TF>
+__global__ void k_prolong2d_blk (bmg_geom gc, bmg_geom gf, const TC * __restrict__ s,
+                                 TF * __restrict__ f, BCH bc)
+{
+  const int cj = blockIdx.x*blockDim.x + threadIdx.x, ci = blockIdx.y*blockDim.y + threadIdx.y;
+  if (ci >= gc.n || cj >= gc.n) return;
+  TC m[3][3];
+#pragma unroll
+  for (int di = 0; di < 3; di++)
+#pragma unroll
+    for (int dj = 0; dj < 3; dj++)
+      m[di][dj] = s[cidx<2> (gc, ci + di - 1, cj + dj - 1, 0)];
+#pragma unroll
+  for (int a = 0; a < 2; a++) {
+    TF w[2];
+#pragma unroll
+    for (int b = 0; b < 2; b++) {
+      const int cx = a ? 1 : -1, cy = b ? 1 : -1;
+      const TC v = (TC(9)*m[1][1] + TC(3)*(m[1 + cx][1] + m[1][1 + cy]) + m[1 + cx][1 + cy])/TC(16);
+      w[b] = (TF) v;
+    }
+    const int i = 2*ci + a, j = 2*cj;
+    TF * q = f + cidx<2> (gf, i, j, 0);
+    q[0] = w[0];
+    q[1] = w[1];
+    ghosts_homog<2, TF> (f, gf, i, j, 0, w[0], bc);
+    ghosts_homog<2, TF> (f, gf, i, j + 1, 0, w[1], bc);
+  }
+}
+
 /* coarse = mean of the children, summed in foreach_child order */
 template <int DIM, typename TF, typename TC>
 __global__ void k_restrict (bmg_geom gf, bmg_geom gc, const TF * __restrict__ f,
@@ -465,6 +498,18 @@ template <int DIM>
 void prolong_dim (int stc, int stf, bmg_geom gc, bmg_geom gf, const void * c, void * f,
                   BCH h, int zero, cudaStream_t s)
 {
+  if (DIM == 2 && !zero && gf.n == 2*gc.n) {
+    dim3 gb = grid_shape<2> (gc.n), bb = block_shape<2> ();
+    if (stc == BMG_ST_F64 && stf == BMG_ST_F64)
+      k_prolong2d_blk<double, double><<<gb, bb, 0, s>>> (gc, gf, (const double *) c, (double *) f, h);
+    else if (stc == BMG_ST_F32 && stf == BMG_ST_F32)
+      k_prolong2d_blk<float, float><<<gb, bb, 0, s>>> (gc, gf, (const float *) c, (float *) f, h);
+    else if (stc == BMG_ST_F64 && stf == BMG_ST_F32)
+      k_prolong2d_blk<double, float><<<gb, bb, 0, s>>> (gc, gf, (const double *) c, (float *) f, h);
+    else
+      k_prolong2d_blk<float, double><<<gb, bb, 0, s>>> (gc, gf, (const float *) c, (double *) f, h);
+    return;
+  }
   dim3 gb = grid_shape<DIM> (gf.n), bb = block_shape<DIM> ();
   if (stc == BMG_ST_F64 && stf == BMG_ST_F64)
     k_prolong<DIM, double, double><<<gb, bb, 0, s>>> (gc, gf, (const double *) c, (double *) f, h, zero);
