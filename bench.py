@@ -51,6 +51,11 @@ def load_peaks():
         return 6650.0, "fallback"
 
 
+# dram__bytes_read.sum + dram__bytes_write.sum of one k_relax_tile2d_w launch on
+# the 2048^2 level (ncu, 68.3 + 5.8 MB)
+TILE_LAUNCH_DRAM_BYTES = 74.1e6
+
+
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled during the timed region."""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
@@ -574,10 +579,16 @@ def main():
                     "fp64": {k: st64[k] for k in ("i", "resb", "resa", "nrelax")}},
         "mixed_vs_fp64_rel_error": err,
         "vcycle": {"mixed": fmx, "fp64": f64},
-        "roofline": {"bound": "hbm", "kernel": "k_relax (finest level, red+black sweep)",
+        "roofline": {"bound": "hbm",
+                     "kernel": "k_relax_tile2d_w (finest level, 4 red-black sweeps per launch)",
                      "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak if achieved else None,
-                     "traffic": None, "peak_kind": peak_kind},
+                     # DRAM bytes (read + write) of one finest-level launch of four
+                     # sweeps, from the ncu capture summarised in
+                     # profiles/k_relax_tile2d_w_fp32_2048_ncu.md; the algorithmic
+                     # bytes of that launch are 335.5e6
+                     "traffic": TILE_LAUNCH_DRAM_BYTES, "traffic_per": "launch (4 sweeps)",
+                     "peak_kind": peak_kind},
         "clocks": clk,
         "gpu_launches": int(cmx["launches"]),
         "e2e": {"value": ws * 1e3 / ms_e2e, "unit": "solves/s", "h2d_bytes_per_step": h2d,
