@@ -57,6 +57,8 @@ struct bmg_grid {
   struct bmg_tree * tree;          /* quadtree over the levels, or NULL */
   int div_h;                       /* handle of project ()'s div field, 0 = none yet */
   double * visc_ws;                /* viscosity (): da, res, w, r of each component */
+  double * stage;                  /* host <-> device staging of field values */
+  size_t stage_n;                  /* its size in doubles */
   unsigned long long clock;
 };
 

@@ -201,6 +201,7 @@ void bmg_grid_free (bmg_grid * g)
     }
   free (g->fields);
   cudaFree (g->ws64); cudaFree (g->ws32); cudaFree (g->bproj); cudaFree (g->visc_ws);
+  cudaFree (g->stage);
   cudaFree (g->d_maxres); cudaFree (g->d_partials); cudaFree (g->d_sum);
   cudaFreeHost (g->h_pinned);
   cudaEventDestroy (g->ev0); cudaEventDestroy (g->ev1);
@@ -411,15 +412,33 @@ static size_t field_count (const bmg_grid * g, int l, int face_dim)
   return c;
 }
 
+/* the grid's staging buffer for host values, grown on demand and kept
+   (set and get are synchronous, so one buffer serves every call) */
+static double * stage_buf (bmg_grid * g, size_t count)
+{
+  if (g->stage_n < count) {
+    cudaStreamSynchronize (g->stream);
+    cudaFree (g->stage);
+    g->stage = NULL;
+    g->stage_n = 0;
+    if (cudaMalloc ((void **) &g->stage, count*sizeof (double)) != cudaSuccess) {
+      g->stage = NULL;
+      return NULL;
+    }
+    g->stage_n = count;
+  }
+  return g->stage;
+}
+
 /* staging: compact values on the device (copied from the host if needed) */
 static int stage_in (bmg_grid * g, const double * values, size_t count, int memory,
-                     const double ** dptr, double ** tmp)
+                     const double ** dptr)
 {
-  *tmp = NULL;
   if (memory == BMG_DEVICE) { *dptr = values; return BMG_OK; }
-  CK (cudaMallocAsync ((void **) tmp, count*sizeof (double), g->stream));
-  CK (cudaMemcpyAsync (*tmp, values, count*sizeof (double), cudaMemcpyHostToDevice, g->stream));
-  *dptr = *tmp;
+  double * tmp = stage_buf (g, count);
+  if (!tmp) return fail (BMG_ENOMEM);
+  CK (cudaMemcpyAsync (tmp, values, count*sizeof (double), cudaMemcpyHostToDevice, g->stream));
+  *dptr = tmp;
   return BMG_OK;
 }
 
@@ -433,8 +452,8 @@ int bmg_field_set_level (bmg_grid * g, bmg_scalar s, int level, const double * v
       count != field_count (g, level, f->face_dim))
     return fail (BMG_EINVAL);
   CK (cudaSetDevice (g->device));
-  const double * d; double * tmp;
-  int st = stage_in (g, values, count, memory, &d, &tmp);
+  const double * d;
+  int st = stage_in (g, values, count, memory, &d);
   if (st) return st;
   CL (bmg_launch_pack (g->dim, BMG_ST_F64, g->g64[level], f->face_dim, d, f->lv[level], g->stream));
   if (f->face_dim >= 0 && (g->periodic[f->face_dim] || level0_periodic (g, level)))
@@ -443,7 +462,6 @@ int bmg_field_set_level (bmg_grid * g, bmg_scalar s, int level, const double * v
        on a periodic level 0 every neighbour slot takes the cell's value,
        the upper face of every component included (multigrid.h:655-664) */
     CL (bmg_launch_face_wrap (g->dim, g->g64[level], f->face_dim, f->lv[level], g->stream));
-  if (tmp) CK (cudaFreeAsync (tmp, g->stream));
   if (f->face_dim < 0 && level == g->depth) {
     int r = refresh_bc_ghosts (g, s.i);
     if (r) return r;
@@ -468,14 +486,12 @@ int bmg_field_get_level (bmg_grid * g, bmg_scalar s, int level, double * values,
   CK (cudaSetDevice (g->device));
   double * d = values, * tmp = NULL;
   if (memory != BMG_DEVICE) {
-    CK (cudaMallocAsync ((void **) &tmp, count*sizeof (double), g->stream));
+    if (!(tmp = stage_buf (g, count))) return fail (BMG_ENOMEM);
     d = tmp;
   }
   CL (bmg_launch_unpack (g->dim, g->g64[level], f->face_dim, f->lv[level], d, g->stream));
-  if (tmp) {
+  if (tmp)
     CK (cudaMemcpyAsync (values, tmp, count*sizeof (double), cudaMemcpyDeviceToHost, g->stream));
-    CK (cudaFreeAsync (tmp, g->stream));
-  }
   CK (cudaStreamSynchronize (g->stream));
   return BMG_OK;
 }
@@ -1323,27 +1339,27 @@ int bmg_adjoint_gradients (bmg_grid * g, bmg_scalar mu, bmg_scalar a, double * c
     const size_t count = field_count (g, L, d);
     double * dst = grad_alpha[d], * tmp = NULL;
     if (memory == BMG_HOST) {
-      CK (cudaMallocAsync ((void **) &tmp, count*sizeof (double), g->stream));
+      /* the staging buffer: reused in stream order by the next copy */
+      if (!(tmp = stage_buf (g, count))) return fail (BMG_ENOMEM);
       dst = tmp;
     }
     CL (bmg_launch_adjoint_faces (g->dim, g->g64[L], d, g->periodic[d], fm->lv[L], fa->lv[L],
                                   delta_of (g, L), dst, g->stream));
     if (tmp) {
       CK (cudaMemcpyAsync (grad_alpha[d], tmp, count*sizeof (double), cudaMemcpyDeviceToHost, g->stream));
-      CK (cudaFreeAsync (tmp, g->stream));
     }
   }
   if (grad_lambda) {
     const size_t count = field_count (g, L, -1);
     double * dst = grad_lambda, * tmp = NULL;
     if (memory == BMG_HOST) {
-      CK (cudaMallocAsync ((void **) &tmp, count*sizeof (double), g->stream));
+      /* the staging buffer: reused in stream order by the next copy */
+      if (!(tmp = stage_buf (g, count))) return fail (BMG_ENOMEM);
       dst = tmp;
     }
     CL (bmg_launch_adjoint_cells (g->dim, g->g64[L], fm->lv[L], fa->lv[L], dst, g->stream));
     if (tmp) {
       CK (cudaMemcpyAsync (grad_lambda, tmp, count*sizeof (double), cudaMemcpyDeviceToHost, g->stream));
-      CK (cudaFreeAsync (tmp, g->stream));
     }
   }
   CK (cudaStreamSynchronize (g->stream));
