@@ -1260,8 +1260,14 @@ __device__ __forceinline__ void bot_level2d (const bmg_geom g, void * dav, const
   const T * b = (const T *) resv, * ax = (const T *) axv, * ay = (const T *) ayv,
     * lam = (const T *) lamv;
   const T D2 = (T) Delta*(T) Delta;
-  /* four cells per colour per thread in FP32, two in FP64 (registers) */
+  /* up to four cells per colour per thread in FP32, two in FP64
+     (registers); one where the level's cells of a colour fit the threads,
+     so that the small levels' passes carry no empty slots */
   constexpr int K = sizeof (T) == 4 ? 4 : 2;
+  if (fast && g.n >= 2 && g.n*(g.n >> 1) <= nt) {
+    bot_sweeps2d_reg<T, 1> (g, a, b, ax, ay, (T) axc, (T) ayc, lam, (T) lamc, D2, bc, nrelax, nt, small);
+    return;
+  }
   if (fast && g.n >= 2 && g.n*(g.n >> 1) <= K*nt) {
     bot_sweeps2d_reg<T, K> (g, a, b, ax, ay, (T) axc, (T) ayc, lam, (T) lamc, D2, bc, nrelax, nt, small);
     return;
