@@ -587,8 +587,14 @@ k_relax_tile2d (bmg_geom g, T * __restrict__ out, const T * __restrict__ in,
    operations: the shared-memory pipe, which bounds k_relax_tile2d, carries
    less than half the traffic. */
 namespace tw {
-constexpr int TS = 48, S = 4, H = 2*S, W = TS + 2*H, M = W/2, WM = W*M, BX = 8, BY = 64;
+constexpr int W = 64, M = W/2, WM = W*M, BX = 8, BY = 64;
 static_assert (W == 8*BX && W - 2 <= BY && BY % 8 == 0, "one row of eight cells per thread");
+/* a tile of TS x TS cells in the W x W staged region: a halo of
+   H = (W - TS)/2 cells, S = H/2 sweeps per launch (48: 4 sweeps, 32: 8) */
+template <int TS> struct Tile {
+  static constexpr int H = (W - TS)/2, S = H/2;
+  static_assert (TS % 4 == 0 && H % 2 == 0 && H > 0, "tile of quads, even halo");
+};
 }
 
 /* shared-memory accesses by 32-bit byte address plus a constant offset
@@ -621,13 +627,14 @@ __device__ __forceinline__ void sts_f1 (unsigned a, float v)
   asm volatile ("st.shared.f32 [%0], %1;" :: "r"(a), "f"(v) : "memory");
 }
 
-template <bool LAM>
+template <int TS, bool LAM>
 __global__ void __launch_bounds__ (tw::BX*tw::BY, 2)
 k_relax_tile2d_w (bmg_geom g, float * __restrict__ out, const float * __restrict__ in,
                   const float * __restrict__ res, Coef<float> ax, Coef<float> ay, Coef<float> lam,
                   float Delta, BCH bc, int nsweeps)
 {
   using namespace tw;
+  constexpr int H = Tile<TS>::H;
   __shared__ __align__ (16) float sa[2*WM];     /* colour c of staged cell (p, q) at c*WM + p*M + q/2 */
   const int n = g.n, tx = threadIdx.x, ty = threadIdx.y, tid = ty*BX + tx, nth = BX*BY;
   constexpr int RW = 32/BX;                     /* rows per warp, all of one parity */
@@ -837,7 +844,7 @@ k_relax_tile2d_w (bmg_geom g, float * __restrict__ out, const float * __restrict
   }
 }
 
-template <bool LAM>
+template <int TS, bool LAM>
 int launch_tile_w (bmg_geom g, void * out, const void * in, const void * res,
                    const bmg_coef * alpha, bmg_coef lambda, double Delta, BCH h, int nsweeps,
                    cudaStream_t s)
@@ -854,7 +861,7 @@ int launch_tile_w (bmg_geom g, void * out, const void * in, const void * res,
   at[0].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = at;
   cfg.numAttrs = 1;
-  return (int) cudaLaunchKernelEx (&cfg, k_relax_tile2d_w<LAM>, g, (float *) out, (const float *) in,
+  return (int) cudaLaunchKernelEx (&cfg, k_relax_tile2d_w<TS, LAM>, g, (float *) out, (const float *) in,
                                    (const float *) res, coef_of<float> (alpha[0]),
                                    coef_of<float> (alpha[1]), coef_of<float> (lambda),
                                    (float) Delta, h, nsweeps);
@@ -1432,10 +1439,14 @@ int launch_tile (bmg_geom g, void * out, const void * in, const void * res,
 
 extern "C" {
 
+/* the FP32 level whose register-weight tiles are 32 x 32 (eight sweeps per
+   launch): a latency-bound level, where halving the launches and doubling
+   the CTAs outweighs the deeper halo */
+#define BMG_DEEP_TILE_N 512
+
 int bmg_tile_sweeps (int st, int n)
 {
-  (void) st; (void) n;
-  return 4;
+  return st == BMG_ST_F32 && n == BMG_DEEP_TILE_N ? 8 : 4;
 }
 
 int bmg_launch_relax_tile (int dim, int st, bmg_geom g, void * out, const void * in,
@@ -1455,8 +1466,11 @@ int bmg_launch_relax_tile (int dim, int st, bmg_geom g, void * out, const void *
       : launch_tile<double, 40, 4, 16, 64> (g, out, in, res, alpha, lambda, Delta, h, nsweeps, s);
   else
     e = small ? launch_tile<float, 16, 4, 8, 32> (g, out, in, res, alpha, lambda, Delta, h, nsweeps, s)
-      : lambda.p ? launch_tile_w<true> (g, out, in, res, alpha, lambda, Delta, h, nsweeps, s)
-      : launch_tile_w<false> (g, out, in, res, alpha, lambda, Delta, h, nsweeps, s);
+      : g.n == BMG_DEEP_TILE_N ?
+        (lambda.p ? launch_tile_w<32, true> (g, out, in, res, alpha, lambda, Delta, h, nsweeps, s)
+                  : launch_tile_w<32, false> (g, out, in, res, alpha, lambda, Delta, h, nsweeps, s))
+      : lambda.p ? launch_tile_w<48, true> (g, out, in, res, alpha, lambda, Delta, h, nsweeps, s)
+      : launch_tile_w<48, false> (g, out, in, res, alpha, lambda, Delta, h, nsweeps, s);
   if (e) return e;
   cudaError_t r = cudaGetLastError ();
   return r == cudaSuccess ? 0 : (int) r;
