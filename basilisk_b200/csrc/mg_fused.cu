@@ -4,28 +4,37 @@
  * The reference's V-cycle (poisson.h:32-90) relaxes every level nrelax times,
  * and mg_solve raises nrelax while a cycle reduces the residual by less than
  * 1.2 (poisson.h:198-204): on stiff problems nrelax reaches 30-50, so the
- * solve is a long chain of small relaxation sweeps.  Two kernels replace the
- * one-launch-per-colour sweeps of mg_kernels.cu on the red-black path:
+ * solve is a long chain of small relaxation sweeps.  These kernels replace
+ * the one-launch-per-colour sweeps of mg_kernels.cu on the red-black path:
  *
- *   k_relax_tile2d  S complete red-black sweeps of a 2D level in one launch.
- *                   Each CTA stages a TS x TS tile plus a 2S-cell halo of
- *                   da, res, alpha_x, alpha_y (and lambda) in shared memory,
- *                   updates red then black cells on a region that shrinks by
- *                   one cell per colour pass, and writes the TS x TS interior
- *                   back to the partner buffer (CTAs read halos that other
- *                   CTAs own, so a launch never writes what it reads).  The
- *                   halo is recomputed redundantly, so each array is read
- *                   about once per S sweeps instead of twice per sweep.
- *   k_bottom        the coarse end of the cycle in one single-CTA launch:
- *                   restriction of res down to minlevel, the coarsest zero,
- *                   then for each level up to a small one the bilinear
- *                   prolongation and all nrelax sweeps, with __syncthreads
- *                   between colour passes.  Those levels are pure latency
- *                   when each pass is a launch.
+ *   k_relax_tile2d    S complete red-black sweeps of a 2D level in one
+ *                     launch.  Each CTA stages a TS x TS tile plus a
+ *                     2S-cell halo of da, res, alpha_x, alpha_y (and lambda)
+ *                     in shared memory, updates red then black cells on a
+ *                     region that shrinks by one cell per colour pass, and
+ *                     writes the TS x TS interior back to the partner buffer
+ *                     (CTAs read halos that other CTAs own, so a launch never
+ *                     writes what it reads).  The halo is recomputed
+ *                     redundantly, so each array is read about once per S
+ *                     sweeps instead of twice per sweep.  FP64 levels (in the
+ *                     reference's evaluation order) and the small FP32
+ *                     levels.
+ *   k_relax_tile2d_w  the same temporal blocking for the large FP32 levels of
+ *                     the mixed form, with each thread's cells' coefficients
+ *                     divided by the diagonal once per launch and kept in
+ *                     registers: only the iterate is staged.
+ *   k_bottom          the coarse end of the cycle in one single-CTA launch:
+ *                     restriction of res down to minlevel, the coarsest zero,
+ *                     then for each level up to a small one the bilinear
+ *                     prolongation and all nrelax sweeps, with barriers
+ *                     between colour passes.  Those levels are pure latency
+ *                     when each pass is a launch.
  *
- * Both compute every cell update with relax_value's expression and order and
- * write the same ghost images as the unfused kernels, so their results are
- * bit-identical to the red / boundary / black sequence of the oracle.
+ * The FP64 paths compute every cell update with relax_value's expression and
+ * order and write the same ghost images as the unfused kernels, so their
+ * results are bit-identical to the red / boundary / black sequence of the
+ * oracle; the FP32 paths of the mixed form relax the same operator up to
+ * FP32 rounding.
  */
 #include <cuda_runtime.h>
 #include <stdio.h>
@@ -179,77 +188,9 @@ __device__ __forceinline__ void put_quad (T * a0, T * a1, int off, const Quad<T>
   *(T2 *) (a1 + off) = o;
 }
 
-/* BX x BY threads: thread (tx, ty) updates the CPT cells CPT tx ..
-   CPT tx + CPT - 1 of each colour of row ty + lo in every colour pass
-   (CPT = 2 or 4); MINB CTAs per SM bound the registers */
-template <typename T> struct Vec4;
-template <> struct Vec4<float> { typedef float4 type; };
-
-/* One colour pass of an FP32 tile that lies inside the domain, four cells
-   of colour C per thread.  Everything that does not change between passes
-   is hoisted by the caller: the column offset o of the thread's colour
-   cells (the same in every pass, since the row advances by one per pass
-   while the colour alternates) and the thread's quad m0.  With C a
-   template parameter every array offset is a constant, so each operand is
-   one 16-byte shared load from one base address. */
-template <int C, bool LAM, int W, int M, int MY>
-__device__ __forceinline__ void tile_pass4 (float * __restrict__ smb, int k, int pr, int m0, int o,
-                                            float D2, float lamc)
-{
-  constexpr int WM = W*M, WX = (W + 1)*M, WY = W*MY;
-  constexpr int OR = 2*WM, OX = 4*WM, OY = OX + 2*WX, OL = OY + 2*WY;
-  constexpr int CO = C ^ 1;
-  const int p = k + 1 + pr;
-  if (p >= W - k - 1) return;
-  const int ci = p*M + m0, cy = p*MY + m0;
-  const float * __restrict__ A = smb + CO*WM + ci;             /* the other colour */
-  const float4 up = *(const float4 *) (A - M), dn = *(const float4 *) (A + M);
-  const float4 mid = *(const float4 *) A;
-  const float4 rr = *(const float4 *) (smb + OR + C*WM + ci);
-  const float4 xl = *(const float4 *) (smb + OX + C*WX + ci);
-  const float4 xu = *(const float4 *) (smb + OX + CO*WX + ci + M);
-  const float4 yl = *(const float4 *) (smb + OY + C*WY + cy);
-  const float4 y4 = *(const float4 *) (smb + OY + CO*WY + cy);
-  float4 lv;
-  if (LAM) lv = *(const float4 *) (smb + OL + C*WM + ci);
-  else lv = make_float4 (lamc, lamc, lamc, lamc);
-  /* left / right neighbours and right faces of the four cells */
-  float v[5], yr[4];
-  if (o == 0) {
-    v[0] = A[-1]; v[1] = mid.x; v[2] = mid.y; v[3] = mid.z; v[4] = mid.w;
-    yr[0] = y4.x; yr[1] = y4.y; yr[2] = y4.z; yr[3] = y4.w;
-  }
-  else {
-    v[0] = mid.x; v[1] = mid.y; v[2] = mid.z; v[3] = mid.w; v[4] = A[4];
-    yr[0] = y4.y; yr[1] = y4.z; yr[2] = y4.w; yr[3] = smb[OY + CO*WY + cy + 4];
-  }
-  const float rv[4] = {rr.x, rr.y, rr.z, rr.w}, lvv[4] = {lv.x, lv.y, lv.z, lv.w};
-  const float xlv[4] = {xl.x, xl.y, xl.z, xl.w}, xuv[4] = {xu.x, xu.y, xu.z, xu.w};
-  const float ylv[4] = {yl.x, yl.y, yl.z, yl.w};
-  const float upv[4] = {up.x, up.y, up.z, up.w}, dnv[4] = {dn.x, dn.y, dn.z, dn.w};
-  float out[4];
-#pragma unroll
-  for (int e = 0; e < 4; e++) {
-    /* relax_value (poisson.h:303-319) in FP32 with fused multiply-adds */
-    float nn = (-D2)*rv[e], d = (-lvv[e])*D2;
-    nn = fmaf (xlv[e], upv[e], fmaf (xuv[e], dnv[e], nn));
-    nn = fmaf (ylv[e], v[e], fmaf (yr[e], v[e + 1], nn));
-    d += xuv[e] + xlv[e];
-    d += yr[e] + ylv[e];
-    out[e] = __fdividef (nn, d);
-  }
-  /* the valid columns of colour C shrink by one cell per pass */
-  const int mlo = (k + 2 - o) >> 1, mhi = (W - k - o) >> 1;
-  float * __restrict__ a = smb + C*WM + ci;
-  if (m0 >= mlo && m0 + 4 <= mhi)
-    *(float4 *) a = make_float4 (out[0], out[1], out[2], out[3]);
-  else {
-#pragma unroll
-    for (int e = 0; e < 4; e++)
-      if (m0 + e >= mlo && m0 + e < mhi) a[e] = out[e];
-  }
-}
-
+/* BX x BY threads: thread (tx, ty) updates the CPT = 2 cells 2 tx, 2 tx + 1
+   of each colour of row ty + lo in every colour pass; MINB CTAs per SM bound
+   the registers */
 template <typename T, int TS, int S, bool LAM, int BX, int BY, int CPT, int MINB>
 __global__ void __launch_bounds__ (BX*BY, MINB)
 k_relax_tile2d (bmg_geom g, T * __restrict__ out, const T * __restrict__ in,
@@ -259,7 +200,7 @@ k_relax_tile2d (bmg_geom g, T * __restrict__ out, const T * __restrict__ in,
   typedef TileShape<T, TS, S> Sh;
   constexpr int H = Sh::H, W = Sh::W, M = Sh::M, MY = Sh::MY;
   static_assert (M % CPT == 0 && M <= CPT*BX && W - 2 <= BY, "CPT cells per thread per row");
-  static_assert (CPT == 2 || (CPT == 4 && sizeof (T) == 4), "pairs, or quads of FP32 cells");
+  static_assert (CPT == 2, "pairs of cells per thread and colour");
   typedef typename Pair<T>::type T2;
   extern __shared__ __align__ (16) unsigned char smem_raw[];
   /* the colour-c arrays, as offsets from one shared base (no pointer
@@ -401,20 +342,7 @@ k_relax_tile2d (bmg_geom g, T * __restrict__ out, const T * __restrict__ in,
   __syncthreads ();
 
   const T D2 = Delta*Delta;
-  if constexpr (CPT == 4) {
-    if (inner) {
-      /* column offset of the thread's cells: (c - base - p) & 1 with
-         p = k + 1 + pr and c = k & 1, the same in every pass */
-      const int o = (base + 1 + pr) & 1, m0 = 4*tx;
-      for (int sw = 0; sw < nsweeps; sw++) {
-        tile_pass4<0, LAM, W, M, MY> (smb, 2*sw, pr, m0, o, D2, lam.c);
-        __syncthreads ();
-        tile_pass4<1, LAM, W, M, MY> (smb, 2*sw + 1, pr, m0, o, D2, lam.c);
-        __syncthreads ();
-      }
-    }
-  }
-  for (int sw = 0; sw < ((CPT == 4 && inner) ? 0 : nsweeps); sw++)
+  for (int sw = 0; sw < nsweeps; sw++)
 #pragma unroll
     for (int c = 0; c < 2; c++) {
       const int k = 2*sw + c;
@@ -429,66 +357,7 @@ k_relax_tile2d (bmg_geom g, T * __restrict__ out, const T * __restrict__ in,
          lo + pr; a warp covers RW rows of one parity (pr interleaves them),
          so the colour offset o, and every branch on it, is uniform per warp */
       const int p = lo + pr;
-      if constexpr (CPT == 4) {
-        typedef typename Vec4<T>::type T4;
-        if (p < hi) {
-          const int o = (c - base - p) & 1;
-          const int mlo = (lo - o + 1) >> 1, mhi = (hi - o + 1) >> 1;
-          const int m0 = 4*tx;
-          bool ok[4];
-#pragma unroll
-          for (int e = 0; e < 4; e++) ok[e] = m0 + e >= mlo && m0 + e < mhi;
-          if (!inner) {
-            const int gi = i0 + p, gj = j0 + 2*m0 + o;
-            const bool rowok = px || (unsigned) gi < (unsigned) n;
-#pragma unroll
-            for (int e = 0; e < 4; e++)
-              ok[e] = ok[e] && rowok && (py || (unsigned) (gj + 2*e) < (unsigned) n);
-          }
-          if (ok[0] || ok[1] || ok[2] || ok[3]) {
-            const int ci = p*M + m0;
-            const T4 up = *(const T4 *) &o_a[ci - M], dn = *(const T4 *) &o_a[ci + M];
-            const T4 mid = *(const T4 *) &o_a[ci];
-            /* the other colour's cells [m0 - 1 + o .. m0 + 3 + o]: cell e has
-               v[e] on its left and v[e + 1] on its right */
-            T v[5];
-            if (o == 0) { v[0] = o_a[ci - 1]; v[1] = mid.x; v[2] = mid.y; v[3] = mid.z; v[4] = mid.w; }
-            else { v[0] = mid.x; v[1] = mid.y; v[2] = mid.z; v[3] = mid.w; v[4] = o_a[ci + 4]; }
-            const T4 rr = *(const T4 *) &r[ci];
-            const T4 xl = *(const T4 *) &xr[ci], xu = *(const T4 *) &xo[ci + M];
-            const T4 yl = *(const T4 *) &yr[p*MY + m0], y4 = *(const T4 *) &yo[p*MY + m0];
-            T yrv[4];
-            if (o == 0) { yrv[0] = y4.x; yrv[1] = y4.y; yrv[2] = y4.z; yrv[3] = y4.w; }
-            else { yrv[0] = y4.y; yrv[1] = y4.z; yrv[2] = y4.w; yrv[3] = yo[p*MY + m0 + 4]; }
-            T4 lv;
-            if (LAM) lv = *(const T4 *) &l[ci];
-            else { lv.x = lam.c; lv.y = lam.c; lv.z = lam.c; lv.w = lam.c; }
-            const T rrv[4] = {rr.x, rr.y, rr.z, rr.w}, lvv[4] = {lv.x, lv.y, lv.z, lv.w};
-            const T xlv[4] = {xl.x, xl.y, xl.z, xl.w}, xuv[4] = {xu.x, xu.y, xu.z, xu.w};
-            const T ylv[4] = {yl.x, yl.y, yl.z, yl.w};
-            const T upv[4] = {up.x, up.y, up.z, up.w}, dnv[4] = {dn.x, dn.y, dn.z, dn.w};
-            T out[4];
-#pragma unroll
-            for (int e = 0; e < 4; e++) {
-              /* relax_value's expression (poisson.h:303-319) */
-              T nn = (-D2)*rrv[e], d = (-lvv[e])*D2;
-              nn = tile_acc (nn, xuv[e], dnv[e], xlv[e], upv[e]); d += xuv[e] + xlv[e];
-              nn = tile_acc (nn, yrv[e], v[e + 1], ylv[e], v[e]); d += yrv[e] + ylv[e];
-              out[e] = relax_div (nn, d);
-            }
-            if (ok[0] && ok[1] && ok[2] && ok[3]) {
-              T4 w; w.x = out[0]; w.y = out[1]; w.z = out[2]; w.w = out[3];
-              *(T4 *) &a[ci] = w;
-            }
-            else {
-#pragma unroll
-              for (int e = 0; e < 4; e++)
-                if (ok[e]) a[ci + e] = out[e];
-            }
-          }
-        }
-      }
-      else if (p < hi) {
+      if (p < hi) {
         const int o = (c - base - p) & 1;        /* column offset of colour c */
         const int mlo = (lo - o + 1) >> 1, mhi = (hi - o + 1) >> 1;
         const int m0 = 2*tx;
