@@ -1331,7 +1331,7 @@ __device__ __forceinline__ void bot_sweeps2d (const bmg_geom g, T * a, const T *
 __device__ __forceinline__ float fma_t (float a, float b, float c) { return fmaf (a, b, c); }
 __device__ __forceinline__ double fma_t (double a, double b, double c) { return fma (a, b, c); }
 
-template <typename T, int K>
+template <typename T, int K, bool EXACT>
 __device__ __forceinline__ void bot_sweeps2d_reg (const bmg_geom g, T * a, const T * b,
                                                   const T * ax, const T * ay, T axc,
                                                   T ayc, const T * lam, T lamc,
@@ -1371,14 +1371,22 @@ __device__ __forceinline__ void bot_sweeps2d_reg (const bmg_geom g, T * a, const
         const int e = (i + 1)*P + 1 + j;
         const T x0 = ax ? ax[e] : axc, x1 = ax ? ax[e + P] : axc;
         const T y0 = ay ? ay[e] : ayc, y1 = ay ? ay[e + 1] : ayc;
-        T d = (-(lam ? lam[e] : lamc))*D2;
-        d += x1 + x0;
-        d += y1 + y0;
-        const T inv = T(1)/d;
-        wx0[c][k] = x0*inv; wx1[c][k] = x1*inv; wy0[c][k] = y0*inv; wy1[c][k] = y1*inv;
-        beta[c][k] = ((-D2)*b[e])*inv;
+        if (EXACT) {
+          /* the plain form: the coefficients as they are, and -Delta^2 b */
+          wx0[c][k] = x0; wx1[c][k] = x1; wy0[c][k] = y0; wy1[c][k] = y1;
+          beta[c][k] = (-D2)*b[e];
+        }
+        else {
+          T d = (-(lam ? lam[e] : lamc))*D2;
+          d += x1 + x0;
+          d += y1 + y0;
+          const T inv = T(1)/d;
+          wx0[c][k] = x0*inv; wx1[c][k] = x1*inv; wy0[c][k] = y0*inv; wy1[c][k] = y1*inv;
+          beta[c][k] = ((-D2)*b[e])*inv;
+        }
       }
     }
+  const T dl = (-lamc)*D2;                    /* lambda constant in the exact form */
   for (int sw = 0; sw < nrelax; sw++)
 #pragma unroll
     for (int c = 0; c < 2; c++) {
@@ -1388,8 +1396,18 @@ __device__ __forceinline__ void bot_sweeps2d_reg (const bmg_geom g, T * a, const
       for (int k = 0; k < K; k++) {
         const int t = ij[c][k] < 0 ? 0 : ij[c][k];
         e[k] = ((t >> 16) + 1)*P + 1 + (t & 0xffff);
-        v[k] = fma_t (wy0[c][k], a[e[k] - 1], fma_t (wy1[c][k], a[e[k] + 1],
-               fma_t (wx0[c][k], a[e[k] - P], fma_t (wx1[c][k], a[e[k] + P], beta[c][k]))));
+        if (EXACT) {
+          /* relax_value's expression and order (poisson.h:303-319) */
+          T d = dl;
+          d += wx1[c][k] + wx0[c][k];
+          d += wy1[c][k] + wy0[c][k];
+          T m = beta[c][k] + (wx1[c][k]*a[e[k] + P] + wx0[c][k]*a[e[k] - P]);
+          m = m + (wy1[c][k]*a[e[k] + 1] + wy0[c][k]*a[e[k] - 1]);
+          v[k] = m/d;
+        }
+        else
+          v[k] = fma_t (wy0[c][k], a[e[k] - 1], fma_t (wy1[c][k], a[e[k] + 1],
+                 fma_t (wx0[c][k], a[e[k] - P], fma_t (wx1[c][k], a[e[k] + P], beta[c][k]))));
       }
 #pragma unroll
       for (int k = 0; k < K; k++)
@@ -1425,11 +1443,18 @@ __device__ __forceinline__ void bot_level2d (const bmg_geom g, void * dav, const
      so that the small levels' passes carry no empty slots */
   constexpr int K = sizeof (T) == 4 ? 4 : 2;
   if (fast && g.n >= 2 && g.n*(g.n >> 1) <= nt) {
-    bot_sweeps2d_reg<T, 1> (g, a, b, ax, ay, (T) axc, (T) ayc, lam, (T) lamc, D2, bc, nrelax, nt, small);
+    bot_sweeps2d_reg<T, 1, false> (g, a, b, ax, ay, (T) axc, (T) ayc, lam, (T) lamc, D2, bc, nrelax, nt, small);
     return;
   }
   if (fast && g.n >= 2 && g.n*(g.n >> 1) <= K*nt) {
-    bot_sweeps2d_reg<T, K> (g, a, b, ax, ay, (T) axc, (T) ayc, lam, (T) lamc, D2, bc, nrelax, nt, small);
+    bot_sweeps2d_reg<T, K, false> (g, a, b, ax, ay, (T) axc, (T) ayc, lam, (T) lamc, D2, bc, nrelax, nt, small);
+    return;
+  }
+  /* the plain FP64 form with lambda constant, on the levels whose cells of
+     a colour fit the threads: the same register ownership with the exact
+     coefficients, in the reference's evaluation order */
+  if (!fast && sizeof (T) == 8 && !lam && g.n >= 2 && g.n*(g.n >> 1) <= nt) {
+    bot_sweeps2d_reg<T, 1, true> (g, a, b, ax, ay, (T) axc, (T) ayc, lam, (T) lamc, D2, bc, nrelax, nt, small);
     return;
   }
   if (ax && lam)
