@@ -215,14 +215,25 @@ typedef struct {
   int * ii, * jj, * kk;
 } cells_t;
 
+/* grows *p to n elements of size sz; on failure *p is left as it was (and
+   freed by the caller) */
+static int grow (void ** p, size_t n, size_t sz)
+{
+  void * q = realloc (*p, n*sz);
+  if (!q) return BMG_ENOMEM;
+  *p = q;
+  return BMG_OK;
+}
+
 static int push_cell (cells_t * c, int l, int i, int j, int k, int leaf)
 {
   if (c->ncell == c->cap) {
-    c->cap = 2*c->cap + 1024;
-    c->level = realloc (c->level, c->cap); c->leaf = realloc (c->leaf, c->cap);
-    c->ii = realloc (c->ii, c->cap*sizeof (int)); c->jj = realloc (c->jj, c->cap*sizeof (int));
-    c->kk = realloc (c->kk, c->cap*sizeof (int));
-    if (!c->level || !c->leaf || !c->ii || !c->jj || !c->kk) return BMG_ENOMEM;
+    const long cap = 2*c->cap + 1024;
+    if (grow ((void **) &c->level, cap, 1) || grow ((void **) &c->leaf, cap, 1) ||
+        grow ((void **) &c->ii, cap, sizeof (int)) || grow ((void **) &c->jj, cap, sizeof (int)) ||
+        grow ((void **) &c->kk, cap, sizeof (int)))
+      return BMG_ENOMEM;
+    c->cap = cap;
   }
   c->level[c->ncell] = (unsigned char) l; c->leaf[c->ncell] = (unsigned char) leaf;
   c->ii[c->ncell] = i; c->jj[c->ncell] = j; c->kk[c->ncell] = k;
@@ -247,9 +258,9 @@ static void read_cell (read_ctx * c, int l, int i, int j, int k)
   const long at = c->cells->ncell;
   if (push_cell (c->cells, l, i, j, k, (flags & LEAF) != 0)) { c->err = BMG_ENOMEM; return; }
   if ((at + 1)*c->nvals > c->vcap) {
-    c->vcap = 2*c->vcap + 1024*c->nvals;
-    c->vals = realloc (c->vals, c->vcap*sizeof (double));
-    if (!c->vals) { c->err = BMG_ENOMEM; return; }
+    const long vcap = 2*c->vcap + 1024*c->nvals;
+    if (grow ((void **) &c->vals, vcap, sizeof (double))) { c->err = BMG_ENOMEM; return; }
+    c->vcap = vcap;
   }
   if (fread (c->vals + at*c->nvals, sizeof (double), c->nvals, c->fp) != (size_t) c->nvals) {
     c->err = BMG_EINVAL;
