@@ -121,7 +121,10 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def dist_init():
+def dist_init(backend=None, timeout_s=600):
+    """One process per GPU (torchrun's RANK / LOCAL_RANK / WORLD_SIZE): NCCL
+    with a device, gloo without one (the host-side tests).  The replicas
+    exchange nothing but the barrier and the maximum of their times."""
     import torch
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -129,9 +132,14 @@ def dist_init():
     if ws > 1:
         import datetime
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
-                                device_id=torch.device("cuda", local))
+        if backend is None:
+            backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=timeout_s),
+                                    device_id=torch.device("cuda", local))
+        else:
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=timeout_s))
     elif torch.cuda.is_available():
         torch.cuda.set_device(local)
     return ws, rank, local
@@ -144,11 +152,13 @@ def barrier(ws):
 
 
 def max_over_ranks(ws, v):
+    """The maximum of v over the ranks (the slowest replica's time)."""
     if ws == 1:
         return v
     import torch
     import torch.distributed as dist
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
