@@ -12,6 +12,39 @@
 
 namespace bmgd {
 
+/* programmatic dependent launch (sm_90+).  A kernel launched with
+   pdl_launch starts while its predecessor in the stream drains; it calls
+   pdl_wait () before touching global memory (the predecessor has then
+   completed and its writes are visible) and pdl_trigger () to let its own
+   successor be scheduled.  Only the launch latency overlaps: the order of
+   every memory access is that of plain stream order. */
+__device__ __forceinline__ void pdl_wait ()
+{
+  asm volatile ("griddepcontrol.wait;" ::: "memory");
+}
+
+__device__ __forceinline__ void pdl_trigger ()
+{
+  asm volatile ("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+template <typename... KArgs, typename... Args>
+inline cudaError_t pdl_launch (void (*k) (KArgs...), dim3 grid, dim3 block, size_t smem,
+                               cudaStream_t s, Args... args)
+{
+  cudaLaunchConfig_t cfg;
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx (&cfg, k, ((KArgs) args)...);
+}
+
 /* ---------------------------------------------------------------- */
 /* layout                                                            */
 /* ---------------------------------------------------------------- */

@@ -1492,6 +1492,8 @@ __global__ void __launch_bounds__ (BOT_THREADS, 1) k_bottom (const __grid_consta
 {
   extern __shared__ __align__ (16) unsigned char bsm[];
   const BCH bc = P.bc;
+  pdl_wait ();
+  pdl_trigger ();
   /* stage the coefficients of every level (asynchronous copies) */
   for (int m = 0; m < P.nlev; m++) {
     const BotLevel & L = P.lv[m];
@@ -1711,9 +1713,9 @@ int bmg_launch_bottom (int dim, const bmg_bottom_level * lv, int nlev, bmg_geom 
     if (e != cudaSuccess) return (int) e;
     configured[dev][dim - 1] = 1;
   }
-  if (dim == 1) k_bottom<1><<<1, BOT_THREADS, bytes, s>>> (P);
-  else if (dim == 2) k_bottom<2><<<1, BOT_THREADS, bytes, s>>> (P);
-  else k_bottom<3><<<1, BOT_THREADS, bytes, s>>> (P);
+  if (dim == 1) pdl_launch (k_bottom<1>, dim3 (1), dim3 (BOT_THREADS), bytes, s, P);
+  else if (dim == 2) pdl_launch (k_bottom<2>, dim3 (1), dim3 (BOT_THREADS), bytes, s, P);
+  else pdl_launch (k_bottom<3>, dim3 (1), dim3 (BOT_THREADS), bytes, s, P);
   cudaError_t r = cudaGetLastError ();
   return r == cudaSuccess ? 0 : (int) r;
 }

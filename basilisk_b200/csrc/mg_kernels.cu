@@ -70,6 +70,8 @@ template <int DIM, typename TC, typename TF>
 __global__ void k_prolong (bmg_geom gc, bmg_geom gf, const TC * __restrict__ s,
                            TF * __restrict__ f, BCH bc, int zero)
 {
+  pdl_wait ();
+  pdl_trigger ();
   int i, j, k;
   if (!cell_of_thread<DIM> (gf.n, i, j, k)) return;
   TC v = TC(0);
@@ -106,6 +108,8 @@ template <typename TC, typename TF>
 __global__ void k_prolong2d_blk (bmg_geom gc, bmg_geom gf, const TC * __restrict__ s,
                                  TF * __restrict__ f, BCH bc)
 {
+  pdl_wait ();
+  pdl_trigger ();
   const int cj = blockIdx.x*blockDim.x + threadIdx.x, ci = blockIdx.y*blockDim.y + threadIdx.y;
   if (ci >= gc.n || cj >= gc.n) return;
   TC m[3][3];
@@ -137,6 +141,8 @@ template <int DIM, typename TF, typename TC>
 __global__ void k_restrict (bmg_geom gf, bmg_geom gc, const TF * __restrict__ f,
                             TC * __restrict__ c)
 {
+  pdl_wait ();
+  pdl_trigger ();
   int i, j, k;
   if (!cell_of_thread<DIM> (gc.n, i, j, k)) return;
   TC sum = TC(0);
@@ -252,6 +258,8 @@ __global__ void k_residual (bmg_geom g, bmg_geom gr, const double * __restrict__
                             double Delta, TR * __restrict__ res,
                             unsigned long long * maxres)
 {
+  pdl_wait ();
+  pdl_trigger ();
   int i, j, k;
   double m = 0.;
   const double rD = 1./Delta;
@@ -288,6 +296,8 @@ template <int DIM, typename TD>
 __global__ void k_correct (bmg_geom g, bmg_geom gd, double * a, const TD * __restrict__ da,
                            bmg_bcdesc bc)
 {
+  pdl_wait ();
+  pdl_trigger ();
   int i, j, k;
   if (!cell_of_thread<DIM> (g.n, i, j, k)) return;
   const long long id = cidx<DIM> (g, i, j, k);
@@ -501,24 +511,24 @@ void prolong_dim (int stc, int stf, bmg_geom gc, bmg_geom gf, const void * c, vo
   if (DIM == 2 && !zero && gf.n == 2*gc.n) {
     dim3 gb = grid_shape<2> (gc.n), bb = block_shape<2> ();
     if (stc == BMG_ST_F64 && stf == BMG_ST_F64)
-      k_prolong2d_blk<double, double><<<gb, bb, 0, s>>> (gc, gf, (const double *) c, (double *) f, h);
+      pdl_launch (k_prolong2d_blk<double, double>, gb, bb, 0, s, gc, gf, (const double *) c, (double *) f, h);
     else if (stc == BMG_ST_F32 && stf == BMG_ST_F32)
-      k_prolong2d_blk<float, float><<<gb, bb, 0, s>>> (gc, gf, (const float *) c, (float *) f, h);
+      pdl_launch (k_prolong2d_blk<float, float>, gb, bb, 0, s, gc, gf, (const float *) c, (float *) f, h);
     else if (stc == BMG_ST_F64 && stf == BMG_ST_F32)
-      k_prolong2d_blk<double, float><<<gb, bb, 0, s>>> (gc, gf, (const double *) c, (float *) f, h);
+      pdl_launch (k_prolong2d_blk<double, float>, gb, bb, 0, s, gc, gf, (const double *) c, (float *) f, h);
     else
-      k_prolong2d_blk<float, double><<<gb, bb, 0, s>>> (gc, gf, (const float *) c, (double *) f, h);
+      pdl_launch (k_prolong2d_blk<float, double>, gb, bb, 0, s, gc, gf, (const float *) c, (double *) f, h);
     return;
   }
   dim3 gb = grid_shape<DIM> (gf.n), bb = block_shape<DIM> ();
   if (stc == BMG_ST_F64 && stf == BMG_ST_F64)
-    k_prolong<DIM, double, double><<<gb, bb, 0, s>>> (gc, gf, (const double *) c, (double *) f, h, zero);
+    pdl_launch (k_prolong<DIM, double, double>, gb, bb, 0, s, gc, gf, (const double *) c, (double *) f, h, zero);
   else if (stc == BMG_ST_F32 && stf == BMG_ST_F32)
-    k_prolong<DIM, float, float><<<gb, bb, 0, s>>> (gc, gf, (const float *) c, (float *) f, h, zero);
+    pdl_launch (k_prolong<DIM, float, float>, gb, bb, 0, s, gc, gf, (const float *) c, (float *) f, h, zero);
   else if (stc == BMG_ST_F64 && stf == BMG_ST_F32)
-    k_prolong<DIM, double, float><<<gb, bb, 0, s>>> (gc, gf, (const double *) c, (float *) f, h, zero);
+    pdl_launch (k_prolong<DIM, double, float>, gb, bb, 0, s, gc, gf, (const double *) c, (float *) f, h, zero);
   else
-    k_prolong<DIM, float, double><<<gb, bb, 0, s>>> (gc, gf, (const float *) c, (double *) f, h, zero);
+    pdl_launch (k_prolong<DIM, float, double>, gb, bb, 0, s, gc, gf, (const float *) c, (double *) f, h, zero);
 }
 
 template <int DIM>
@@ -527,13 +537,13 @@ void restrict_dim (int stf, int stc, bmg_geom gf, bmg_geom gc, const void * f, v
 {
   dim3 gb = grid_shape<DIM> (gc.n), bb = block_shape<DIM> ();
   if (stf == BMG_ST_F64 && stc == BMG_ST_F64)
-    k_restrict<DIM, double, double><<<gb, bb, 0, s>>> (gf, gc, (const double *) f, (double *) c);
+    pdl_launch (k_restrict<DIM, double, double>, gb, bb, 0, s, gf, gc, (const double *) f, (double *) c);
   else if (stf == BMG_ST_F32 && stc == BMG_ST_F32)
-    k_restrict<DIM, float, float><<<gb, bb, 0, s>>> (gf, gc, (const float *) f, (float *) c);
+    pdl_launch (k_restrict<DIM, float, float>, gb, bb, 0, s, gf, gc, (const float *) f, (float *) c);
   else if (stf == BMG_ST_F32 && stc == BMG_ST_F64)
-    k_restrict<DIM, float, double><<<gb, bb, 0, s>>> (gf, gc, (const float *) f, (double *) c);
+    pdl_launch (k_restrict<DIM, float, double>, gb, bb, 0, s, gf, gc, (const float *) f, (double *) c);
   else
-    k_restrict<DIM, double, float><<<gb, bb, 0, s>>> (gf, gc, (const double *) f, (float *) c);
+    pdl_launch (k_restrict<DIM, double, float>, gb, bb, 0, s, gf, gc, (const double *) f, (float *) c);
 }
 
 template <int DIM>
@@ -553,12 +563,12 @@ void residual_dim (int st, bmg_geom g, bmg_geom gr, const double * a, const doub
   int ex;
   const bool pow2 = Delta > 0. && frexp (Delta, &ex) == 0.5 && ex > -1000 && ex < 1000;
   if (st == BMG_ST_F64) {
-    if (pow2) k_residual<DIM, double, true><<<gb, bb, 0, s>>> (g, gr, a, b, ax, ay, az, lam, Delta, (double *) res, maxres);
-    else k_residual<DIM, double, false><<<gb, bb, 0, s>>> (g, gr, a, b, ax, ay, az, lam, Delta, (double *) res, maxres);
+    if (pow2) pdl_launch (k_residual<DIM, double, true>, gb, bb, 0, s, g, gr, a, b, ax, ay, az, lam, Delta, (double *) res, maxres);
+    else pdl_launch (k_residual<DIM, double, false>, gb, bb, 0, s, g, gr, a, b, ax, ay, az, lam, Delta, (double *) res, maxres);
   }
   else {
-    if (pow2) k_residual<DIM, float, true><<<gb, bb, 0, s>>> (g, gr, a, b, ax, ay, az, lam, Delta, (float *) res, maxres);
-    else k_residual<DIM, float, false><<<gb, bb, 0, s>>> (g, gr, a, b, ax, ay, az, lam, Delta, (float *) res, maxres);
+    if (pow2) pdl_launch (k_residual<DIM, float, true>, gb, bb, 0, s, g, gr, a, b, ax, ay, az, lam, Delta, (float *) res, maxres);
+    else pdl_launch (k_residual<DIM, float, false>, gb, bb, 0, s, g, gr, a, b, ax, ay, az, lam, Delta, (float *) res, maxres);
   }
 }
 
@@ -568,9 +578,9 @@ void correct_dim (int st, bmg_geom g, bmg_geom gd, double * a, const void * da,
 {
   dim3 gb = grid_shape<DIM> (g.n), bb = block_shape<DIM> ();
   if (st == BMG_ST_F64)
-    k_correct<DIM, double><<<gb, bb, 0, s>>> (g, gd, a, (const double *) da, bc);
+    pdl_launch (k_correct<DIM, double>, gb, bb, 0, s, g, gd, a, (const double *) da, bc);
   else
-    k_correct<DIM, float><<<gb, bb, 0, s>>> (g, gd, a, (const float *) da, bc);
+    pdl_launch (k_correct<DIM, float>, gb, bb, 0, s, g, gd, a, (const float *) da, bc);
 }
 
 template <int DIM>

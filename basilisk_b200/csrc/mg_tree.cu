@@ -48,6 +48,8 @@ __device__ __forceinline__ double coef (const bmg_tree_coef & c, long long id)
 
 __global__ void k_set (const uint32_t * __restrict__ list, long n, TL T, double * s, double v)
 {
+  pdl_wait ();
+  pdl_trigger ();
   GRID_STRIDE (k, n) {
     int l, i, j;
     unpack (list[k], l, i, j);
@@ -70,6 +72,8 @@ __device__ __forceinline__ double bilinear (const TL & T, const double * s, int 
 /* foreach_level (l) s[] = bilinear (point, s) (poisson.h:64-68) */
 __global__ void k_prolong (const uint32_t * __restrict__ list, long n, TL T, double * s)
 {
+  pdl_wait ();
+  pdl_trigger ();
   GRID_STRIDE (k, n) {
     int l, i, j;
     unpack (list[k], l, i, j);
@@ -89,6 +93,8 @@ __device__ __forceinline__ void halo_child (const uint32_t * list, long k, const
 
 __global__ void k_halo (const uint32_t * __restrict__ list, long n, TL T, double * s)
 {
+  pdl_wait ();
+  pdl_trigger ();
   GRID_STRIDE (k, 4*n)
     halo_child (list, k, T, s);
 }
@@ -111,6 +117,8 @@ __device__ __forceinline__ void restrict_cell (const uint32_t * list, long k, co
 
 __global__ void k_restrict (const uint32_t * __restrict__ list, long n, TL T, double * s)
 {
+  pdl_wait ();
+  pdl_trigger ();
   GRID_STRIDE (k, n)
     restrict_cell (list, k, T, s);
 }
@@ -130,6 +138,8 @@ __device__ __forceinline__ bool refined_at (const TL & T, const unsigned char * 
 __global__ void k_restrict_faces (const uint32_t * __restrict__ list, long n, TL T,
                                   const unsigned char * __restrict__ fl, double * ax, double * ay)
 {
+  pdl_wait ();
+  pdl_trigger ();
   GRID_STRIDE (k, n) {
     int l, i, j;
     unpack (list[k], l, i, j);
@@ -176,6 +186,8 @@ __device__ __forceinline__ void ghost_value (const bmg_tree_rule & r, const TL &
 __global__ void k_bc (const bmg_tree_rule * __restrict__ rules, long n, TL T, double * s,
                       bmg_tree_bc bc, int homog)
 {
+  pdl_wait ();
+  pdl_trigger ();
   GRID_STRIDE (k, n)
     ghost_value (rules[k], T, s, bc, homog);
 }
@@ -187,6 +199,8 @@ __global__ void k_stage (const uint32_t * __restrict__ list, long n, int op,
                          const bmg_tree_rule * __restrict__ rules, long nr, TL T, double * s,
                          bmg_tree_bc bc, int homog)
 {
+  pdl_wait ();
+  pdl_trigger ();
   const long w = op == BMG_T_OP_HALO ? 4*n : op == BMG_T_OP_RESTRICT ? n : 0;
   GRID_STRIDE (k, w + nr) {
     if (k >= w) ghost_value (rules[k - w], T, s, bc, homog);
@@ -200,6 +214,8 @@ __global__ void k_relax (const uint32_t * __restrict__ list, long n, TL T,
                          const double * a, const double * __restrict__ b,
                          bmg_tree_coef ax, bmg_tree_coef ay, bmg_tree_coef lam, double * out)
 {
+  pdl_wait ();
+  pdl_trigger ();
   GRID_STRIDE (k, n) {
     int l, i, j;
     unpack (list[k], l, i, j);
@@ -220,6 +236,8 @@ __global__ void k_relax (const uint32_t * __restrict__ list, long n, TL T,
 __global__ void k_jacobi (const uint32_t * __restrict__ list, long n, TL T, double * a,
                           const double * __restrict__ c)
 {
+  pdl_wait ();
+  pdl_trigger ();
   GRID_STRIDE (k, n) {
     int l, i, j;
     unpack (list[k], l, i, j);
@@ -256,6 +274,8 @@ __global__ void k_residual (const uint32_t * __restrict__ list, long n, TL T,
                             const double * __restrict__ b, bmg_tree_coef ax, bmg_tree_coef ay,
                             bmg_tree_coef lam, double * res, unsigned long long * maxres)
 {
+  pdl_wait ();
+  pdl_trigger ();
   double m = 0.;
   GRID_STRIDE (k, n) {
     int l, i, j;
@@ -291,6 +311,8 @@ __global__ void k_residual (const uint32_t * __restrict__ list, long n, TL T,
 __global__ void k_add (const uint32_t * __restrict__ list, long n, TL T, double * a,
                        const double * __restrict__ da)
 {
+  pdl_wait ();
+  pdl_trigger ();
   GRID_STRIDE (k, n) {
     int l, i, j;
     unpack (list[k], l, i, j);
@@ -303,6 +325,8 @@ __global__ void k_add (const uint32_t * __restrict__ list, long n, TL T, double 
 __global__ void k_sum_partial (const uint32_t * __restrict__ list, long n, TL T,
                                const double * __restrict__ s, double * partials)
 {
+  pdl_wait ();
+  pdl_trigger ();
   __shared__ double sh[256];
   double v = 0.;
   GRID_STRIDE (k, n) {
@@ -321,6 +345,8 @@ __global__ void k_sum_partial (const uint32_t * __restrict__ list, long n, TL T,
 
 __global__ void k_sum_final (const double * __restrict__ partials, int np, double * out)
 {
+  pdl_wait ();
+  pdl_trigger ();
   __shared__ double sh[1024];
   sh[threadIdx.x] = (int) threadIdx.x < np ? partials[threadIdx.x] : 0.;
   __syncthreads ();
@@ -354,7 +380,7 @@ int bmg_tree_launch_set (const uint32_t * list, long n, const bmg_tree_levels * 
                          double * s, double v, cudaStream_t st)
 {
   if (n <= 0) return 0;
-  k_set<<<blocks_for (n), NT, 0, st>>> (list, n, *T, s, v);
+  pdl_launch (k_set, dim3 (blocks_for (n)), dim3 (NT), 0, st, list, n, *T, s, v);
   return status ();
 }
 
@@ -362,7 +388,7 @@ int bmg_tree_launch_prolong (const uint32_t * list, long n, const bmg_tree_level
                              double * s, cudaStream_t st)
 {
   if (n <= 0) return 0;
-  k_prolong<<<blocks_for (n), NT, 0, st>>> (list, n, *T, s);
+  pdl_launch (k_prolong, dim3 (blocks_for (n)), dim3 (NT), 0, st, list, n, *T, s);
   return status ();
 }
 
@@ -370,7 +396,7 @@ int bmg_tree_launch_halo (const uint32_t * list, long n, const bmg_tree_levels *
                           double * s, cudaStream_t st)
 {
   if (n <= 0) return 0;
-  k_halo<<<blocks_for (4*n), NT, 0, st>>> (list, n, *T, s);
+  pdl_launch (k_halo, dim3 (blocks_for (4*n)), dim3 (NT), 0, st, list, n, *T, s);
   return status ();
 }
 
@@ -378,7 +404,7 @@ int bmg_tree_launch_restrict (const uint32_t * list, long n, const bmg_tree_leve
                               double * s, cudaStream_t st)
 {
   if (n <= 0) return 0;
-  k_restrict<<<blocks_for (n), NT, 0, st>>> (list, n, *T, s);
+  pdl_launch (k_restrict, dim3 (blocks_for (n)), dim3 (NT), 0, st, list, n, *T, s);
   return status ();
 }
 
@@ -387,7 +413,7 @@ int bmg_tree_launch_restrict_faces (const uint32_t * list, long n, const bmg_tre
                                     cudaStream_t st)
 {
   if (n <= 0) return 0;
-  k_restrict_faces<<<blocks_for (n), NT, 0, st>>> (list, n, *T, flags, ax, ay);
+  pdl_launch (k_restrict_faces, dim3 (blocks_for (n)), dim3 (NT), 0, st, list, n, *T, flags, ax, ay);
   return status ();
 }
 
@@ -395,7 +421,7 @@ int bmg_tree_launch_bc (const bmg_tree_rule * rules, long n, const bmg_tree_leve
                         double * s, const bmg_tree_bc * bc, int homogeneous, cudaStream_t st)
 {
   if (n <= 0) return 0;
-  k_bc<<<blocks_for (n), NT, 0, st>>> (rules, n, *T, s, *bc, homogeneous);
+  pdl_launch (k_bc, dim3 (blocks_for (n)), dim3 (NT), 0, st, rules, n, *T, s, *bc, homogeneous);
   return status ();
 }
 
@@ -405,7 +431,7 @@ int bmg_tree_launch_stage (const uint32_t * list, long n, int op, const bmg_tree
 {
   const long w = (op == BMG_T_OP_HALO ? 4*n : op == BMG_T_OP_RESTRICT ? n : 0) + nrules;
   if (w <= 0) return 0;
-  k_stage<<<blocks_for (w), NT, 0, st>>> (list, n, op, rules, nrules, *T, s, *bc, homogeneous);
+  pdl_launch (k_stage, dim3 (blocks_for (w)), dim3 (NT), 0, st, list, n, op, rules, nrules, *T, s, *bc, homogeneous);
   return status ();
 }
 
@@ -415,7 +441,7 @@ int bmg_tree_launch_relax (const uint32_t * list, long n, const bmg_tree_levels 
                            cudaStream_t st)
 {
   if (n <= 0) return 0;
-  k_relax<<<blocks_for (n), NT, 0, st>>> (list, n, *T, a, b, ax, ay, lambda, out);
+  pdl_launch (k_relax, dim3 (blocks_for (n)), dim3 (NT), 0, st, list, n, *T, a, b, ax, ay, lambda, out);
   return status ();
 }
 
@@ -423,7 +449,7 @@ int bmg_tree_launch_jacobi (const uint32_t * list, long n, const bmg_tree_levels
                             double * a, const double * c, cudaStream_t st)
 {
   if (n <= 0) return 0;
-  k_jacobi<<<blocks_for (n), NT, 0, st>>> (list, n, *T, a, c);
+  pdl_launch (k_jacobi, dim3 (blocks_for (n)), dim3 (NT), 0, st, list, n, *T, a, c);
   return status ();
 }
 
@@ -433,7 +459,7 @@ int bmg_tree_launch_residual (const uint32_t * leaves, long n, const bmg_tree_le
                               double * res, unsigned long long * maxres, cudaStream_t st)
 {
   if (n <= 0) return 0;
-  k_residual<<<blocks_for (n), NT, 0, st>>> (leaves, n, *T, flags, a, b, ax, ay, lambda, res, maxres);
+  pdl_launch (k_residual, dim3 (blocks_for (n)), dim3 (NT), 0, st, leaves, n, *T, flags, a, b, ax, ay, lambda, res, maxres);
   return status ();
 }
 
@@ -441,7 +467,7 @@ int bmg_tree_launch_add (const uint32_t * leaves, long n, const bmg_tree_levels 
                          double * a, const double * da, cudaStream_t st)
 {
   if (n <= 0) return 0;
-  k_add<<<blocks_for (n), NT, 0, st>>> (leaves, n, *T, a, da);
+  pdl_launch (k_add, dim3 (blocks_for (n)), dim3 (NT), 0, st, leaves, n, *T, a, da);
   return status ();
 }
 
@@ -450,8 +476,8 @@ int bmg_tree_launch_sum (const uint32_t * list, long n, const bmg_tree_levels * 
                          cudaStream_t st)
 {
   if (npartials < 1 || npartials > 1024) return (int) cudaErrorInvalidValue;
-  k_sum_partial<<<npartials, 256, 0, st>>> (list, n, *T, s, partials);
-  k_sum_final<<<1, 1024, 0, st>>> (partials, npartials, out);
+  pdl_launch (k_sum_partial, dim3 (npartials), dim3 (256), 0, st, list, n, *T, s, partials);
+  pdl_launch (k_sum_final, dim3 (1), dim3 (1024), 0, st, partials, npartials, out);
   return status ();
 }
 
