@@ -387,3 +387,31 @@ def test_bad_handles_rejected():
         g.poisson(a, v.components[0])
     with pytest.raises((ValueError, bmg.BMGError)):
         a.set(np.zeros((3, 3, 3)))
+
+
+def test_mixed_form_error_on_the_headline_workload():
+    """The 2048^2 two-phase workload in the mixed and the plain FP64 forms,
+    both driven to a maximum residual of 5e-10 (the FP64 form's own floor on
+    this problem is about 2e-10: the residual's rounding, with Laplacian terms
+    of order |a|/Delta^2 and a density ratio of 1000): the mixed form's
+    solution agrees with the FP64 one to 2e-8 relative (max norm; 5.7e-9
+    measured); the difference is that of two solutions at that residual, not
+    the FP32 arithmetic (at tolerance 1e-6 both differ by 1.7e-5)."""
+    import basilisk_b200 as bmg
+    from basilisk_b200 import problems
+    prob = problems.two_phase_2d(depth=11, seed=1)
+    sols = {}
+    bmg.set_niter(nitermax=400)
+    try:
+        for prec in ("fp64", "mixed"):
+            g, a, b, alpha, lam = gpu_grid(prob, relax="rbgs", precision=prec)
+            st = g.poisson(a, b, alpha=alpha, lambda_=lam, tolerance=5e-10)
+            assert st["resa"] <= 5e-10, (prec, st)
+            sols[prec] = a.get()
+            g.close()
+    finally:
+        bmg.set_niter(nitermax=100)
+    ref = sols["fp64"]
+    rel = np.abs(sols["mixed"] - ref).max() / np.abs(ref).max()
+    print("mixed vs fp64 at residual 5e-10: %.3g relative" % rel)
+    assert rel <= 2e-8
