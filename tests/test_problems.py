@@ -61,3 +61,16 @@ def test_band_refinement():
     assert not cond(9, 0.75, 0.5)                  # never past the depth
     assert cond(7, 0.75, 0.5)                      # on the circle r = 0.25
     assert not cond(7, 0.5, 0.5)                   # far from it
+
+
+def test_two_phase_tree_configuration():
+    """The quadtree workload (two_phase_tree): every cell below level 5 and a
+    band of four cells of each level around r = 0.25 refined up to level 11,
+    2:1 balanced, gives 77,068 leaves on levels 5 to 11 (the tree oracle's
+    refine, tree-common.h:308-326)."""
+    from oracle import tree as otree
+    t = otree.Tree(11)
+    t.refine(problems.band_refinement(11, 5))
+    assert t.depth == 11 and t.leaves == 77068
+    levels = [l for l in range(12) if ((t.flags(l) & otree.LEAF) != 0).any()]
+    assert levels == list(range(5, 12))
