@@ -13,6 +13,15 @@ library (``bmg_adjoint_gradients``):
                  interior cell's term only)
     dl/dlambda = -mu a
 
+On a singular problem (no Dirichlet side and no lambda: periodic or Neumann
+walls, pure Poisson) the solution is defined up to a constant.  The forward
+pass then solves for the zero-mean projection of b (the compatibility
+condition) and returns the zero-mean solution; the backward pass projects
+dl/da to zero mean before the adjoint solve and returns the zero-mean
+adjoint, so the gradients are those of that well-defined map.  A solve that
+does not reach the tolerance raises ``BMGError`` (status ENOTCONV) instead of
+returning an unconverged field.
+
 The function keeps only the forward solution for the backward pass.
 ``chain`` runs time-stepped sequences of solves with a checkpoint every k
 steps (the solutions inside a segment are recomputed in the backward pass).
@@ -51,6 +60,8 @@ class Problem:
             self.mu.bc(side, kind, 0.0)          # the homogeneous twin
         self.alpha = g.face_vector() if alpha else None
         self.lam = g.scalar() if lam else None
+        # no Dirichlet side and no lambda: L has the constants as its null space
+        self.singular = not lam and not any(kind == "dirichlet" for kind, _ in self.bc.values())
         self.stats = []
 
     def close(self):
@@ -69,18 +80,28 @@ class Problem:
         st = self.grid.poisson(a, b, alpha=self.alpha, lambda_=self.lam,
                                tolerance=self.tolerance, nrelax=self.nrelax)
         self.stats.append(st)
+        if st["status"] != _lib.OK:
+            raise _lib.BMGError(st["status"], "differentiable solve (residual %g after %d "
+                                "V-cycles, tolerance %g)" % (st["resa"], st["i"], self.tolerance))
         a.get(out=out)
+        if self.singular:
+            out -= out.mean()
         return st
+
+    def _compatible(self, rhs):
+        """the right-hand side of a solve: its zero-mean projection on a
+        singular problem (in FP64, before the solve)"""
+        return rhs - rhs.mean() if self.singular else rhs
 
     def forward_one(self, b, alpha, lam, out):
         self._set_coefficients(alpha, lam)
-        self.b.set(b)
+        self.b.set(self._compatible(b))
         return self._solve(self.a, self.b, out)
 
     def backward_one(self, a_sol, grad_a, alpha, lam, grad_b, grad_alpha, grad_lam):
         """mu from dl/da, then the coefficient gradients; grad_b receives mu."""
         self._set_coefficients(alpha, lam)
-        self.rhs.set(grad_a)
+        self.rhs.set(self._compatible(grad_a))
         self._solve(self.mu, self.rhs, grad_b)
         # a with the ghosts of its boundary conditions, for the face kernel
         self.a.set(a_sol)

@@ -603,6 +603,10 @@ static int ensure_workspace (bmg_grid * g, int mixed)
     CK (cudaMalloc ((void **) &g->ws32, W32_N*total32 (g)*sizeof (float)));
     CK (cudaMemsetAsync (g->ws32, 0, W32_N*total32 (g)*sizeof (float), g->stream));
   }
+  /* the zero-mean copy of b of the mixed form's singular problems: part of
+     the workspace, so that a solve itself allocates nothing */
+  if (mixed && !g->bproj)
+    CK (cudaMalloc ((void **) &g->bproj, g->g64[g->depth].size*sizeof (double)));
   return BMG_OK;
 }
 
@@ -1035,7 +1039,6 @@ static int solve (bmg_grid * g, field_t * a, field_t * b, coefs_t * c, int nrela
   /* mixed form, singular problem: FP64 zero-mean projection of b */
   const double * bdata = b->lv[L];
   if (mixed && is_singular (g, a, c)) {
-    if (!g->bproj) CK (cudaMalloc ((void **) &g->bproj, g->g64[L].size*sizeof (double)));
     CK (cudaMemcpyAsync (g->bproj, b->lv[L], g->g64[L].size*sizeof (double),
                          cudaMemcpyDeviceToDevice, g->stream));
     CL (bmg_launch_shift (g->dim, g->g64[L], g->bproj, g->d_sum, 1./(double) ncells (g, L), g->stream));

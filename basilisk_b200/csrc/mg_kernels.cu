@@ -925,9 +925,24 @@ extern "C" int bmg_sum_noalloc (const double * values, size_t count, double * re
     cudaGetLastError ();
     return 7; /* BMG_ENODEV */
   }
-  /* once per device, with that device current: the device address of the
-     scratch array (its name in host code is only a stand-in) */
-  if (!noalloc_scratch_ptr[dev]) {
+  cudaStream_t s = (cudaStream_t) stream;
+  /* the device address of the scratch array (its name in host code is only
+     a stand-in), looked up with the device current.  Outside a stream
+     capture it is looked up on every call, so that a context that was torn
+     down and created again (cudaDeviceReset) gets the module's new address;
+     inside a capture the address cached by the last call outside one is
+     used (the first call on a device must come before any capture). */
+  enum cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing (s, &cs) != cudaSuccess) {
+    cudaGetLastError ();
+    return 2; /* BMG_ECUDA */
+  }
+  if (cs == cudaStreamCaptureStatusNone || !noalloc_scratch_ptr[dev]) {
+    if (cs != cudaStreamCaptureStatusNone) {
+      fprintf (stderr, "bmg_sum_noalloc: the first call on device %d is inside a stream "
+               "capture; call it once before capturing\n", dev);
+      return 1; /* BMG_EINVAL */
+    }
     void * p = NULL;
     cudaError_t e = cudaGetSymbolAddress (&p, bmg_noalloc_scratch);
     if (e != cudaSuccess || !p) {
@@ -937,7 +952,6 @@ extern "C" int bmg_sum_noalloc (const double * values, size_t count, double * re
     }
     noalloc_scratch_ptr[dev] = (double *) p;
   }
-  cudaStream_t s = (cudaStream_t) stream;
   const int np = (int) ((count + BMG_NOALLOC_TILE - 1)/BMG_NOALLOC_TILE);
   /* nothing accumulates across calls: stage 1 overwrites the np partials
      that stage 2 reads, and stage 2 overwrites *result (count 0: one empty

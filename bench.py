@@ -274,6 +274,26 @@ def cpu_solve(prob, threads=None):
     return time.perf_counter() - t0, st, threads
 
 
+def oracle_floor(prob, threads=None):
+    """The oracle's red-black solve of the workload driven to its residual
+    floor: to 1e-9, then on to 3e-10 (further cycles stall above 2e-10 while
+    nrelax climbs to 100).  Returns (solution at the floor, its max residual,
+    the 1e-9 iterate)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from oracle import oracle
+    from helpers import oracle_grid
+    threads = threads or os.cpu_count()
+    oracle.set_globals(2, nitermax=400)
+    try:
+        g = oracle_grid(prob, relax=oracle.RELAX_RBGS, threads=threads)
+        g.poisson(tolerance=1e-9)
+        a9 = g.get_a()
+        st = g.poisson(tolerance=3e-10)
+        return g.get_a(), st["resa"], a9
+    finally:
+        oracle.set_globals(2, nitermax=100)
+
+
 def run_workload(args, ws, rank, local):
     """The other workloads of the scope table, one JSON line each (not the
     headline): the quadtree problem (two_phase_tree, depth 11), the 3D
@@ -574,6 +594,9 @@ def main():
     relax_avg_ms = cmx["relax_ms"] / max(1, cmx["relax_sweeps"])
     relax_bytes = cmx["relax_bytes"] / max(1, cmx["relax_sweeps"])
     achieved = relax_bytes / (relax_avg_ms * 1e-3) / 1e9 if relax_avg_ms else None
+    # the DRAM rate of the same kernel: its measured traffic per launch of
+    # four sweeps over the time of four sweeps
+    dram = TILE_LAUNCH_DRAM_BYTES / (4 * relax_avg_ms * 1e-3) / 1e9 if relax_avg_ms else None
     line = {
         "metric": METRIC, "value": ws * 1e3 / ms_mx, "unit": "solves/s", "n_gpus": ws,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_mx,
@@ -594,17 +617,34 @@ def main():
                      "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak if achieved else None,
                      # DRAM bytes (read + write) of one finest-level launch of four
-                     # sweeps, from the ncu capture summarised in
-                     # profiles/k_relax_tile2d_w_fp32_2048_ncu.md; the algorithmic
+                     # sweeps, from an ncu capture of that kernel; the algorithmic
                      # bytes of that launch are 335.5e6
                      "traffic": TILE_LAUNCH_DRAM_BYTES, "traffic_per": "launch (4 sweeps)",
-                     "peak_kind": peak_kind},
+                     "peak_kind": peak_kind,
+                     "note": "achieved counts algorithmic bytes (5 arrays per cell per sweep); "
+                             "with 4 sweeps per launch on on-chip tiles the DRAM traffic is "
+                             "lower, so the DRAM rate (dram_achieved) is the HBM utilisation "
+                             "and vcycle_frac the whole V-cycle's algorithmic rate",
+                     "dram_achieved": dram, "dram_frac": dram / peak if dram else None,
+                     "vcycle_frac": {"mixed": fmx["vcycle_gbs"] / peak if fmx["vcycle_gbs"] else None,
+                                     "fp64": f64["vcycle_gbs"] / peak if f64["vcycle_gbs"] else None}},
         "clocks": clk,
         "gpu_launches": int(cmx["launches"]),
         "e2e": {"value": ws * 1e3 / ms_e2e, "unit": "solves/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
     }
     if not args.no_cpu:
+        try:
+            af, fres, a9 = oracle_floor(prob)
+            rel = lambda x: float(np.abs(x - af).max() / np.abs(af).max())
+            line["error_vs_oracle"] = {
+                "fp64": rel(a64), "mixed": rel(amx), "oracle_floor": fres,
+                "oracle_1e-9_vs_floor": rel(a9),
+                "note": "max |a - a_oracle| / max |a_oracle|, both forms at residual 1e-6, "
+                        "the oracle (red-black, FP64) driven to its residual floor"}
+        except Exception as e:  # reported, never required
+            line["error_vs_oracle"] = {"fp64": None, "mixed": None, "oracle_floor": None,
+                                       "note": "failed: %s" % e}
         try:
             t, st, threads = cpu_solve(prob)
             line["cpu_baseline"] = {

@@ -297,9 +297,12 @@ int bmg_adjoint_gradients (bmg_grid * grid, bmg_scalar mu, bmg_scalar a,
    let nothing else allocate.  It allocates nothing: its scratch is a static
    32 KB device array inside the library (4096 partial sums), so count is at
    most 16,777,216 (4096^2 in 2D, 256^3 in 3D); larger counts are rejected
-   with BMG_EINVAL and a message on stderr.  The first call on a device looks
-   up the scratch's device address with that device current; make that
-   first call before any stream capture.  All calls share the scratch: calls
+   with BMG_EINVAL and a message on stderr.  Every call outside a stream
+   capture looks up the scratch's device address with the current device
+   (so a context created again after cudaDeviceReset is followed); a call
+   inside a capture uses the address found by the last call outside one, so
+   make one call on each device before any stream capture (a first call
+   inside a capture fails with BMG_EINVAL).  All calls share the scratch: calls
    that overlap on the GPU (different streams, no ordering) race.  The
    result is asynchronous on stream.  No counterpart in the reference. */
 int bmg_sum_noalloc (const double * values, size_t count, double * result, void * stream);

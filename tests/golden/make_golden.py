@@ -1,9 +1,9 @@
 """Collect the reference's golden logs for the Poisson path into a fixture.
 
 Reads the Basilisk test logs (``src/test/*.ref``, ``*.cref``) from the
-reference checkout given as argv[1] (default: the read-only mount used when
-this fixture was made) and writes ``reference_logs.json`` next to this
-script.  The logs are the reference's own known-answer outputs; the drivers
+``src`` directory of a reference checkout, given as argv[1] or in the
+environment variable BASILISK_SRC, and writes ``reference_logs.json`` next
+to this script.  The logs are the reference's own known-answer outputs; the drivers
 in ``tests/golden_drivers.py`` reproduce the programs that printed them.
 Run once; the committed JSON is what the tests read.
 """
@@ -27,7 +27,9 @@ LOGS = {
 
 
 def main():
-    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference/src"
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("BASILISK_SRC")
+    if not root:
+        sys.exit("usage: make_golden.py <basilisk checkout>/src  (or set BASILISK_SRC)")
     out = {}
     for key, (prog, log) in LOGS.items():
         with open(os.path.join(root, log)) as f:

@@ -104,6 +104,60 @@ def test_gradient_matches_dense_solve(case):
     prob.close()
 
 
+def test_singular_periodic_poisson_matches_pinned_dense_solve():
+    """32x32 periodic pure Poisson (lambda = 0, L singular): b with a non-zero
+    mean and a loss that is not invariant under a + const.  The reference
+    map is the zero-mean solution of the zero-mean projection of b, i.e. a
+    dense solve of (L + J/N) a = b - mean(b), J the all-ones matrix (it
+    pins mean(a) = 0 and is regular); gradients in b and alpha agree to
+    1e-6 relative."""
+    import torch
+    from basilisk_b200.autograd import solve
+    depth, n = 5, 32
+    prob = make_problem(depth, (0, 1), False, lam=False)
+    assert prob.singular
+    b, kx, ky, _, aobs = random_inputs(n, 7, lam=False)
+    b = b + 0.3                                       # incompatible as given
+    ax, ay = torch.exp(kx), torch.exp(ky)
+    ax[n] = ax[0]; ay[:, n] = ay[:, 0]
+    ins = [t.clone().requires_grad_(True) for t in (b, ax, ay)]
+    a = solve(prob, ins[0], alpha=[ins[1], ins[2]])
+    assert abs(a.mean().item()) < 1e-12 * a.abs().max().item()
+    loss = 0.5 * ((a - aobs) ** 2).sum() + (a * aobs).sum()
+    g_ours = torch.autograd.grad(loss, ins)
+    ref = [t.clone().requires_grad_(True) for t in (b, ax, ay)]
+    L = dense_operator(n, [ref[1], ref[2]], None, 1.0 / n, (True, True), False)
+    N = n * n
+    Lp = L + torch.full((N, N), 1.0 / N, dtype=torch.float64, device=L.device)
+    bz = ref[0] - ref[0].mean()
+    ad = torch.linalg.solve(Lp, bz.reshape(-1)).reshape(n, n)
+    assert torch.allclose(a.detach(), ad.detach(), rtol=0, atol=1e-9 * ad.abs().max().item())
+    loss_d = 0.5 * ((ad - aobs) ** 2).sum() + (ad * aobs).sum()
+    g_ref = torch.autograd.grad(loss_d, ref)
+    for name, go, gr in zip(("b", "alpha_x", "alpha_y"), g_ours, g_ref):
+        if name == "alpha_x":
+            go, gr = go[:n], gr[:n]
+        if name == "alpha_y":
+            go, gr = go[:, :n], gr[:, :n]
+        err = (go - gr).abs().max().item() / gr.abs().max().item()
+        assert err < RTOL, (name, err)
+    prob.close()
+
+
+def test_unconverged_solve_raises():
+    """A solve that cannot reach its tolerance within NITERMAX cycles raises
+    instead of returning an unconverged field."""
+    import torch
+    from basilisk_b200 import _lib
+    from basilisk_b200.autograd import solve
+    prob = make_problem(4, (), True, lam=False, tol=1e-30)
+    b, kx, ky, _, _ = random_inputs(16, 8, lam=False)
+    with pytest.raises(_lib.BMGError) as e:
+        solve(prob, b, alpha=[torch.exp(kx), torch.exp(ky)])
+    assert e.value.status == _lib.ENOTCONV
+    prob.close()
+
+
 def test_gradient_matches_central_differences():
     """Directional derivatives in b, kappa (alpha = exp(kappa) on faces) and
     lambda against central differences with h = 1e-6."""
