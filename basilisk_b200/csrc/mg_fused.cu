@@ -713,6 +713,293 @@ k_relax_tile2d_w (bmg_geom g, float * __restrict__ out, const float * __restrict
   }
 }
 
+/* ---------------------------------------------------------------- */
+/* persistent level kernel: all nrelax sweeps of one FP32 level       */
+/* ---------------------------------------------------------------- */
+
+/* The middle levels of the mixed form's cycle (128^2 .. 512^2) are
+   latency-bound as launches of S sweeps: every launch loads the
+   coefficients of its tiles again, runs 2S colour passes and drains.  This
+   kernel does all nrelax sweeps of such a level in one cooperative launch:
+   each CTA owns one TS x TS tile for the whole launch, computes its staged
+   region's weights (as k_relax_tile2d_w) once, and then repeats blocks of
+   S sweeps -- stage the iterate of the W x W region from the partner
+   buffer, 2S colour passes in shared memory, the tile interior (and its
+   ghost images) back to global memory -- with a grid-wide barrier between
+   blocks, so that a block reads the tiles its neighbours wrote in the one
+   before.  The first block stages the bilinear prolongation of the coarse
+   level (multigrid-common.h:124-140, the expression of k_prolong2d_blk)
+   instead of an iterate, which fuses the level's prolongation in.  Blocks
+   alternate between the two buffers: block b writes buf[b & 1].
+
+   The grid barrier is a counter in global memory (zeroed before the
+   launch): thread 0 of each CTA adds one after a fence and waits for
+   (b + 1) x CTAs.  Its wait is bounded: after PERSIST_SPIN_LIMIT polls it
+   sets the error flag sync[1], which makes every later barrier return at
+   once, and the host turns the flag into an error status.  The launch is
+   cooperative, so all CTAs are resident together, and it triggers no
+   dependent launch, so no later kernel can take the slots of CTAs that are
+   not resident yet.  Iterate loads bypass L1 (ld.global.cg): the buffers
+   are written by other CTAs during the launch. */
+#define PERSIST_SPIN_LIMIT (1u << 20)
+
+__device__ __forceinline__ unsigned ld_acquire_u32 (const unsigned * p)
+{
+  unsigned v;
+  asm volatile ("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ void grid_sync (unsigned * sync, unsigned target)
+{
+  __syncthreads ();
+  if (threadIdx.x == 0 && threadIdx.y == 0) {
+    __threadfence ();
+    atomicAdd (sync, 1u);
+    if (!ld_acquire_u32 (sync + 1)) {
+      unsigned spins = 0;
+      while (ld_acquire_u32 (sync) < target) {
+        if (++spins > PERSIST_SPIN_LIMIT) { atomicExch (sync + 1, 1u); break; }
+        __nanosleep (64);
+      }
+    }
+    __threadfence ();
+  }
+  __syncthreads ();
+}
+
+namespace pw {
+/* W x W staged cells, BX x BY threads, each owning eight cells of one row;
+   the rows of a warp all have the same parity */
+template <int W> struct Shape {
+  static constexpr int M = W/2, WM = W*M, BX = W/8, BY = W, NT = BX*BY, RW = 32/BX;
+  static_assert (W % 8 == 0 && 32 % BX == 0 && BY % (2*RW) == 0, "rows of one parity per warp");
+};
+}
+
+template <int W, int TS, bool LAM>
+__global__ void __launch_bounds__ (W*W/8, W == 64 ? 1 : 4)
+k_level_w (bmg_geom g, float * buf0, float * buf1, const float * __restrict__ res,
+           Coef<float> ax, Coef<float> ay, Coef<float> lam, float Delta, BCH bc, int nrelax,
+           bmg_geom gc, const float * __restrict__ coarse, unsigned * sync)
+{
+  typedef pw::Shape<W> Sh;
+  constexpr int M = Sh::M, WM = Sh::WM, BX = Sh::BX, RW = Sh::RW, nth = Sh::NT;
+  constexpr int H = (W - TS)/2, S = H/2;
+  static_assert (TS % 4 == 0 && H % 2 == 0 && H > 0, "tile of quads, even halo");
+  __shared__ __align__ (16) float sa[2*WM];
+  const int n = g.n, tx = threadIdx.x, ty = threadIdx.y, tid = ty*BX + tx;
+  const int p = 2*RW*(ty/(2*RW)) + 2*(ty % RW) + ((ty/RW) & 1);
+  const int i0 = blockIdx.y*TS - H, j0 = blockIdx.x*TS - H;
+  const int px = bc.periodic[0], py = bc.periodic[1];
+  const int base = (i0 + j0) & 1;
+  const bool inner = i0 >= 0 && i0 + W <= n && j0 >= 0 && j0 + W <= n;
+  const int q0 = 8*tx, m0 = 4*tx, gi = i0 + p;
+  const float D2 = Delta*Delta;
+
+  /* the weights of the thread's eight cells, once for all sweeps */
+  float r8[8], xl8[8], xu8[8], yl8[9], l8[8];
+  if (inner) {
+    const long long id = cidx<2> (g, gi, j0 + q0, 0);
+    const Quad<float> r0 = load_quad (res + id), r1 = load_quad (res + id + 4);
+    r8[0] = r0.x; r8[1] = r0.y; r8[2] = r0.z; r8[3] = r0.w;
+    r8[4] = r1.x; r8[5] = r1.y; r8[6] = r1.z; r8[7] = r1.w;
+    if (ax.p) {
+      const Quad<float> a0 = load_quad (ax.p + id), a1 = load_quad (ax.p + id + 4);
+      const Quad<float> b0 = load_quad (ax.p + id + g.P), b1 = load_quad (ax.p + id + g.P + 4);
+      xl8[0] = a0.x; xl8[1] = a0.y; xl8[2] = a0.z; xl8[3] = a0.w;
+      xl8[4] = a1.x; xl8[5] = a1.y; xl8[6] = a1.z; xl8[7] = a1.w;
+      xu8[0] = b0.x; xu8[1] = b0.y; xu8[2] = b0.z; xu8[3] = b0.w;
+      xu8[4] = b1.x; xu8[5] = b1.y; xu8[6] = b1.z; xu8[7] = b1.w;
+    }
+    else
+#pragma unroll
+      for (int q = 0; q < 8; q++) xl8[q] = xu8[q] = ax.c;
+    if (ay.p) {
+      const Quad<float> a0 = load_quad (ay.p + id), a1 = load_quad (ay.p + id + 4);
+      yl8[0] = a0.x; yl8[1] = a0.y; yl8[2] = a0.z; yl8[3] = a0.w;
+      yl8[4] = a1.x; yl8[5] = a1.y; yl8[6] = a1.z; yl8[7] = a1.w;
+      yl8[8] = ay.p[id + 8];
+    }
+    else
+#pragma unroll
+      for (int q = 0; q < 9; q++) yl8[q] = ay.c;
+    if (LAM) {
+      const Quad<float> a0 = load_quad (lam.p + id), a1 = load_quad (lam.p + id + 4);
+      l8[0] = a0.x; l8[1] = a0.y; l8[2] = a0.z; l8[3] = a0.w;
+      l8[4] = a1.x; l8[5] = a1.y; l8[6] = a1.z; l8[7] = a1.w;
+    }
+  }
+  else {
+    const int ri = real_index (gi, n, px);
+    const int flo = real_face (gi, n, px), fhi = real_face (gi + 1, n, px);
+#pragma unroll
+    for (int q = 0; q < 9; q++) {
+      const int rj = real_index (j0 + q0 + q, n, py), fj = real_face (j0 + q0 + q, n, py);
+      yl8[q] = ri >= 0 && fj >= 0 ? ay.at (cidx<2> (g, ri, fj, 0)) : 0.f;
+      if (q == 8) break;
+      const bool ok = ri >= 0 && rj >= 0;
+      r8[q] = ok ? res[cidx<2> (g, ri, rj, 0)] : 0.f;
+      xl8[q] = flo >= 0 && rj >= 0 ? ax.at (cidx<2> (g, flo, rj, 0)) : 0.f;
+      xu8[q] = fhi >= 0 && rj >= 0 ? ax.at (cidx<2> (g, fhi, rj, 0)) : 0.f;
+      if (LAM) l8[q] = ok ? lam.p[cidx<2> (g, ri, rj, 0)] : 0.f;
+    }
+  }
+  float wxl[2][4], wxu[2][4], wyl[2][4], wyr[2][4], be[2][4];
+  unsigned valid = 0;
+  const bool rowok = px || (unsigned) gi < (unsigned) n;
+#pragma unroll
+  for (int c = 0; c < 2; c++)
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+      const bool odd = (c ^ base ^ p) & 1;
+      const int q = 2*e + (odd ? 1 : 0);
+      const float xl = odd ? xl8[2*e + 1] : xl8[2*e], xu = odd ? xu8[2*e + 1] : xu8[2*e];
+      const float yl = odd ? yl8[2*e + 1] : yl8[2*e], yr = odd ? yl8[2*e + 2] : yl8[2*e + 1];
+      const float rv = odd ? r8[2*e + 1] : r8[2*e];
+      const float lv = LAM ? (odd ? l8[2*e + 1] : l8[2*e]) : lam.c;
+      const bool ok = rowok && (py || (unsigned) (j0 + q0 + q) < (unsigned) n);
+      float d = (-lv)*D2;
+      d += xu + xl;
+      d += yr + yl;
+      const float inv = ok ? __fdividef (1.f, d) : 0.f;
+      wxl[c][e] = xl*inv; wxu[c][e] = xu*inv;
+      wyl[c][e] = yl*inv; wyr[c][e] = yr*inv;
+      be[c][e] = ((-D2)*rv)*inv;
+      valid |= (ok ? 1u : 0u) << (4*c + e);
+    }
+
+  const int cq = (base + p) & 1;                /* colour of the even columns */
+  const int glo_i = px ? -1 : -1 - i0, ghi_i = px ? -1 : n - i0;
+  const int glo_j = py ? -1 : -1 - j0, ghi_j = py ? -1 : n - j0;
+  const bool has_ghosts = !inner &&
+    ((glo_i >= 0 && glo_i < W) || (ghi_i >= 0 && ghi_i < W) ||
+     (glo_j >= 0 && glo_j < W) || (ghi_j >= 0 && ghi_j < W));
+  auto refresh = [&] () {
+    for (int t = tid; t < 4*W; t += nth) {
+      const int line = t/W, u = t - line*W;
+      int pp, q, pm, qm, f;
+      if (line == 0) { pp = glo_i; q = u; pm = pp + 1; qm = q; f = bc.fac[1]; }
+      else if (line == 1) { pp = ghi_i; q = u; pm = pp - 1; qm = q; f = bc.fac[0]; }
+      else if (line == 2) { pp = u; q = glo_j; pm = pp; qm = q + 1; f = bc.fac[3]; }
+      else { pp = u; q = ghi_j; pm = pp; qm = q - 1; f = bc.fac[2]; }
+      if (pp < 0 || pp >= W || q < 0 || q >= W || pm < 0 || pm >= W || qm < 0 || qm >= W)
+        continue;
+      if (line < 2 ? real_index (j0 + q, n, py) < 0 : real_index (i0 + pp, n, px) < 0)
+        continue;
+      const int c = (base + pp + q) & 1;
+      sa[c*WM + pp*M + (q >> 1)] = sa[(c ^ 1)*WM + pm*M + (qm >> 1)]*float(f);
+    }
+  };
+  const unsigned sbase = (unsigned) __cvta_generic_to_shared (sa);
+  const int o0 = (base ^ p) & 1;
+  const int nblk = (nrelax + S - 1)/S;
+  const unsigned nctas = gridDim.x*gridDim.y;
+  const int ri = real_index (gi, n, px);
+
+  for (int blk = 0; blk < nblk; blk++) {
+    const int ks = nrelax - blk*S < S ? nrelax - blk*S : S;
+    if (blk == 0) {
+      /* the bilinear prolongation of the coarse level at the eight cells
+         (zero outside the domain; box ghosts are refreshed below) */
+#pragma unroll
+      for (int q = 0; q < 8; q++) {
+        const int rj = real_index (j0 + q0 + q, n, py);
+        float v = 0.f;
+        if (ri >= 0 && rj >= 0) {
+          const int ci = ri >> 1, cj = rj >> 1, cx = (ri & 1) ? 1 : -1, cy = (rj & 1) ? 1 : -1;
+          const float c00 = coarse[cidx<2> (gc, ci, cj, 0)];
+          const float c10 = coarse[cidx<2> (gc, ci + cx, cj, 0)];
+          const float c01 = coarse[cidx<2> (gc, ci, cj + cy, 0)];
+          const float c11 = coarse[cidx<2> (gc, ci + cx, cj + cy, 0)];
+          v = (9.f*c00 + 3.f*(c10 + c01) + c11)/16.f;
+        }
+        sa[((cq + q) & 1)*WM + p*M + ((q0 + q) >> 1)] = v;
+      }
+    }
+    else {
+      const float * src = (blk & 1) ? buf0 : buf1;
+      if (inner) {
+        const long long id = cidx<2> (g, gi, j0 + q0, 0);
+        const float4 a = __ldcg ((const float4 *) (src + id)), b = __ldcg ((const float4 *) (src + id + 4));
+        const Quad<float> va = {a.x, a.y, a.z, a.w}, vb = {b.x, b.y, b.z, b.w};
+        put_quad (sa + cq*WM, sa + (cq ^ 1)*WM, p*M + m0, va);
+        put_quad (sa + cq*WM, sa + (cq ^ 1)*WM, p*M + m0 + 2, vb);
+      }
+      else {
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+          const int rj = real_index (j0 + q0 + q, n, py);
+          sa[((cq + q) & 1)*WM + p*M + ((q0 + q) >> 1)] =
+            ri >= 0 && rj >= 0 ? __ldcg (src + cidx<2> (g, ri, rj, 0)) : 0.f;
+        }
+      }
+    }
+    __syncthreads ();
+    if (has_ghosts) {
+      refresh ();
+      __syncthreads ();
+    }
+    for (int sw = 0; sw < ks; sw++)
+#pragma unroll
+      for (int c = 0; c < 2; c++) {
+        const int k = 2*sw + c;
+        if (p >= k + 1 && p < W - k - 1) {
+          const int o = o0 ^ c;
+          const unsigned aup = sbase + 4u*((c ^ 1)*WM + (p - 1)*M + m0);
+          const float4 up = lds_f4<0> (aup), mid = lds_f4<4*M> (aup), dn = lds_f4<8*M> (aup);
+          float v[5];
+          if (o == 0) { v[0] = lds_f1<4*M - 4> (aup); v[1] = mid.x; v[2] = mid.y; v[3] = mid.z; v[4] = mid.w; }
+          else { v[0] = mid.x; v[1] = mid.y; v[2] = mid.z; v[3] = mid.w; v[4] = lds_f1<4*M + 16> (aup); }
+          const float upv[4] = {up.x, up.y, up.z, up.w}, dnv[4] = {dn.x, dn.y, dn.z, dn.w};
+          float nv[4];
+#pragma unroll
+          for (int e = 0; e < 4; e++)
+            nv[e] = fmaf (wyr[c][e], v[e + 1], fmaf (wyl[c][e], v[e],
+                    fmaf (wxu[c][e], dnv[e], fmaf (wxl[c][e], upv[e], be[c][e]))));
+          const unsigned aw = sbase + 4u*(c*WM + p*M + m0);
+          const unsigned vc = (valid >> (4*c)) & 15u;
+          if (vc == 15u)
+            sts_f4 (aw, make_float4 (nv[0], nv[1], nv[2], nv[3]));
+          else {
+            if (vc & 1u) sts_f1 (aw, nv[0]);
+            if (vc & 2u) sts_f1 (aw + 4, nv[1]);
+            if (vc & 4u) sts_f1 (aw + 8, nv[2]);
+            if (vc & 8u) sts_f1 (aw + 12, nv[3]);
+          }
+        }
+        __syncthreads ();
+        if (has_ghosts) {
+          refresh ();
+          __syncthreads ();
+        }
+      }
+    /* the tile interior, with its ghost images, into this block's buffer */
+    float * dst = (blk & 1) ? buf1 : buf0;
+    if (inner) {
+      constexpr int QT = TS/4;
+      for (int idx = tid; idx < TS*QT; idx += nth) {
+        const int rr = idx/QT, k = idx - rr*QT;
+        const int pp = rr + H, q = H + 4*k, c0 = (base + pp + q) & 1, m = q >> 1;
+        const float4 v = make_float4 (sa[c0*WM + pp*M + m], sa[(c0 ^ 1)*WM + pp*M + m],
+                                      sa[c0*WM + pp*M + m + 1], sa[(c0 ^ 1)*WM + pp*M + m + 1]);
+        __stcg ((float4 *) (dst + cidx<2> (g, blockIdx.y*TS + rr, blockIdx.x*TS + 4*k, 0)), v);
+      }
+    }
+    else
+      for (int idx = tid; idx < TS*TS; idx += nth) {
+        const int rr = idx/TS, s = idx - rr*TS;
+        const int oi = blockIdx.y*TS + rr, oj = blockIdx.x*TS + s;
+        if (oi >= n || oj >= n) continue;
+        const int pp = rr + H, q = s + H;
+        const float v = sa[((base + pp + q) & 1)*WM + pp*M + (q >> 1)];
+        dst[cidx<2> (g, oi, oj, 0)] = v;
+        ghosts_homog<2, float> (dst, g, oi, oj, 0, v, bc);
+      }
+    if (blk + 1 < nblk) grid_sync (sync, (unsigned) (blk + 1)*nctas);
+  }
+}
+
 /* FP64 shared-memory accesses by 32-bit byte address plus a constant
    offset */
 template <int OFF>
@@ -1568,6 +1855,44 @@ __global__ void __launch_bounds__ (BOT_THREADS, 1) k_bottom (const __grid_consta
     bot_copy_st<DIM> (P.lv[m].st, P.lv[m].g, P.lv[m].da, P.sm[m].gs, sm_at (bsm, P.sm[m].off_da), 0);
 }
 
+/* one cooperative launch of k_level_w; -1 when its CTAs cannot all be
+   resident at once on this device (the caller then uses tile launches) */
+template <int W, int TS, bool LAM>
+int launch_level_w (bmg_geom g, float * b0, float * b1, const float * res, const bmg_coef * alpha,
+                    bmg_coef lambda, double Delta, BCH h, int nrelax, bmg_geom gc,
+                    const float * coarse, unsigned * sync, cudaStream_t s)
+{
+  const dim3 grid ((g.n + TS - 1)/TS, (g.n + TS - 1)/TS, 1), block (W/8, W, 1);
+  static int resident[64];
+  int dev = 0;
+  cudaGetDevice (&dev);
+  if (dev < 0 || dev >= 64) return (int) cudaErrorInvalidDevice;
+  if (!resident[dev]) {
+    int nb = 0, sms = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor (&nb, k_level_w<W, TS, LAM>, W*W/8, 0);
+    if (e != cudaSuccess) return (int) e;
+    e = cudaDeviceGetAttribute (&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return (int) e;
+    resident[dev] = nb*sms > 0 ? nb*sms : -1;
+  }
+  if ((long long) grid.x*grid.y > resident[dev]) return -1;
+  cudaLaunchConfig_t cfg;
+  memset (&cfg, 0, sizeof cfg);
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeCooperative;
+  at[0].val.cooperative = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return (int) cudaLaunchKernelEx (&cfg, k_level_w<W, TS, LAM>, g, b0, b1, res,
+                                   coef_of<float> (alpha[0]), coef_of<float> (alpha[1]),
+                                   coef_of<float> (lambda), (float) Delta, h, nrelax, gc,
+                                   coarse, sync);
+}
+
 template <typename T, int TS, int S, bool LAM, int BX, int BY, int CPT, int MINB>
 int launch_tile_v (bmg_geom g, void * out, const void * in, const void * res,
                    const bmg_coef * alpha, bmg_coef lambda, double Delta, BCH h, int nsweeps,
@@ -1655,6 +1980,33 @@ int bmg_launch_relax_tile (int dim, int st, bmg_geom g, void * out, const void *
   if (e) return e;
   cudaError_t r = cudaGetLastError ();
   return r == cudaSuccess ? 0 : (int) r;
+}
+
+int bmg_level_persist_sweeps (int st, int n)
+{
+  if (st != BMG_ST_F32) return 0;
+  return n == 128 || n == 256 || n == 512 ? 4 : 0;
+}
+
+int bmg_launch_level_persist (bmg_geom g, void * buf0, void * buf1, const void * res,
+                              const bmg_coef * alpha, bmg_coef lambda, double Delta,
+                              const bmg_bcdesc * bc, int nrelax, bmg_geom gc, const void * coarse,
+                              unsigned * sync, cudaStream_t s)
+{
+  if (nrelax < 1 || !bmg_level_persist_sweeps (BMG_ST_F32, g.n)) return -1;
+  BCH h = bch_of (bc);
+  float * b0 = (float *) buf0, * b1 = (float *) buf1;
+  const float * r = (const float *) res, * c = (const float *) coarse;
+  int e;
+  if (g.n == 512)
+    e = lambda.p ? launch_level_w<64, 48, true> (g, b0, b1, r, alpha, lambda, Delta, h, nrelax, gc, c, sync, s)
+      : launch_level_w<64, 48, false> (g, b0, b1, r, alpha, lambda, Delta, h, nrelax, gc, c, sync, s);
+  else
+    e = lambda.p ? launch_level_w<32, 16, true> (g, b0, b1, r, alpha, lambda, Delta, h, nrelax, gc, c, sync, s)
+      : launch_level_w<32, 16, false> (g, b0, b1, r, alpha, lambda, Delta, h, nrelax, gc, c, sync, s);
+  if (e) return e;
+  cudaError_t q = cudaGetLastError ();
+  return q == cudaSuccess ? 0 : (int) q;
 }
 
 size_t bmg_bottom_smem (int dim, const bmg_bottom_level * lv, int nlev)

@@ -169,6 +169,9 @@ int bmg_grid_new (bmg_grid ** out, int dim, int depth)
   g->fields = calloc (g->cap, sizeof (field_t));
   g->nfields = 1;   /* handle 0 means "unset" */
   CK (cudaMalloc ((void **) &g->d_maxres, 2*sizeof (unsigned long long)));
+  CK (cudaMalloc ((void **) &g->d_sync, 2*sizeof (unsigned)));
+  CK (cudaMemset (g->d_sync, 0, 2*sizeof (unsigned)));
+  g->persist = getenv ("BMG_NO_PERSIST") == NULL;
   g->npartials = bmg_sum_partials (dim, g->g64[depth]);
   CK (cudaMalloc ((void **) &g->d_partials, (g->npartials + 1)*sizeof (double)));
   CK (cudaMalloc ((void **) &g->d_sum, 2*sizeof (double)));
@@ -202,7 +205,7 @@ void bmg_grid_free (bmg_grid * g)
   free (g->fields);
   cudaFree (g->ws64); cudaFree (g->ws32); cudaFree (g->bproj); cudaFree (g->visc_ws);
   cudaFree (g->stage);
-  cudaFree (g->d_maxres); cudaFree (g->d_partials); cudaFree (g->d_sum);
+  cudaFree (g->d_maxres); cudaFree (g->d_sync); cudaFree (g->d_partials); cudaFree (g->d_sum);
   cudaFreeHost (g->h_pinned);
   cudaEventDestroy (g->ev0); cudaEventDestroy (g->ev1);
   cudaEventDestroy (g->evr0); cudaEventDestroy (g->evr1);
@@ -835,6 +838,28 @@ static int cycle_launches (bmg_grid * g, field_t * a, const levels_t * lv, const
     const int st = lv->st[l];
     const bmg_geom gl = geom_st (g, l, st);
     cur[l] = lv->da[l]; oth[l] = lv->da2[l];
+    /* a middle level of the mixed form: prolongation and all nrelax sweeps
+       in one cooperative launch (falls through when it does not apply) */
+    const int ps = bmg_level_persist_sweeps (st, gl.n);
+    if (g->persist && ps && g->relax == BMG_RELAX_RBGS && dim == 2 && l > minlevel &&
+        lv->st[l - 1] == BMG_ST_F32 && !(g->timing && l == L && maxlevel == L)) {
+      const bmg_coef * al = c->alpha32[l];
+      CK (cudaMemsetAsync (g->d_sync, 0, sizeof (unsigned), s));
+      const int e = bmg_launch_level_persist (gl, lv->da[l], lv->da2[l], lv->res[l], al,
+                                              c->lambda32[l], delta_of (g, l), dabc, nrelax,
+                                              geom_st (g, l - 1, BMG_ST_F32), cur[l - 1],
+                                              g->d_sync, s);
+      if (e > 0) CL (e);
+      if (e == 0) {
+        const int nblk = (nrelax + ps - 1)/ps;
+        if (!(nblk & 1)) { cur[l] = lv->da2[l]; oth[l] = lv->da[l]; }
+        bytes += ncells (g, l - 1)*es_of (BMG_ST_F32) + ncells (g, l)*es_of (st);
+        bytes += nrelax*narr*ncells (g, l)*es_of (st);
+        sweeps += nrelax;
+        launches++;
+        continue;
+      }
+    }
     if (l == minlevel) {
       /* zero on the coarsest level (poisson.h:54-58) */
       CL (bmg_launch_prolong (dim, st, st, gl, gl, NULL, cur[l], dabc, 1, s));
@@ -954,6 +979,9 @@ static int run_cycle (bmg_grid * g, field_t * a, const double * bdata, const lev
       if (!r) r = residual_max (g, a, bdata, c, lv->res[L], lv->st[L], &dummy, 0, &victim->w);
       cudaError_t me = cudaMemcpyAsync (g->h_pinned, g->d_maxres, sizeof (double),
                                         cudaMemcpyDeviceToHost, g->stream);
+      if (me == cudaSuccess)
+        me = cudaMemcpyAsync (g->h_pinned + 3, g->d_sync + 1, sizeof (unsigned),
+                              cudaMemcpyDeviceToHost, g->stream);
       cudaError_t ee = cudaStreamEndCapture (g->stream, &graph);
       if (r) return r;
       CK (me);
@@ -979,6 +1007,8 @@ static int run_cycle (bmg_grid * g, field_t * a, const double * bdata, const lev
     if (r) return r;
     CK (cudaMemcpyAsync (g->h_pinned, g->d_maxres, sizeof (double), cudaMemcpyDeviceToHost,
                          g->stream));
+    CK (cudaMemcpyAsync (g->h_pinned + 3, g->d_sync + 1, sizeof (unsigned),
+                         cudaMemcpyDeviceToHost, g->stream));
   }
   g->counters.bytes += w.bytes;
   g->counters.launches += w.launches;
@@ -988,6 +1018,20 @@ static int run_cycle (bmg_grid * g, field_t * a, const double * bdata, const lev
     g->counters.relax_sweeps += w.relax_sweeps;
   }
   return BMG_OK;
+}
+
+/* the error flag of the persistent level kernels' grid barrier, as read
+   back after the last cycle (a wait that ran out: the sweeps of that cycle
+   are not valid) */
+static int barrier_status (bmg_grid * g)
+{
+  unsigned flag;
+  memcpy (&flag, g->h_pinned + 3, sizeof flag);
+  if (!flag) return BMG_OK;
+  fprintf (stderr, "bmg: a grid barrier of the persistent level kernel timed out\n");
+  cudaMemsetAsync (g->d_sync, 0, 2*sizeof (unsigned), g->stream);
+  memset (g->h_pinned + 3, 0, sizeof (double));
+  return fail (BMG_ECUDA);
 }
 
 static int is_singular (const bmg_grid * g, const field_t * a, const coefs_t * c)
@@ -1060,6 +1104,8 @@ static int solve (bmg_grid * g, field_t * a, field_t * b, coefs_t * c, int nrela
     if (g->timing) CK (cudaEventRecord (g->ev1, g->stream));
     CK (cudaStreamSynchronize (g->stream));
     s.resa = g->h_pinned[0];
+    r = barrier_status (g);
+    if (r) return r;
     g->counters.cycles++;
     if (g->timing) {
       float ms = 0.f, rms = 0.f;
