@@ -714,289 +714,343 @@ k_relax_tile2d_w (bmg_geom g, float * __restrict__ out, const float * __restrict
 }
 
 /* ---------------------------------------------------------------- */
-/* persistent level kernel: all nrelax sweeps of one FP32 level       */
+/* cluster level kernel: all nrelax sweeps of a middle FP32 level     */
 /* ---------------------------------------------------------------- */
 
-/* The middle levels of the mixed form's cycle (128^2 .. 512^2) are
-   latency-bound as launches of S sweeps: every launch loads the
-   coefficients of its tiles again, runs 2S colour passes and drains.  This
-   kernel does all nrelax sweeps of such a level in one cooperative launch:
-   each CTA owns one TS x TS tile for the whole launch, computes its staged
-   region's weights (as k_relax_tile2d_w) once, and then repeats blocks of
-   S sweeps -- stage the iterate of the W x W region from the partner
-   buffer, 2S colour passes in shared memory, the tile interior (and its
-   ghost images) back to global memory -- with a grid-wide barrier between
-   blocks, so that a block reads the tiles its neighbours wrote in the one
-   before.  The first block stages the bilinear prolongation of the coarse
-   level (multigrid-common.h:124-140, the expression of k_prolong2d_blk)
-   instead of an iterate, which fuses the level's prolongation in.  Blocks
-   alternate between the two buffers: block b writes buf[b & 1].
+/* The 128^2 and 256^2 levels of the mixed form's cycle are pure latency as
+   launches of four sweeps (about 7 us per launch for a few microseconds of
+   arithmetic).  This kernel relaxes such a level nrelax times in one launch
+   of one thread-block cluster of C CTAs, with the level held on chip for
+   the whole launch:
 
-   The grid barrier is a counter in global memory (zeroed before the
-   launch): thread 0 of each CTA adds one after a fence and waits for
-   (b + 1) x CTAs.  Its wait is bounded: after PERSIST_SPIN_LIMIT polls it
-   sets the error flag sync[1], which makes every later barrier return at
-   once, and the host turns the flag into an error status.  The launch is
-   cooperative, so all CTAs are resident together, and it triggers no
-   dependent launch, so no later kernel can take the slots of CTAs that are
-   not resident yet.  Iterate loads bypass L1 (ld.global.cg): the buffers
-   are written by other CTAs during the launch. */
-#define PERSIST_SPIN_LIMIT (1u << 20)
-
-__device__ __forceinline__ unsigned ld_acquire_u32 (const unsigned * p)
-{
-  unsigned v;
-  asm volatile ("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-  return v;
-}
-
-__device__ __forceinline__ void grid_sync (unsigned * sync, unsigned target)
-{
-  __syncthreads ();
-  if (threadIdx.x == 0 && threadIdx.y == 0) {
-    __threadfence ();
-    atomicAdd (sync, 1u);
-    if (!ld_acquire_u32 (sync + 1)) {
-      unsigned spins = 0;
-      while (ld_acquire_u32 (sync) < target) {
-        if (++spins > PERSIST_SPIN_LIMIT) { atomicExch (sync + 1, 1u); break; }
-        __nanosleep (64);
-      }
-    }
-    __threadfence ();
-  }
-  __syncthreads ();
-}
-
-namespace pw {
-/* W x W staged cells, BX x BY threads, each owning eight cells of one row;
-   the rows of a warp all have the same parity */
-template <int W> struct Shape {
-  static constexpr int M = W/2, WM = W*M, BX = W/8, BY = W, NT = BX*BY, RW = 32/BX;
-  static_assert (W % 8 == 0 && 32 % BX == 0 && BY % (2*RW) == 0, "rows of one parity per warp");
+     - CTA r owns R = N/C full rows [rR, rR + R) and stages them with H = 8
+       rows of halo on either side (R + 2H rows x N columns, colour-split
+       in shared memory as in k_relax_tile2d_w, with a ghost column on each
+       side);
+     - every thread owns eight consecutive cells of one staged row per
+       segment (SEG segments) and keeps their weights -- the coefficients
+       divided by the diagonal, computed once per launch -- in registers;
+     - a block of S = 4 sweeps stages the owned rows from the CTA's own
+       exchange buffer and the halo rows from its neighbours' exchange
+       buffers (distributed shared memory), runs 2S colour passes on the
+       staged rows (staleness moves in one row per pass and never reaches
+       the owned rows), writes the owned rows to its exchange buffer and
+       meets the cluster at one barrier.  Exchange buffers alternate, so a
+       block never overwrites what a neighbour may still be reading;
+     - the first block stages the bilinear prolongation of the coarse level
+       (multigrid-common.h:124-140, the expression of k_prolong2d_blk)
+       instead, which fuses the level's prolongation in;
+     - box ghost cells (rows -1 and N on the first and last CTA, columns -1
+       and N everywhere) and periodic ghost columns are written by the
+       thread that updates their mirror cell, right after the update: only
+       that cell reads them in a colour pass.  Periodic rows come from the
+       neighbour across the wrap.
+   The level's final iterate, with every ghost image, goes to out.  The
+   weights and the arithmetic of a cell update are those of
+   k_relax_tile2d_w (the relaxation of relax_value, poisson.h:303-319, up
+   to FP32 rounding).  Row and column indices: i along x (rows, sides
+   left/right), j along y (the contiguous axis, sides bottom/top). */
+namespace cl {
+template <int N, int C, int SEG> struct Shape {
+  static constexpr int R = N/C, H = 8, S = 4;
+  static constexpr int BYR = R + 2*H;             /* staged rows */
+  static constexpr int BX = N/(8*SEG);            /* threads per row */
+  static constexpr int NT = BX*BYR;
+  static constexpr int RW = 32/BX;                /* rows per warp */
+  static constexpr int OFS = 4;                   /* interior m = 0; ghost m = -1 at OFS - 1 */
+  static constexpr int MP = N/2 + 8;              /* colour row pitch (16-byte rows) */
+  static constexpr int SAW = BYR*MP, OWW = R*MP;  /* one colour of the staged / owned rows */
+  static constexpr size_t bytes = sizeof (float)*(2*SAW + 4*OWW);
+  static_assert (R >= H && 32 % BX == 0 && BYR % (2*RW) == 0 && NT <= 1024, "cluster level shape");
 };
 }
 
-template <int W, int TS, bool LAM>
-__global__ void __launch_bounds__ (W*W/8, W == 64 ? 1 : 4)
-k_level_w (bmg_geom g, float * buf0, float * buf1, const float * __restrict__ res,
-           Coef<float> ax, Coef<float> ay, Coef<float> lam, float Delta, BCH bc, int nrelax,
-           bmg_geom gc, const float * __restrict__ coarse, unsigned * sync)
+__device__ __forceinline__ void cluster_barrier ()
 {
-  typedef pw::Shape<W> Sh;
-  constexpr int M = Sh::M, WM = Sh::WM, BX = Sh::BX, RW = Sh::RW, nth = Sh::NT;
-  constexpr int H = (W - TS)/2, S = H/2;
-  static_assert (TS % 4 == 0 && H % 2 == 0 && H > 0, "tile of quads, even halo");
-  __shared__ __align__ (16) float sa[2*WM];
-  const int n = g.n, tx = threadIdx.x, ty = threadIdx.y, tid = ty*BX + tx;
+  asm volatile ("barrier.cluster.arrive.release.aligned;\n"
+                "barrier.cluster.wait.acquire.aligned;\n" ::: "memory");
+}
+
+__device__ __forceinline__ unsigned cluster_rank ()
+{
+  unsigned r;
+  asm volatile ("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+
+/* the generic address of the same shared-memory location in CTA rank */
+template <typename T>
+__device__ __forceinline__ T * cluster_map (T * p, unsigned rank)
+{
+  unsigned long long r;
+  asm volatile ("mapa.u64 %0, %1, %2;" : "=l"(r) : "l"(p), "r"(rank));
+  return (T *) r;
+}
+
+template <int N, int C, int SEG, bool LAM>
+__global__ void __launch_bounds__ (cl::Shape<N, C, SEG>::NT, 1)
+k_level_cluster (bmg_geom g, float * __restrict__ out, const float * __restrict__ res,
+                 Coef<float> ax, Coef<float> ay, Coef<float> lam, float Delta, BCH bc, int nrelax,
+                 bmg_geom gc, const float * __restrict__ coarse)
+{
+  typedef cl::Shape<N, C, SEG> Sh;
+  constexpr int R = Sh::R, H = Sh::H, S = Sh::S, BYR = Sh::BYR, BX = Sh::BX, RW = Sh::RW;
+  constexpr int OFS = Sh::OFS, MP = Sh::MP, SAW = Sh::SAW, OWW = Sh::OWW;
+  extern __shared__ __align__ (16) float csm[];
+  float * sa = csm;                       /* [2][BYR][MP] staged rows */
+  float * own = csm + 2*SAW;              /* [2 buffers][2][R][MP] owned rows */
+  const int tx = threadIdx.x, ty = threadIdx.y;
   const int p = 2*RW*(ty/(2*RW)) + 2*(ty % RW) + ((ty/RW) & 1);
-  const int i0 = blockIdx.y*TS - H, j0 = blockIdx.x*TS - H;
+  const int rank = (int) cluster_rank ();
   const int px = bc.periodic[0], py = bc.periodic[1];
-  const int base = (i0 + j0) & 1;
-  const bool inner = i0 >= 0 && i0 + W <= n && j0 >= 0 && j0 + W <= n;
-  const int q0 = 8*tx, m0 = 4*tx, gi = i0 + p;
+  const int gi = rank*R - H + p;          /* global row of staged row p */
+  const int ri = real_index (gi, N, px);  /* its real row, -1: none */
+  const bool rowok = ri >= 0;
+  const int ce = gi & 1;                  /* colour of the even columns */
   const float D2 = Delta*Delta;
+  pdl_trigger ();
 
-  /* the weights of the thread's eight cells, once for all sweeps */
-  float r8[8], xl8[8], xu8[8], yl8[9], l8[8];
-  if (inner) {
-    const long long id = cidx<2> (g, gi, j0 + q0, 0);
-    const Quad<float> r0 = load_quad (res + id), r1 = load_quad (res + id + 4);
-    r8[0] = r0.x; r8[1] = r0.y; r8[2] = r0.z; r8[3] = r0.w;
-    r8[4] = r1.x; r8[5] = r1.y; r8[6] = r1.z; r8[7] = r1.w;
-    if (ax.p) {
-      const Quad<float> a0 = load_quad (ax.p + id), a1 = load_quad (ax.p + id + 4);
-      const Quad<float> b0 = load_quad (ax.p + id + g.P), b1 = load_quad (ax.p + id + g.P + 4);
-      xl8[0] = a0.x; xl8[1] = a0.y; xl8[2] = a0.z; xl8[3] = a0.w;
-      xl8[4] = a1.x; xl8[5] = a1.y; xl8[6] = a1.z; xl8[7] = a1.w;
-      xu8[0] = b0.x; xu8[1] = b0.y; xu8[2] = b0.z; xu8[3] = b0.w;
-      xu8[4] = b1.x; xu8[5] = b1.y; xu8[6] = b1.z; xu8[7] = b1.w;
-    }
-    else
+  /* weights of the thread's cells: segment sg covers columns q0 .. q0 + 7,
+     q0 = 8 (tx + sg BX); colour c's cells are e = 0..3 at column
+     q0 + 2e + (c ^ ce) */
+  float wxl[SEG][2][4], wxu[SEG][2][4], wyl[SEG][2][4], wyr[SEG][2][4], be[SEG][2][4];
 #pragma unroll
-      for (int q = 0; q < 8; q++) xl8[q] = xu8[q] = ax.c;
-    if (ay.p) {
-      const Quad<float> a0 = load_quad (ay.p + id), a1 = load_quad (ay.p + id + 4);
-      yl8[0] = a0.x; yl8[1] = a0.y; yl8[2] = a0.z; yl8[3] = a0.w;
-      yl8[4] = a1.x; yl8[5] = a1.y; yl8[6] = a1.z; yl8[7] = a1.w;
-      yl8[8] = ay.p[id + 8];
-    }
-    else
+  for (int sg = 0; sg < SEG; sg++) {
+    const int q0 = 8*(tx + sg*BX);
+    float r8[8], xl8[8], xu8[8], yl8[9], l8[8];
 #pragma unroll
-      for (int q = 0; q < 9; q++) yl8[q] = ay.c;
-    if (LAM) {
-      const Quad<float> a0 = load_quad (lam.p + id), a1 = load_quad (lam.p + id + 4);
-      l8[0] = a0.x; l8[1] = a0.y; l8[2] = a0.z; l8[3] = a0.w;
-      l8[4] = a1.x; l8[5] = a1.y; l8[6] = a1.z; l8[7] = a1.w;
+    for (int q = 0; q < 8; q++) { r8[q] = xl8[q] = xu8[q] = yl8[q] = l8[q] = 0.f; }
+    yl8[8] = 0.f;
+    if (rowok) {
+      const int flo = real_face (gi, N, px), fhi = real_face (gi + 1, N, px);
+      const long long id = cidx<2> (g, ri, q0, 0);
+      const Quad<float> r0 = load_quad (res + id), r1 = load_quad (res + id + 4);
+      r8[0] = r0.x; r8[1] = r0.y; r8[2] = r0.z; r8[3] = r0.w;
+      r8[4] = r1.x; r8[5] = r1.y; r8[6] = r1.z; r8[7] = r1.w;
+      if (ax.p) {
+        const long long il = cidx<2> (g, flo, q0, 0), iu = cidx<2> (g, fhi, q0, 0);
+        const Quad<float> a0 = load_quad (ax.p + il), a1 = load_quad (ax.p + il + 4);
+        const Quad<float> b0 = load_quad (ax.p + iu), b1 = load_quad (ax.p + iu + 4);
+        xl8[0] = a0.x; xl8[1] = a0.y; xl8[2] = a0.z; xl8[3] = a0.w;
+        xl8[4] = a1.x; xl8[5] = a1.y; xl8[6] = a1.z; xl8[7] = a1.w;
+        xu8[0] = b0.x; xu8[1] = b0.y; xu8[2] = b0.z; xu8[3] = b0.w;
+        xu8[4] = b1.x; xu8[5] = b1.y; xu8[6] = b1.z; xu8[7] = b1.w;
+      }
+      else
+#pragma unroll
+        for (int q = 0; q < 8; q++) xl8[q] = xu8[q] = ax.c;
+      if (ay.p) {
+        const Quad<float> a0 = load_quad (ay.p + id), a1 = load_quad (ay.p + id + 4);
+        yl8[0] = a0.x; yl8[1] = a0.y; yl8[2] = a0.z; yl8[3] = a0.w;
+        yl8[4] = a1.x; yl8[5] = a1.y; yl8[6] = a1.z; yl8[7] = a1.w;
+        /* face q0 + 8: face N of a periodic direction is face 0 */
+        yl8[8] = ay.p[cidx<2> (g, ri, real_face (q0 + 8, N, py), 0)];
+      }
+      else
+#pragma unroll
+        for (int q = 0; q < 9; q++) yl8[q] = ay.c;
+      if (LAM) {
+        const Quad<float> a0 = load_quad (lam.p + id), a1 = load_quad (lam.p + id + 4);
+        l8[0] = a0.x; l8[1] = a0.y; l8[2] = a0.z; l8[3] = a0.w;
+        l8[4] = a1.x; l8[5] = a1.y; l8[6] = a1.z; l8[7] = a1.w;
+      }
     }
+#pragma unroll
+    for (int c = 0; c < 2; c++)
+#pragma unroll
+      for (int e = 0; e < 4; e++) {
+        const bool odd = (c ^ ce) & 1;
+        const float xl = odd ? xl8[2*e + 1] : xl8[2*e], xu = odd ? xu8[2*e + 1] : xu8[2*e];
+        const float yl = odd ? yl8[2*e + 1] : yl8[2*e], yr = odd ? yl8[2*e + 2] : yl8[2*e + 1];
+        const float rv = odd ? r8[2*e + 1] : r8[2*e];
+        const float lv = LAM ? (odd ? l8[2*e + 1] : l8[2*e]) : lam.c;
+        float d = (-lv)*D2;
+        d += xu + xl;
+        d += yr + yl;
+        const float inv = rowok ? __fdividef (1.f, d) : 0.f;
+        wxl[sg][c][e] = xl*inv; wxu[sg][c][e] = xu*inv;
+        wyl[sg][c][e] = yl*inv; wyr[sg][c][e] = yr*inv;
+        be[sg][c][e] = ((-D2)*rv)*inv;
+      }
   }
-  else {
-    const int ri = real_index (gi, n, px);
-    const int flo = real_face (gi, n, px), fhi = real_face (gi + 1, n, px);
-#pragma unroll
-    for (int q = 0; q < 9; q++) {
-      const int rj = real_index (j0 + q0 + q, n, py), fj = real_face (j0 + q0 + q, n, py);
-      yl8[q] = ri >= 0 && fj >= 0 ? ay.at (cidx<2> (g, ri, fj, 0)) : 0.f;
-      if (q == 8) break;
-      const bool ok = ri >= 0 && rj >= 0;
-      r8[q] = ok ? res[cidx<2> (g, ri, rj, 0)] : 0.f;
-      xl8[q] = flo >= 0 && rj >= 0 ? ax.at (cidx<2> (g, flo, rj, 0)) : 0.f;
-      xu8[q] = fhi >= 0 && rj >= 0 ? ax.at (cidx<2> (g, fhi, rj, 0)) : 0.f;
-      if (LAM) l8[q] = ok ? lam.p[cidx<2> (g, ri, rj, 0)] : 0.f;
-    }
-  }
-  float wxl[2][4], wxu[2][4], wyl[2][4], wyr[2][4], be[2][4];
-  unsigned valid = 0;
-  const bool rowok = px || (unsigned) gi < (unsigned) n;
-#pragma unroll
-  for (int c = 0; c < 2; c++)
-#pragma unroll
-    for (int e = 0; e < 4; e++) {
-      const bool odd = (c ^ base ^ p) & 1;
-      const int q = 2*e + (odd ? 1 : 0);
-      const float xl = odd ? xl8[2*e + 1] : xl8[2*e], xu = odd ? xu8[2*e + 1] : xu8[2*e];
-      const float yl = odd ? yl8[2*e + 1] : yl8[2*e], yr = odd ? yl8[2*e + 2] : yl8[2*e + 1];
-      const float rv = odd ? r8[2*e + 1] : r8[2*e];
-      const float lv = LAM ? (odd ? l8[2*e + 1] : l8[2*e]) : lam.c;
-      const bool ok = rowok && (py || (unsigned) (j0 + q0 + q) < (unsigned) n);
-      float d = (-lv)*D2;
-      d += xu + xl;
-      d += yr + yl;
-      const float inv = ok ? __fdividef (1.f, d) : 0.f;
-      wxl[c][e] = xl*inv; wxu[c][e] = xu*inv;
-      wyl[c][e] = yl*inv; wyr[c][e] = yr*inv;
-      be[c][e] = ((-D2)*rv)*inv;
-      valid |= (ok ? 1u : 0u) << (4*c + e);
-    }
 
-  const int cq = (base + p) & 1;                /* colour of the even columns */
-  const int glo_i = px ? -1 : -1 - i0, ghi_i = px ? -1 : n - i0;
-  const int glo_j = py ? -1 : -1 - j0, ghi_j = py ? -1 : n - j0;
-  const bool has_ghosts = !inner &&
-    ((glo_i >= 0 && glo_i < W) || (ghi_i >= 0 && ghi_i < W) ||
-     (glo_j >= 0 && glo_j < W) || (ghi_j >= 0 && ghi_j < W));
-  auto refresh = [&] () {
-    for (int t = tid; t < 4*W; t += nth) {
-      const int line = t/W, u = t - line*W;
-      int pp, q, pm, qm, f;
-      if (line == 0) { pp = glo_i; q = u; pm = pp + 1; qm = q; f = bc.fac[1]; }
-      else if (line == 1) { pp = ghi_i; q = u; pm = pp - 1; qm = q; f = bc.fac[0]; }
-      else if (line == 2) { pp = u; q = glo_j; pm = pp; qm = q + 1; f = bc.fac[3]; }
-      else { pp = u; q = ghi_j; pm = pp; qm = q - 1; f = bc.fac[2]; }
-      if (pp < 0 || pp >= W || q < 0 || q >= W || pm < 0 || pm >= W || qm < 0 || qm >= W)
-        continue;
-      if (line < 2 ? real_index (j0 + q, n, py) < 0 : real_index (i0 + pp, n, px) < 0)
-        continue;
-      const int c = (base + pp + q) & 1;
-      sa[c*WM + pp*M + (q >> 1)] = sa[(c ^ 1)*WM + pm*M + (qm >> 1)]*float(f);
+  /* ghost cells this thread writes after updating a cell: the box row
+     ghost of rows 0 and N - 1, the column ghost of columns 0 and N - 1
+     (box: the factor times the cell; periodic: the image across the wrap) */
+  /* (a staged row 0 or BYR - 1 is never updated and has no ghost row
+     inside the staged region: when R == H a neighbour's halo reaches the
+     domain's first or last row there) */
+  const bool rowghost_lo = !px && gi == 0 && p >= 1, rowghost_hi = !px && gi == N - 1 && p <= BYR - 2;
+  const float frow = rowghost_lo ? (float) bc.fac[1] : (float) bc.fac[0];
+  const float fbot = (float) bc.fac[3], ftop = (float) bc.fac[2];
+  const bool first_col = tx == 0, last_col = tx == BX - 1;
+  auto put_ghosts = [&] (int sg, int c, const float * nv) {
+    /* colour-c cells of segment sg in row p were just written (values nv) */
+    const int m0 = 4*(tx + sg*BX);
+    if (rowghost_lo || rowghost_hi) {
+      float * gr = sa + (c ^ 1)*SAW + (rowghost_lo ? p - 1 : p + 1)*MP + OFS + m0;
+#pragma unroll
+      for (int e = 0; e < 4; e++) gr[e] = nv[e]*frow;
+    }
+    const int o = c ^ ce;
+    if (sg == 0 && first_col && o == 0) {          /* cell j = 0 */
+      if (py) sa[c*SAW + p*MP + OFS + N/2] = nv[0];
+      else sa[(c ^ 1)*SAW + p*MP + OFS - 1] = nv[0]*fbot;
+    }
+    if (sg == SEG - 1 && last_col && o == 1) {     /* cell j = N - 1 */
+      if (py) sa[c*SAW + p*MP + OFS - 1] = nv[3];
+      else sa[(c ^ 1)*SAW + p*MP + OFS + N/2] = nv[3]*ftop;
     }
   };
+  /* the ghosts of a freshly staged row (both colours), from its cells */
+  auto stage_ghosts = [&] () {
+    if (!rowok) return;
+    const int c0 = ce;               /* colour of column 0 */
+    const int cl = ce ^ 1;           /* colour of column N - 1 */
+    if (first_col) {
+      const float v = sa[c0*SAW + p*MP + OFS];
+      if (py) sa[c0*SAW + p*MP + OFS + N/2] = v;
+      else sa[(c0 ^ 1)*SAW + p*MP + OFS - 1] = v*fbot;
+    }
+    if (last_col) {
+      const float v = sa[cl*SAW + p*MP + OFS + N/2 - 1];
+      if (py) sa[cl*SAW + p*MP + OFS - 1] = v;
+      else sa[(cl ^ 1)*SAW + p*MP + OFS + N/2] = v*ftop;
+    }
+    if (rowghost_lo || rowghost_hi) {
+      const int pg = rowghost_lo ? p - 1 : p + 1;
+#pragma unroll
+      for (int sg = 0; sg < SEG; sg++) {
+        const int m0 = 4*(tx + sg*BX);
+#pragma unroll
+        for (int c = 0; c < 2; c++)
+#pragma unroll
+          for (int e = 0; e < 4; e++)
+            sa[(c ^ 1)*SAW + pg*MP + OFS + m0 + e] = sa[c*SAW + p*MP + OFS + m0 + e]*frow;
+      }
+    }
+  };
+
   const unsigned sbase = (unsigned) __cvta_generic_to_shared (sa);
-  const int o0 = (base ^ p) & 1;
   const int nblk = (nrelax + S - 1)/S;
-  const unsigned nctas = gridDim.x*gridDim.y;
-  const int ri = real_index (gi, n, px);
+  /* neighbours across the rows, -1: none (a box side) */
+  const int up = rank > 0 ? rank - 1 : (px ? C - 1 : -1);
+  const int dn = rank < C - 1 ? rank + 1 : (px ? 0 : -1);
+  grid_dependency_wait ();
 
   for (int blk = 0; blk < nblk; blk++) {
     const int ks = nrelax - blk*S < S ? nrelax - blk*S : S;
     if (blk == 0) {
-      /* the bilinear prolongation of the coarse level at the eight cells
-         (zero outside the domain; box ghosts are refreshed below) */
+      /* the bilinear prolongation of the coarse level: the thread's eight
+         cells of a segment have six consecutive coarse parents (with
+         their neighbours) in each of two coarse rows */
 #pragma unroll
-      for (int q = 0; q < 8; q++) {
-        const int rj = real_index (j0 + q0 + q, n, py);
-        float v = 0.f;
-        if (ri >= 0 && rj >= 0) {
-          const int ci = ri >> 1, cj = rj >> 1, cx = (ri & 1) ? 1 : -1, cy = (rj & 1) ? 1 : -1;
-          const float c00 = coarse[cidx<2> (gc, ci, cj, 0)];
-          const float c10 = coarse[cidx<2> (gc, ci + cx, cj, 0)];
-          const float c01 = coarse[cidx<2> (gc, ci, cj + cy, 0)];
-          const float c11 = coarse[cidx<2> (gc, ci + cx, cj + cy, 0)];
-          v = (9.f*c00 + 3.f*(c10 + c01) + c11)/16.f;
+      for (int sg = 0; sg < SEG; sg++) {
+        const int q0 = 8*(tx + sg*BX), m0 = 4*(tx + sg*BX);
+        float v8[8];
+        if (rowok) {
+          const int ci = ri >> 1, cx = (ri & 1) ? 1 : -1, cj0 = (q0 >> 1) - 1;
+          const long long b0 = cidx<2> (gc, ci, cj0, 0), b1 = cidx<2> (gc, ci + cx, cj0, 0);
+          float r0[6], r1[6];
+#pragma unroll
+          for (int u = 0; u < 6; u++) { r0[u] = coarse[b0 + u]; r1[u] = coarse[b1 + u]; }
+#pragma unroll
+          for (int q = 0; q < 8; q++) {
+            const int u = 1 + (q >> 1), cy = (q & 1) ? 1 : -1;
+            v8[q] = (9.f*r0[u] + 3.f*(r1[u] + r0[u + cy]) + r1[u + cy])/16.f;
+          }
         }
-        sa[((cq + q) & 1)*WM + p*M + ((q0 + q) >> 1)] = v;
+        else
+#pragma unroll
+          for (int q = 0; q < 8; q++) v8[q] = 0.f;
+        /* even columns have colour ce */
+        *(float4 *) (sa + ce*SAW + p*MP + OFS + m0) = make_float4 (v8[0], v8[2], v8[4], v8[6]);
+        *(float4 *) (sa + (ce ^ 1)*SAW + p*MP + OFS + m0) = make_float4 (v8[1], v8[3], v8[5], v8[7]);
       }
     }
     else {
-      const float * src = (blk & 1) ? buf0 : buf1;
-      if (inner) {
-        const long long id = cidx<2> (g, gi, j0 + q0, 0);
-        const float4 a = __ldcg ((const float4 *) (src + id)), b = __ldcg ((const float4 *) (src + id + 4));
-        const Quad<float> va = {a.x, a.y, a.z, a.w}, vb = {b.x, b.y, b.z, b.w};
-        put_quad (sa + cq*WM, sa + (cq ^ 1)*WM, p*M + m0, va);
-        put_quad (sa + cq*WM, sa + (cq ^ 1)*WM, p*M + m0 + 2, vb);
-      }
-      else {
+      /* owned rows from this CTA's exchange buffer, halo rows from the
+         neighbours' (written in the previous block) */
+      const int src = (blk - 1) & 1;
+      int u = rank, r = p - H;
+      if (p < H) { u = up; r = R - H + p; }
+      else if (p >= H + R) { u = dn; r = p - H - R; }
+      const float * ob = own + src*2*OWW;
+      const float * q = u < 0 ? NULL : (u == rank ? ob : cluster_map (ob, (unsigned) u));
 #pragma unroll
-        for (int q = 0; q < 8; q++) {
-          const int rj = real_index (j0 + q0 + q, n, py);
-          sa[((cq + q) & 1)*WM + p*M + ((q0 + q) >> 1)] =
-            ri >= 0 && rj >= 0 ? __ldcg (src + cidx<2> (g, ri, rj, 0)) : 0.f;
+      for (int sg = 0; sg < SEG; sg++) {
+        const int m0 = 4*(tx + sg*BX);
+#pragma unroll
+        for (int c = 0; c < 2; c++) {
+          float4 v = make_float4 (0.f, 0.f, 0.f, 0.f);
+          if (q) v = *(const float4 *) (q + c*OWW + r*MP + OFS + m0);
+          *(float4 *) (sa + c*SAW + p*MP + OFS + m0) = v;
         }
       }
     }
     __syncthreads ();
-    if (has_ghosts) {
-      refresh ();
-      __syncthreads ();
-    }
+    stage_ghosts ();
+    __syncthreads ();
+
     for (int sw = 0; sw < ks; sw++)
 #pragma unroll
       for (int c = 0; c < 2; c++) {
         const int k = 2*sw + c;
-        if (p >= k + 1 && p < W - k - 1) {
-          const int o = o0 ^ c;
-          const unsigned aup = sbase + 4u*((c ^ 1)*WM + (p - 1)*M + m0);
-          const float4 up = lds_f4<0> (aup), mid = lds_f4<4*M> (aup), dn = lds_f4<8*M> (aup);
-          float v[5];
-          if (o == 0) { v[0] = lds_f1<4*M - 4> (aup); v[1] = mid.x; v[2] = mid.y; v[3] = mid.z; v[4] = mid.w; }
-          else { v[0] = mid.x; v[1] = mid.y; v[2] = mid.z; v[3] = mid.w; v[4] = lds_f1<4*M + 16> (aup); }
-          const float upv[4] = {up.x, up.y, up.z, up.w}, dnv[4] = {dn.x, dn.y, dn.z, dn.w};
-          float nv[4];
+        if (rowok && p >= k + 1 && p < BYR - k - 1) {
+          const int o = c ^ ce;
 #pragma unroll
-          for (int e = 0; e < 4; e++)
-            nv[e] = fmaf (wyr[c][e], v[e + 1], fmaf (wyl[c][e], v[e],
-                    fmaf (wxu[c][e], dnv[e], fmaf (wxl[c][e], upv[e], be[c][e]))));
-          const unsigned aw = sbase + 4u*(c*WM + p*M + m0);
-          const unsigned vc = (valid >> (4*c)) & 15u;
-          if (vc == 15u)
-            sts_f4 (aw, make_float4 (nv[0], nv[1], nv[2], nv[3]));
-          else {
-            if (vc & 1u) sts_f1 (aw, nv[0]);
-            if (vc & 2u) sts_f1 (aw + 4, nv[1]);
-            if (vc & 4u) sts_f1 (aw + 8, nv[2]);
-            if (vc & 8u) sts_f1 (aw + 12, nv[3]);
+          for (int sg = 0; sg < SEG; sg++) {
+            const int m0 = 4*(tx + sg*BX);
+            const unsigned aup = sbase + 4u*((c ^ 1)*SAW + (p - 1)*MP + OFS + m0);
+            const float4 upq = lds_f4<0> (aup), mid = lds_f4<4*MP> (aup), dnq = lds_f4<8*MP> (aup);
+            float v[5];
+            if (o == 0) { v[0] = lds_f1<4*MP - 4> (aup); v[1] = mid.x; v[2] = mid.y; v[3] = mid.z; v[4] = mid.w; }
+            else { v[0] = mid.x; v[1] = mid.y; v[2] = mid.z; v[3] = mid.w; v[4] = lds_f1<4*MP + 16> (aup); }
+            const float upv[4] = {upq.x, upq.y, upq.z, upq.w}, dnv[4] = {dnq.x, dnq.y, dnq.z, dnq.w};
+            float nv[4];
+#pragma unroll
+            for (int e = 0; e < 4; e++)
+              nv[e] = fmaf (wyr[sg][c][e], v[e + 1], fmaf (wyl[sg][c][e], v[e],
+                      fmaf (wxu[sg][c][e], dnv[e], fmaf (wxl[sg][c][e], upv[e], be[sg][c][e]))));
+            sts_f4 (sbase + 4u*(c*SAW + p*MP + OFS + m0), make_float4 (nv[0], nv[1], nv[2], nv[3]));
+            put_ghosts (sg, c, nv);
           }
         }
         __syncthreads ();
-        if (has_ghosts) {
-          refresh ();
-          __syncthreads ();
-        }
       }
-    /* the tile interior, with its ghost images, into this block's buffer */
-    float * dst = (blk & 1) ? buf1 : buf0;
-    if (inner) {
-      constexpr int QT = TS/4;
-      for (int idx = tid; idx < TS*QT; idx += nth) {
-        const int rr = idx/QT, k = idx - rr*QT;
-        const int pp = rr + H, q = H + 4*k, c0 = (base + pp + q) & 1, m = q >> 1;
-        const float4 v = make_float4 (sa[c0*WM + pp*M + m], sa[(c0 ^ 1)*WM + pp*M + m],
-                                      sa[c0*WM + pp*M + m + 1], sa[(c0 ^ 1)*WM + pp*M + m + 1]);
-        __stcg ((float4 *) (dst + cidx<2> (g, blockIdx.y*TS + rr, blockIdx.x*TS + 4*k, 0)), v);
+    /* the owned rows into this block's exchange buffer, then the cluster
+       barrier: the buffer is complete before any neighbour stages from it,
+       and every CTA has staged from the other buffer before it is reused */
+    if (p >= H && p < H + R) {
+      float * ob = own + (blk & 1)*2*OWW;
+#pragma unroll
+      for (int sg = 0; sg < SEG; sg++) {
+        const int m0 = 4*(tx + sg*BX);
+#pragma unroll
+        for (int c = 0; c < 2; c++)
+          *(float4 *) (ob + c*OWW + (p - H)*MP + OFS + m0) =
+            *(const float4 *) (sa + c*SAW + p*MP + OFS + m0);
       }
     }
-    else
-      for (int idx = tid; idx < TS*TS; idx += nth) {
-        const int rr = idx/TS, s = idx - rr*TS;
-        const int oi = blockIdx.y*TS + rr, oj = blockIdx.x*TS + s;
-        if (oi >= n || oj >= n) continue;
-        const int pp = rr + H, q = s + H;
-        const float v = sa[((base + pp + q) & 1)*WM + pp*M + (q >> 1)];
-        dst[cidx<2> (g, oi, oj, 0)] = v;
-        ghosts_homog<2, float> (dst, g, oi, oj, 0, v, bc);
-      }
-    if (blk + 1 < nblk) grid_sync (sync, (unsigned) (blk + 1)*nctas);
+    cluster_barrier ();
+  }
+
+  /* the owned rows, with every ghost image, to global memory */
+  if (p >= H && p < H + R) {
+#pragma unroll
+    for (int sg = 0; sg < SEG; sg++) {
+      const int q0 = 8*(tx + sg*BX), m0 = 4*(tx + sg*BX);
+      const float4 a = *(const float4 *) (sa + ce*SAW + p*MP + OFS + m0);
+      const float4 b = *(const float4 *) (sa + (ce ^ 1)*SAW + p*MP + OFS + m0);
+      const float v8[8] = {a.x, b.x, a.y, b.y, a.z, b.z, a.w, b.w};
+      float * o8 = out + cidx<2> (g, gi, q0, 0);
+      *(float4 *) o8 = make_float4 (v8[0], v8[1], v8[2], v8[3]);
+      *(float4 *) (o8 + 4) = make_float4 (v8[4], v8[5], v8[6], v8[7]);
+      if (gi == 0 || gi == N - 1 || q0 == 0 || q0 + 8 == N)
+#pragma unroll
+        for (int q = 0; q < 8; q++)
+          ghosts_homog<2, float> (out, g, gi, q0 + q, 0, v8[q], bc);
+    }
   }
 }
 
@@ -1855,42 +1909,46 @@ __global__ void __launch_bounds__ (BOT_THREADS, 1) k_bottom (const __grid_consta
     bot_copy_st<DIM> (P.lv[m].st, P.lv[m].g, P.lv[m].da, P.sm[m].gs, sm_at (bsm, P.sm[m].off_da), 0);
 }
 
-/* one cooperative launch of k_level_w; -1 when its CTAs cannot all be
-   resident at once on this device (the caller then uses tile launches) */
-template <int W, int TS, bool LAM>
-int launch_level_w (bmg_geom g, float * b0, float * b1, const float * res, const bmg_coef * alpha,
-                    bmg_coef lambda, double Delta, BCH h, int nrelax, bmg_geom gc,
-                    const float * coarse, unsigned * sync, cudaStream_t s)
+/* one launch of k_level_cluster (one cluster of C CTAs); -1 when this
+   device cannot schedule such a cluster (the caller then uses tile
+   launches) */
+template <int N, int C, int SEG, bool LAM>
+int launch_level_cluster (bmg_geom g, float * out, const float * res, const bmg_coef * alpha,
+                          bmg_coef lambda, double Delta, BCH h, int nrelax, bmg_geom gc,
+                          const float * coarse, cudaStream_t s)
 {
-  const dim3 grid ((g.n + TS - 1)/TS, (g.n + TS - 1)/TS, 1), block (W/8, W, 1);
-  static int resident[64];
+  typedef cl::Shape<N, C, SEG> Sh;
+  auto kern = k_level_cluster<N, C, SEG, LAM>;
+  static int ok[64];
   int dev = 0;
   cudaGetDevice (&dev);
   if (dev < 0 || dev >= 64) return (int) cudaErrorInvalidDevice;
-  if (!resident[dev]) {
-    int nb = 0, sms = 0;
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor (&nb, k_level_w<W, TS, LAM>, W*W/8, 0);
-    if (e != cudaSuccess) return (int) e;
-    e = cudaDeviceGetAttribute (&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (e != cudaSuccess) return (int) e;
-    resident[dev] = nb*sms > 0 ? nb*sms : -1;
-  }
-  if ((long long) grid.x*grid.y > resident[dev]) return -1;
   cudaLaunchConfig_t cfg;
   memset (&cfg, 0, sizeof cfg);
-  cfg.gridDim = grid;
-  cfg.blockDim = block;
-  cfg.dynamicSmemBytes = 0;
+  cfg.gridDim = dim3 (C, 1, 1);
+  cfg.blockDim = dim3 (Sh::BX, Sh::BYR, 1);
+  cfg.dynamicSmemBytes = Sh::bytes;
   cfg.stream = s;
-  cudaLaunchAttribute at[1];
-  at[0].id = cudaLaunchAttributeCooperative;
-  at[0].val.cooperative = 1;
+  cudaLaunchAttribute at[2];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = C; at[0].val.clusterDim.y = 1; at[0].val.clusterDim.z = 1;
+  at[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[1].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = at;
-  cfg.numAttrs = 1;
-  return (int) cudaLaunchKernelEx (&cfg, k_level_w<W, TS, LAM>, g, b0, b1, res,
-                                   coef_of<float> (alpha[0]), coef_of<float> (alpha[1]),
-                                   coef_of<float> (lambda), (float) Delta, h, nrelax, gc,
-                                   coarse, sync);
+  cfg.numAttrs = 2;
+  if (!ok[dev]) {
+    cudaError_t e = cudaFuncSetAttribute (kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) Sh::bytes);
+    if (e == cudaSuccess && C > 8)
+      e = cudaFuncSetAttribute (kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    int nc = 0;
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveClusters (&nc, kern, &cfg);
+    cudaGetLastError ();
+    ok[dev] = e == cudaSuccess && nc >= 1 ? 1 : -1;
+  }
+  if (ok[dev] < 0) return -1;
+  return (int) cudaLaunchKernelEx (&cfg, kern, g, out, res, coef_of<float> (alpha[0]),
+                                   coef_of<float> (alpha[1]), coef_of<float> (lambda),
+                                   (float) Delta, h, nrelax, gc, coarse);
 }
 
 template <typename T, int TS, int S, bool LAM, int BX, int BY, int CPT, int MINB>
@@ -1982,28 +2040,29 @@ int bmg_launch_relax_tile (int dim, int st, bmg_geom g, void * out, const void *
   return r == cudaSuccess ? 0 : (int) r;
 }
 
-int bmg_level_persist_sweeps (int st, int n)
+int bmg_level_cluster_ok (int st, int n)
 {
-  if (st != BMG_ST_F32) return 0;
-  return n == 128 || n == 256 || n == 512 ? 4 : 0;
+  return st == BMG_ST_F32 && (n == 64 || n == 128 || n == 256);
 }
 
-int bmg_launch_level_persist (bmg_geom g, void * buf0, void * buf1, const void * res,
-                              const bmg_coef * alpha, bmg_coef lambda, double Delta,
-                              const bmg_bcdesc * bc, int nrelax, bmg_geom gc, const void * coarse,
-                              unsigned * sync, cudaStream_t s)
+int bmg_launch_level_cluster (bmg_geom g, void * out, const void * res, const bmg_coef * alpha,
+                              bmg_coef lambda, double Delta, const bmg_bcdesc * bc, int nrelax,
+                              bmg_geom gc, const void * coarse, cudaStream_t s)
 {
-  if (nrelax < 1 || !bmg_level_persist_sweeps (BMG_ST_F32, g.n)) return -1;
+  if (nrelax < 1 || !bmg_level_cluster_ok (BMG_ST_F32, g.n)) return -1;
   BCH h = bch_of (bc);
-  float * b0 = (float *) buf0, * b1 = (float *) buf1;
+  float * o = (float *) out;
   const float * r = (const float *) res, * c = (const float *) coarse;
   int e;
-  if (g.n == 512)
-    e = lambda.p ? launch_level_w<64, 48, true> (g, b0, b1, r, alpha, lambda, Delta, h, nrelax, gc, c, sync, s)
-      : launch_level_w<64, 48, false> (g, b0, b1, r, alpha, lambda, Delta, h, nrelax, gc, c, sync, s);
+  if (g.n == 256)
+    e = lambda.p ? launch_level_cluster<256, 16, 2, true> (g, o, r, alpha, lambda, Delta, h, nrelax, gc, c, s)
+      : launch_level_cluster<256, 16, 2, false> (g, o, r, alpha, lambda, Delta, h, nrelax, gc, c, s);
+  else if (g.n == 128)
+    e = lambda.p ? launch_level_cluster<128, 16, 1, true> (g, o, r, alpha, lambda, Delta, h, nrelax, gc, c, s)
+      : launch_level_cluster<128, 16, 1, false> (g, o, r, alpha, lambda, Delta, h, nrelax, gc, c, s);
   else
-    e = lambda.p ? launch_level_w<32, 16, true> (g, b0, b1, r, alpha, lambda, Delta, h, nrelax, gc, c, sync, s)
-      : launch_level_w<32, 16, false> (g, b0, b1, r, alpha, lambda, Delta, h, nrelax, gc, c, sync, s);
+    e = lambda.p ? launch_level_cluster<64, 8, 1, true> (g, o, r, alpha, lambda, Delta, h, nrelax, gc, c, s)
+      : launch_level_cluster<64, 8, 1, false> (g, o, r, alpha, lambda, Delta, h, nrelax, gc, c, s);
   if (e) return e;
   cudaError_t q = cudaGetLastError ();
   return q == cudaSuccess ? 0 : (int) q;

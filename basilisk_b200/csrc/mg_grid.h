@@ -48,8 +48,8 @@ struct bmg_grid {
   float * ws32;         /* da, da2, res, alpha x/y/z, lambda: FP32 levels */
   double * bproj;       /* zero-mean copy of b (mixed form, singular problems) */
   unsigned long long * d_maxres;
-  unsigned * d_sync;    /* persistent level kernels: barrier counter, error flag */
-  int persist;          /* use them (BMG_NO_PERSIST unset in the environment) */
+  int cluster_levels;   /* cluster kernels for the middle levels of the mixed form
+                           (on unless BMG_NO_CLUSTER is set in the environment) */
   double * d_sum, * d_partials;
   int npartials;
   double * h_pinned;

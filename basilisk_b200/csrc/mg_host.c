@@ -169,9 +169,7 @@ int bmg_grid_new (bmg_grid ** out, int dim, int depth)
   g->fields = calloc (g->cap, sizeof (field_t));
   g->nfields = 1;   /* handle 0 means "unset" */
   CK (cudaMalloc ((void **) &g->d_maxres, 2*sizeof (unsigned long long)));
-  CK (cudaMalloc ((void **) &g->d_sync, 2*sizeof (unsigned)));
-  CK (cudaMemset (g->d_sync, 0, 2*sizeof (unsigned)));
-  g->persist = getenv ("BMG_NO_PERSIST") == NULL;
+  g->cluster_levels = getenv ("BMG_NO_CLUSTER") == NULL;
   g->npartials = bmg_sum_partials (dim, g->g64[depth]);
   CK (cudaMalloc ((void **) &g->d_partials, (g->npartials + 1)*sizeof (double)));
   CK (cudaMalloc ((void **) &g->d_sum, 2*sizeof (double)));
@@ -205,7 +203,7 @@ void bmg_grid_free (bmg_grid * g)
   free (g->fields);
   cudaFree (g->ws64); cudaFree (g->ws32); cudaFree (g->bproj); cudaFree (g->visc_ws);
   cudaFree (g->stage);
-  cudaFree (g->d_maxres); cudaFree (g->d_sync); cudaFree (g->d_partials); cudaFree (g->d_sum);
+  cudaFree (g->d_maxres); cudaFree (g->d_partials); cudaFree (g->d_sum);
   cudaFreeHost (g->h_pinned);
   cudaEventDestroy (g->ev0); cudaEventDestroy (g->ev1);
   cudaEventDestroy (g->evr0); cudaEventDestroy (g->evr1);
@@ -761,12 +759,17 @@ static cudaError_t record_event (cudaEvent_t e, cudaStream_t s)
 /* the levels of the single-CTA bottom solve: minlevel up to the largest
    level with at most BMG_BOTTOM_CELLS cells whose staged arrays fit the
    bottom kernel's shared memory; fills bl[0..top-minlevel] */
+static int use_cluster (const bmg_grid * g, const levels_t * lv, int l, int minlevel, int maxlevel);
+
 static int bottom_top (const bmg_grid * g, const levels_t * lv, const coefs_t * c,
                        int minlevel, int maxlevel, bmg_bottom_level * bl)
 {
   int top = minlevel - 1;
   for (int l = minlevel; l <= maxlevel; l++) {
     if (l > minlevel && ncells (g, l) > BMG_BOTTOM_CELLS) break;
+    /* a level that has a cluster kernel is relaxed by it, not by the
+       single CTA */
+    if (use_cluster (g, lv, l, minlevel, maxlevel)) break;
     bmg_bottom_level * b = &bl[l - minlevel];
     memset (b, 0, sizeof *b);
     b->st = lv->st[l];
@@ -782,6 +785,18 @@ static int bottom_top (const bmg_grid * g, const levels_t * lv, const coefs_t * 
     top = l;
   }
   return top < minlevel ? minlevel : top;
+}
+
+/* whether level l of a cycle is relaxed by the cluster level kernel: a
+   128^2 or 256^2 (or, below the tile levels, 64^2) FP32 level of the mixed
+   form's red-black cycle above minlevel, whose coarse level is FP32 too;
+   not the finest level while its sweeps are being timed */
+static int use_cluster (const bmg_grid * g, const levels_t * lv, int l, int minlevel, int maxlevel)
+{
+  return g->cluster_levels && g->relax == BMG_RELAX_RBGS && g->dim == 2 && l > minlevel &&
+    lv->st[l] == BMG_ST_F32 && lv->st[l - 1] == BMG_ST_F32 &&
+    bmg_level_cluster_ok (BMG_ST_F32, 1 << l) &&
+    !(g->timing && l == g->depth && maxlevel == g->depth);
 }
 
 /* the launches of one mg_cycle (poisson.h:32-90).  Each level's final
@@ -839,20 +854,13 @@ static int cycle_launches (bmg_grid * g, field_t * a, const levels_t * lv, const
     const bmg_geom gl = geom_st (g, l, st);
     cur[l] = lv->da[l]; oth[l] = lv->da2[l];
     /* a middle level of the mixed form: prolongation and all nrelax sweeps
-       in one cooperative launch (falls through when it does not apply) */
-    const int ps = bmg_level_persist_sweeps (st, gl.n);
-    if (g->persist && ps && g->relax == BMG_RELAX_RBGS && dim == 2 && l > minlevel &&
-        lv->st[l - 1] == BMG_ST_F32 && !(g->timing && l == L && maxlevel == L)) {
-      const bmg_coef * al = c->alpha32[l];
-      CK (cudaMemsetAsync (g->d_sync, 0, sizeof (unsigned), s));
-      const int e = bmg_launch_level_persist (gl, lv->da[l], lv->da2[l], lv->res[l], al,
+       in one thread-block cluster (falls through when it does not apply) */
+    if (use_cluster (g, lv, l, minlevel, maxlevel)) {
+      const int e = bmg_launch_level_cluster (gl, lv->da[l], lv->res[l], c->alpha32[l],
                                               c->lambda32[l], delta_of (g, l), dabc, nrelax,
-                                              geom_st (g, l - 1, BMG_ST_F32), cur[l - 1],
-                                              g->d_sync, s);
+                                              geom_st (g, l - 1, BMG_ST_F32), cur[l - 1], s);
       if (e > 0) CL (e);
       if (e == 0) {
-        const int nblk = (nrelax + ps - 1)/ps;
-        if (!(nblk & 1)) { cur[l] = lv->da2[l]; oth[l] = lv->da[l]; }
         bytes += ncells (g, l - 1)*es_of (BMG_ST_F32) + ncells (g, l)*es_of (st);
         bytes += nrelax*narr*ncells (g, l)*es_of (st);
         sweeps += nrelax;
@@ -979,9 +987,7 @@ static int run_cycle (bmg_grid * g, field_t * a, const double * bdata, const lev
       if (!r) r = residual_max (g, a, bdata, c, lv->res[L], lv->st[L], &dummy, 0, &victim->w);
       cudaError_t me = cudaMemcpyAsync (g->h_pinned, g->d_maxres, sizeof (double),
                                         cudaMemcpyDeviceToHost, g->stream);
-      if (me == cudaSuccess)
-        me = cudaMemcpyAsync (g->h_pinned + 3, g->d_sync + 1, sizeof (unsigned),
-                              cudaMemcpyDeviceToHost, g->stream);
+
       cudaError_t ee = cudaStreamEndCapture (g->stream, &graph);
       if (r) return r;
       CK (me);
@@ -1007,8 +1013,6 @@ static int run_cycle (bmg_grid * g, field_t * a, const double * bdata, const lev
     if (r) return r;
     CK (cudaMemcpyAsync (g->h_pinned, g->d_maxres, sizeof (double), cudaMemcpyDeviceToHost,
                          g->stream));
-    CK (cudaMemcpyAsync (g->h_pinned + 3, g->d_sync + 1, sizeof (unsigned),
-                         cudaMemcpyDeviceToHost, g->stream));
   }
   g->counters.bytes += w.bytes;
   g->counters.launches += w.launches;
@@ -1018,20 +1022,6 @@ static int run_cycle (bmg_grid * g, field_t * a, const double * bdata, const lev
     g->counters.relax_sweeps += w.relax_sweeps;
   }
   return BMG_OK;
-}
-
-/* the error flag of the persistent level kernels' grid barrier, as read
-   back after the last cycle (a wait that ran out: the sweeps of that cycle
-   are not valid) */
-static int barrier_status (bmg_grid * g)
-{
-  unsigned flag;
-  memcpy (&flag, g->h_pinned + 3, sizeof flag);
-  if (!flag) return BMG_OK;
-  fprintf (stderr, "bmg: a grid barrier of the persistent level kernel timed out\n");
-  cudaMemsetAsync (g->d_sync, 0, 2*sizeof (unsigned), g->stream);
-  memset (g->h_pinned + 3, 0, sizeof (double));
-  return fail (BMG_ECUDA);
 }
 
 static int is_singular (const bmg_grid * g, const field_t * a, const coefs_t * c)
@@ -1104,8 +1094,6 @@ static int solve (bmg_grid * g, field_t * a, field_t * b, coefs_t * c, int nrela
     if (g->timing) CK (cudaEventRecord (g->ev1, g->stream));
     CK (cudaStreamSynchronize (g->stream));
     s.resa = g->h_pinned[0];
-    r = barrier_status (g);
-    if (r) return r;
     g->counters.cycles++;
     if (g->timing) {
       float ms = 0.f, rms = 0.f;

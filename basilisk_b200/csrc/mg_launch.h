@@ -118,21 +118,16 @@ int bmg_launch_relax_tile (int dim, int st, bmg_geom g, void * out, const void *
                            const void * res, const bmg_coef * alpha, bmg_coef lambda,
                            double Delta, const bmg_bcdesc * bc, int nsweeps, cudaStream_t s);
 
-/* all nrelax red-black sweeps of one FP32 2D level in one cooperative
-   launch, the bilinear prolongation of coarse (FP32, the level below)
-   fused into the first block of sweeps: bmg_level_persist_sweeps () is the
-   number of sweeps per block (0: no such kernel for this level).  Block b
-   writes buf0 (b even) or buf1 (b odd), so the final iterate is in buf0
-   when ceil (nrelax/sweeps) is odd.  sync: two unsigned ints in device
-   memory, sync[0] zeroed before every launch (the grid barrier's
-   counter), sync[1] an error flag set when a barrier wait ran out.
-   Returns 0, -1 when the level's CTAs cannot all be resident at once (use
-   tile launches), or a CUDA error. */
-int bmg_level_persist_sweeps (int st, int n);
-int bmg_launch_level_persist (bmg_geom g, void * buf0, void * buf1, const void * res,
-                              const bmg_coef * alpha, bmg_coef lambda, double Delta,
-                              const bmg_bcdesc * bc, int nrelax, bmg_geom gc, const void * coarse,
-                              unsigned * sync, cudaStream_t s);
+/* all nrelax red-black sweeps of a 128^2 or 256^2 FP32 2D level in one
+   launch of one thread-block cluster, the bilinear prolongation of coarse
+   (FP32, the level below, ghosts included) fused in; the final iterate,
+   with its ghost images, goes to out.  bmg_level_cluster_ok () tells
+   whether a level has such a kernel.  Returns 0, -1 when the device cannot
+   schedule the cluster (use tile launches), or a CUDA error. */
+int bmg_level_cluster_ok (int st, int n);
+int bmg_launch_level_cluster (bmg_geom g, void * out, const void * res, const bmg_coef * alpha,
+                              bmg_coef lambda, double Delta, const bmg_bcdesc * bc, int nrelax,
+                              bmg_geom gc, const void * coarse, cudaStream_t s);
 
 /* one level of the single-CTA bottom solve */
 typedef struct {
