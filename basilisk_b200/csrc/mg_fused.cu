@@ -38,6 +38,7 @@
  */
 #include <cuda_runtime.h>
 #include <stdio.h>
+#include <stdlib.h>
 #include <string.h>
 #include "mg_device.cuh"
 
@@ -1082,132 +1083,122 @@ __device__ __forceinline__ void sts_d1 (unsigned a, double v)
   asm volatile ("st.shared.f64 [%0], %1;" :: "r"(a), "d"(v) : "memory");
 }
 
-/* The plain FP64 form of k_relax_tile2d_w: the same ownership of cells (the
-   thread's eight cells of one row for the whole launch, only the iterate
-   staged, 32 KB), with the coefficients kept exactly in registers and every
-   update in relax_value's expression and order with the IEEE division, so
-   that the result is bit-identical to the reference's red-black sequence
-   (and to k_relax_tile2d). */
+/* The plain FP64 form of k_relax_tile2d_w on large levels: the same
+   temporal blocking (48^2 tiles staged with an 8-cell halo, only the
+   iterate in shared memory, 32 KB), with four cells per thread (two of
+   each colour, 16 x 64 threads) whose exact coefficients and -Delta^2 b
+   stay in registers for the launch, and every update in relax_value's
+   expression and order with the IEEE division, so that the result is
+   bit-identical to the reference's red-black sequence (and to
+   k_relax_tile2d).  Four cells per thread keep the coefficients within 64
+   registers, so an SM holds 32 warps to cover the latency of the dependent
+   FP64 chains (eight cells per thread at 128 registers held 16 and were
+   14 % slower per launch). */
+namespace tx4 {
+constexpr int W = 64, M = W/2, WM = W*M, BX = 16, BY = 64;
+static_assert (W == 4*BX && BY == W, "one row of four cells per thread");
+}
+
 template <int TS, bool LAM>
-__global__ void __launch_bounds__ (tw::BX*tw::BY, 1)
-k_relax_tile2d_x (bmg_geom g, double * __restrict__ out, const double * __restrict__ in,
-                  const double * __restrict__ res, Coef<double> ax, Coef<double> ay, Coef<double> lam,
-                  double Delta, BCH bc, int nsweeps)
+__global__ void __launch_bounds__ (tx4::BX*tx4::BY, 1)
+k_relax_tile2d_x4 (bmg_geom g, double * __restrict__ out, const double * __restrict__ in,
+                   const double * __restrict__ res, Coef<double> ax, Coef<double> ay, Coef<double> lam,
+                   double Delta, BCH bc, int nsweeps)
 {
-  using namespace tw;
-  constexpr int H = Tile<TS>::H;
-  __shared__ __align__ (16) double sa[2*WM];     /* colour c of staged cell (p, q) at c*WM + p*M + q/2 */
+  using namespace tx4;
+  constexpr int H = (W - TS)/2;
+  __shared__ __align__ (16) double sa[2*WM];
   const int n = g.n, tx = threadIdx.x, ty = threadIdx.y, tid = ty*BX + tx, nth = BX*BY;
-  constexpr int RW = 32/BX;                     /* rows per warp, all of one parity */
+  constexpr int RW = 32/BX;
   const int p = 2*RW*(ty/(2*RW)) + 2*(ty % RW) + ((ty/RW) & 1);
   const int i0 = blockIdx.y*TS - H, j0 = blockIdx.x*TS - H;
   const int px = bc.periodic[0], py = bc.periodic[1];
   const int base = (i0 + j0) & 1;
   const bool inner = i0 >= 0 && i0 + W <= n && j0 >= 0 && j0 + W <= n;
-  const int q0 = 8*tx, m0 = 4*tx, gi = i0 + p;
+  const int q0 = 4*tx, m0 = 2*tx, gi = i0 + p;
   const double D2 = Delta*Delta;
   grid_dependents_launch ();
 
-  /* the coefficients of the thread's eight columns q0 .. q0 + 7 of row p
-     (x faces below and above, y faces left of each column and right of the
-     last), res and lambda */
-  double r8[8], xl8[8], xu8[8], yl8[9], l8[8];
+  double r4[4], xl4[4], xu4[4], yl4[5], l4[4];
   if (inner) {
     const long long id = cidx<2> (g, gi, j0 + q0, 0);
-    const Quad<double> r0 = load_quad (res + id), r1 = load_quad (res + id + 4);
-    r8[0] = r0.x; r8[1] = r0.y; r8[2] = r0.z; r8[3] = r0.w;
-    r8[4] = r1.x; r8[5] = r1.y; r8[6] = r1.z; r8[7] = r1.w;
+    const Quad<double> r0 = load_quad (res + id);
+    r4[0] = r0.x; r4[1] = r0.y; r4[2] = r0.z; r4[3] = r0.w;
     if (ax.p) {
-      const Quad<double> a0 = load_quad (ax.p + id), a1 = load_quad (ax.p + id + 4);
-      const Quad<double> b0 = load_quad (ax.p + id + g.P), b1 = load_quad (ax.p + id + g.P + 4);
-      xl8[0] = a0.x; xl8[1] = a0.y; xl8[2] = a0.z; xl8[3] = a0.w;
-      xl8[4] = a1.x; xl8[5] = a1.y; xl8[6] = a1.z; xl8[7] = a1.w;
-      xu8[0] = b0.x; xu8[1] = b0.y; xu8[2] = b0.z; xu8[3] = b0.w;
-      xu8[4] = b1.x; xu8[5] = b1.y; xu8[6] = b1.z; xu8[7] = b1.w;
+      const Quad<double> a0 = load_quad (ax.p + id), b0 = load_quad (ax.p + id + g.P);
+      xl4[0] = a0.x; xl4[1] = a0.y; xl4[2] = a0.z; xl4[3] = a0.w;
+      xu4[0] = b0.x; xu4[1] = b0.y; xu4[2] = b0.z; xu4[3] = b0.w;
     }
     else
 #pragma unroll
-      for (int q = 0; q < 8; q++) xl8[q] = xu8[q] = ax.c;
+      for (int q = 0; q < 4; q++) xl4[q] = xu4[q] = ax.c;
     if (ay.p) {
-      const Quad<double> a0 = load_quad (ay.p + id), a1 = load_quad (ay.p + id + 4);
-      yl8[0] = a0.x; yl8[1] = a0.y; yl8[2] = a0.z; yl8[3] = a0.w;
-      yl8[4] = a1.x; yl8[5] = a1.y; yl8[6] = a1.z; yl8[7] = a1.w;
-      yl8[8] = ay.p[id + 8];
+      const Quad<double> a0 = load_quad (ay.p + id);
+      yl4[0] = a0.x; yl4[1] = a0.y; yl4[2] = a0.z; yl4[3] = a0.w;
+      yl4[4] = ay.p[id + 4];
     }
     else
 #pragma unroll
-      for (int q = 0; q < 9; q++) yl8[q] = ay.c;
+      for (int q = 0; q < 5; q++) yl4[q] = ay.c;
     if (LAM) {
-      const Quad<double> a0 = load_quad (lam.p + id), a1 = load_quad (lam.p + id + 4);
-      l8[0] = a0.x; l8[1] = a0.y; l8[2] = a0.z; l8[3] = a0.w;
-      l8[4] = a1.x; l8[5] = a1.y; l8[6] = a1.z; l8[7] = a1.w;
+      const Quad<double> a0 = load_quad (lam.p + id);
+      l4[0] = a0.x; l4[1] = a0.y; l4[2] = a0.z; l4[3] = a0.w;
     }
   }
   else {
-    /* outside the domain: zero, or the periodic image */
     const int ri = real_index (gi, n, px);
     const int flo = real_face (gi, n, px), fhi = real_face (gi + 1, n, px);
 #pragma unroll
-    for (int q = 0; q < 9; q++) {
+    for (int q = 0; q < 5; q++) {
       const int rj = real_index (j0 + q0 + q, n, py), fj = real_face (j0 + q0 + q, n, py);
-      yl8[q] = ri >= 0 && fj >= 0 ? ay.at (cidx<2> (g, ri, fj, 0)) : 0.;
-      if (q == 8) break;
+      yl4[q] = ri >= 0 && fj >= 0 ? ay.at (cidx<2> (g, ri, fj, 0)) : 0.;
+      if (q == 4) break;
       const bool ok = ri >= 0 && rj >= 0;
-      r8[q] = ok ? res[cidx<2> (g, ri, rj, 0)] : 0.;
-      xl8[q] = flo >= 0 && rj >= 0 ? ax.at (cidx<2> (g, flo, rj, 0)) : 0.;
-      xu8[q] = fhi >= 0 && rj >= 0 ? ax.at (cidx<2> (g, fhi, rj, 0)) : 0.;
-      if (LAM) l8[q] = ok ? lam.p[cidx<2> (g, ri, rj, 0)] : 0.;
+      r4[q] = ok ? res[cidx<2> (g, ri, rj, 0)] : 0.;
+      xl4[q] = flo >= 0 && rj >= 0 ? ax.at (cidx<2> (g, flo, rj, 0)) : 0.;
+      xu4[q] = fhi >= 0 && rj >= 0 ? ax.at (cidx<2> (g, fhi, rj, 0)) : 0.;
+      if (LAM) l4[q] = ok ? lam.p[cidx<2> (g, ri, rj, 0)] : 0.;
     }
   }
-  /* the iterate is the previous launch's output: its loads are issued
-     before the weights are computed, so that both round trips overlap */
   grid_dependency_wait ();
-  const int cq = (base + p) & 1;                /* colour of the even columns */
+  const int cq = (base + p) & 1;
   if (inner) {
     const long long id = cidx<2> (g, gi, j0 + q0, 0);
-    const Quad<double> va = load_quad (in + id), vb = load_quad (in + id + 4);
+    const Quad<double> va = load_quad (in + id);
     put_quad (sa + cq*WM, sa + (cq ^ 1)*WM, p*M + m0, va);
-    put_quad (sa + cq*WM, sa + (cq ^ 1)*WM, p*M + m0 + 2, vb);
   }
   else {
     const int ri = real_index (gi, n, px);
 #pragma unroll
-    for (int q = 0; q < 8; q++) {
+    for (int q = 0; q < 4; q++) {
       const int rj = real_index (j0 + q0 + q, n, py);
       sa[((cq + q) & 1)*WM + p*M + ((q0 + q) >> 1)] =
         ri >= 0 && rj >= 0 ? in[cidx<2> (g, ri, rj, 0)] : 0.;
     }
   }
-  /* the exact coefficients of cell e of colour c (column 2e + o_c of the
-     eight) and n0 = (-Delta^2) b, the first operation of relax_value
-     (poisson.h:303-319); the diagonal is recomputed in every update, in its
-     order, from -lambda Delta^2 (a register per cell only when lambda is
-     stored) and the four coefficients */
-  double cxl[2][4], cxu[2][4], cyl[2][4], cyr[2][4], cnb[2][4], cdl[2][LAM ? 4 : 1];
+  double cxl[2][2], cxu[2][2], cyl[2][2], cyr[2][2], cnb[2][2], cdl[2][LAM ? 2 : 1];
   const double dlc = (-lam.c)*D2;
-  unsigned valid = 0;                           /* bit 4c + e: a cell that is updated */
+  unsigned valid = 0;
   const bool rowok = px || (unsigned) gi < (unsigned) n;
 #pragma unroll
   for (int c = 0; c < 2; c++)
 #pragma unroll
-    for (int e = 0; e < 4; e++) {
+    for (int e = 0; e < 2; e++) {
       const bool odd = (c ^ base ^ p) & 1;
       const int q = 2*e + (odd ? 1 : 0);
-      const double xl = odd ? xl8[2*e + 1] : xl8[2*e], xu = odd ? xu8[2*e + 1] : xu8[2*e];
-      const double yl = odd ? yl8[2*e + 1] : yl8[2*e], yr = odd ? yl8[2*e + 2] : yl8[2*e + 1];
-      const double rv = odd ? r8[2*e + 1] : r8[2*e];
-      const double lv = LAM ? (odd ? l8[2*e + 1] : l8[2*e]) : lam.c;
+      const double xl = odd ? xl4[2*e + 1] : xl4[2*e], xu = odd ? xu4[2*e + 1] : xu4[2*e];
+      const double yl = odd ? yl4[2*e + 1] : yl4[2*e], yr = odd ? yl4[2*e + 2] : yl4[2*e + 1];
+      const double rv = odd ? r4[2*e + 1] : r4[2*e];
+      const double lv = LAM ? (odd ? l4[2*e + 1] : l4[2*e]) : lam.c;
       const bool ok = rowok && (py || (unsigned) (j0 + q0 + q) < (unsigned) n);
       cxl[c][e] = xl; cxu[c][e] = xu; cyl[c][e] = yl; cyr[c][e] = yr;
       cnb[c][e] = (-D2)*rv;
       if (LAM) cdl[c][LAM ? e : 0] = (-lv)*D2;
-      valid |= (ok ? 1u : 0u) << (4*c + e);
+      valid |= (ok ? 1u : 0u) << (2*c + e);
     }
 
   __syncthreads ();
 
-  /* box ghosts (global -1 and n) of the staged region: ghost = factor x
-     mirror */
   const int glo_i = px ? -1 : -1 - i0, ghi_i = px ? -1 : n - i0;
   const int glo_j = py ? -1 : -1 - j0, ghi_j = py ? -1 : n - j0;
   const bool has_ghosts = !inner &&
@@ -1234,34 +1225,25 @@ k_relax_tile2d_x (bmg_geom g, double * __restrict__ out, const double * __restri
     __syncthreads ();
   }
 
-  /* the colour passes.  Rows shrink by one per pass (whole warps drop out);
-     columns do not: a cell next to the staged region's edge may be updated
-     from stale neighbours, but staleness moves inward by one cell per pass
-     and never reaches the TS x TS interior after 2S passes, so only cells
-     outside the domain (box ghosts, refreshed from their mirrors) are
-     masked.  Shared memory is addressed by 32-bit byte offsets with the
-     row offsets as immediates. */
   const unsigned sbase = (unsigned) __cvta_generic_to_shared (sa);
-  const int o0 = (base ^ p) & 1;               /* column offset of colour 0 in row p */
+  const int o0 = (base ^ p) & 1;
   for (int sw = 0; sw < nsweeps; sw++)
 #pragma unroll
     for (int c = 0; c < 2; c++) {
       const int k = 2*sw + c;
       if (p >= k + 1 && p < W - k - 1) {
         const int o = o0 ^ c;
-        /* the other colour's quad at rows p - 1, p, p + 1 and its left or
+        /* the other colour's pair at rows p - 1, p, p + 1 and its left or
            right neighbour in row p */
         const unsigned aup = sbase + 8u*((c ^ 1)*WM + (p - 1)*M + m0);
-        const double2 u0 = lds_d2<0> (aup), u1 = lds_d2<16> (aup);
-        const double2 m0v = lds_d2<8*M> (aup), m1v = lds_d2<8*M + 16> (aup);
-        const double2 d0 = lds_d2<16*M> (aup), d1 = lds_d2<16*M + 16> (aup);
-        double v[5];
-        if (o == 0) { v[0] = lds_d1<8*M - 8> (aup); v[1] = m0v.x; v[2] = m0v.y; v[3] = m1v.x; v[4] = m1v.y; }
-        else { v[0] = m0v.x; v[1] = m0v.y; v[2] = m1v.x; v[3] = m1v.y; v[4] = lds_d1<8*M + 32> (aup); }
-        const double upv[4] = {u0.x, u0.y, u1.x, u1.y}, dnv[4] = {d0.x, d0.y, d1.x, d1.y};
-        double nv[4];
+        const double2 u0 = lds_d2<0> (aup), m0v = lds_d2<8*M> (aup), d0 = lds_d2<16*M> (aup);
+        double v[3];
+        if (o == 0) { v[0] = lds_d1<8*M - 8> (aup); v[1] = m0v.x; v[2] = m0v.y; }
+        else { v[0] = m0v.x; v[1] = m0v.y; v[2] = lds_d1<8*M + 16> (aup); }
+        const double upv[2] = {u0.x, u0.y}, dnv[2] = {d0.x, d0.y};
+        double nv[2];
 #pragma unroll
-        for (int e = 0; e < 4; e++) {
+        for (int e = 0; e < 2; e++) {
           /* relax_value's expression and order (poisson.h:303-319) */
           double d = LAM ? cdl[c][LAM ? e : 0] : dlc;
           d += cxu[c][e] + cxl[c][e];
@@ -1271,16 +1253,12 @@ k_relax_tile2d_x (bmg_geom g, double * __restrict__ out, const double * __restri
           nv[e] = nn/d;
         }
         const unsigned aw = sbase + 8u*(c*WM + p*M + m0);
-        const unsigned vc = (valid >> (4*c)) & 15u;
-        if (vc == 15u) {
+        const unsigned vc = (valid >> (2*c)) & 3u;
+        if (vc == 3u)
           sts_d2 (aw, make_double2 (nv[0], nv[1]));
-          sts_d2 (aw + 16, make_double2 (nv[2], nv[3]));
-        }
         else {
           if (vc & 1u) sts_d1 (aw, nv[0]);
           if (vc & 2u) sts_d1 (aw + 8, nv[1]);
-          if (vc & 4u) sts_d1 (aw + 16, nv[2]);
-          if (vc & 8u) sts_d1 (aw + 24, nv[3]);
         }
       }
       __syncthreads ();
@@ -1290,7 +1268,6 @@ k_relax_tile2d_x (bmg_geom g, double * __restrict__ out, const double * __restri
       }
     }
 
-  /* the tile interior back, with its ghost images */
   if (inner) {
     constexpr int QT = TS/4;
     for (int idx = tid; idx < TS*QT; idx += nth) {
@@ -1315,11 +1292,11 @@ k_relax_tile2d_x (bmg_geom g, double * __restrict__ out, const double * __restri
 }
 
 template <bool LAM>
-int launch_tile_x (bmg_geom g, void * out, const void * in, const void * res,
-                   const bmg_coef * alpha, bmg_coef lambda, double Delta, BCH h, int nsweeps,
-                   cudaStream_t s)
+int launch_tile_x4 (bmg_geom g, void * out, const void * in, const void * res,
+                    const bmg_coef * alpha, bmg_coef lambda, double Delta, BCH h, int nsweeps,
+                    cudaStream_t s)
 {
-  using namespace tw;
+  using namespace tx4;
   constexpr int TS = 48;
   cudaLaunchConfig_t cfg;
   memset (&cfg, 0, sizeof cfg);
@@ -1332,11 +1309,12 @@ int launch_tile_x (bmg_geom g, void * out, const void * in, const void * res,
   at[0].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = at;
   cfg.numAttrs = 1;
-  return (int) cudaLaunchKernelEx (&cfg, k_relax_tile2d_x<TS, LAM>, g, (double *) out,
+  return (int) cudaLaunchKernelEx (&cfg, k_relax_tile2d_x4<TS, LAM>, g, (double *) out,
                                    (const double *) in, (const double *) res,
                                    coef_of<double> (alpha[0]), coef_of<double> (alpha[1]),
                                    coef_of<double> (lambda), Delta, h, nsweeps);
 }
+
 
 template <int TS, bool LAM>
 int launch_tile_w (bmg_geom g, void * out, const void * in, const void * res,
@@ -2026,8 +2004,8 @@ int bmg_launch_relax_tile (int dim, int st, bmg_geom g, void * out, const void *
   const bool small = g.n <= BMG_SMALL_TILE_N;
   if (st == BMG_ST_F64)
     e = small ? launch_tile<double, 16, 4, 8, 32> (g, out, in, res, alpha, lambda, Delta, h, nsweeps, s)
-      : lambda.p ? launch_tile_x<true> (g, out, in, res, alpha, lambda, Delta, h, nsweeps, s)
-      : launch_tile_x<false> (g, out, in, res, alpha, lambda, Delta, h, nsweeps, s);
+      : lambda.p ? launch_tile_x4<true> (g, out, in, res, alpha, lambda, Delta, h, nsweeps, s)
+      : launch_tile_x4<false> (g, out, in, res, alpha, lambda, Delta, h, nsweeps, s);
   else
     e = small ? launch_tile<float, 16, 4, 8, 32> (g, out, in, res, alpha, lambda, Delta, h, nsweeps, s)
       : g.n == BMG_DEEP_TILE_N ?
