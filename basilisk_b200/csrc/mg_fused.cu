@@ -501,7 +501,8 @@ template <int TS, bool LAM>
 __global__ void __launch_bounds__ (tw::BX*tw::BY, 2)
 k_relax_tile2d_w (bmg_geom g, float * __restrict__ out, const float * __restrict__ in,
                   const float * __restrict__ res, Coef<float> ax, Coef<float> ay, Coef<float> lam,
-                  float Delta, BCH bc, int nsweeps)
+                  float Delta, BCH bc, int nsweeps, double * __restrict__ acor, bmg_geom ga,
+                  bmg_bcdesc abc)
 {
   using namespace tw;
   constexpr int H = Tile<TS>::H;
@@ -690,7 +691,10 @@ k_relax_tile2d_w (bmg_geom g, float * __restrict__ out, const float * __restrict
       }
     }
 
-  /* the tile interior back, with its ghost images */
+  /* the tile interior back, with its ghost images; the last launch of a
+     cycle's finest level also applies the correction a += da
+     (poisson.h:84-89, k_correct's expression) to its tile, with the
+     boundary conditions of a */
   if (inner) {
     constexpr int QT = TS/4;
     for (int idx = tid; idx < TS*QT; idx += nth) {
@@ -699,7 +703,15 @@ k_relax_tile2d_w (bmg_geom g, float * __restrict__ out, const float * __restrict
       Quad<float> v;
       v.x = sa[c0*WM + pp*M + m]; v.z = sa[c0*WM + pp*M + m + 1];
       v.y = sa[(c0 ^ 1)*WM + pp*M + m]; v.w = sa[(c0 ^ 1)*WM + pp*M + m + 1];
-      store_quad (out + cidx<2> (g, blockIdx.y*TS + rr, blockIdx.x*TS + 4*k, 0), v);
+      const int oi = blockIdx.y*TS + rr, oj = blockIdx.x*TS + 4*k;
+      store_quad (out + cidx<2> (g, oi, oj, 0), v);
+      if (acor) {
+        double * ap = acor + cidx<2> (ga, oi, oj, 0);
+        Quad<double> av = load_quad (ap);
+        av.x = av.x + (double) v.x; av.y = av.y + (double) v.y;
+        av.z = av.z + (double) v.z; av.w = av.w + (double) v.w;
+        store_quad (ap, av);
+      }
     }
     return;
   }
@@ -711,6 +723,12 @@ k_relax_tile2d_w (bmg_geom g, float * __restrict__ out, const float * __restrict
     const float v = sa[((base + pp + q) & 1)*WM + pp*M + (q >> 1)];
     out[cidx<2> (g, oi, oj, 0)] = v;
     ghosts_homog<2, float> (out, g, oi, oj, 0, v, bc);
+    if (acor) {
+      const long long ia = cidx<2> (ga, oi, oj, 0);
+      const double an = acor[ia] + (double) v;
+      acor[ia] = an;
+      ghosts_inhomog<2> (acor, ga, oi, oj, 0, an, abc);
+    }
   }
 }
 
@@ -1103,7 +1121,7 @@ template <int TS, bool LAM>
 __global__ void __launch_bounds__ (tx4::BX*tx4::BY, 1)
 k_relax_tile2d_x4 (bmg_geom g, double * __restrict__ out, const double * __restrict__ in,
                    const double * __restrict__ res, Coef<double> ax, Coef<double> ay, Coef<double> lam,
-                   double Delta, BCH bc, int nsweeps)
+                   double Delta, BCH bc, int nsweeps, double * __restrict__ acor, bmg_bcdesc abc)
 {
   using namespace tx4;
   constexpr int H = (W - TS)/2;
@@ -1268,6 +1286,8 @@ k_relax_tile2d_x4 (bmg_geom g, double * __restrict__ out, const double * __restr
       }
     }
 
+  /* (and a += da on the cycle's last launch of the finest level, as in
+     k_relax_tile2d_w) */
   if (inner) {
     constexpr int QT = TS/4;
     for (int idx = tid; idx < TS*QT; idx += nth) {
@@ -1276,7 +1296,13 @@ k_relax_tile2d_x4 (bmg_geom g, double * __restrict__ out, const double * __restr
       Quad<double> v;
       v.x = sa[c0*WM + pp*M + m]; v.z = sa[c0*WM + pp*M + m + 1];
       v.y = sa[(c0 ^ 1)*WM + pp*M + m]; v.w = sa[(c0 ^ 1)*WM + pp*M + m + 1];
-      store_quad (out + cidx<2> (g, blockIdx.y*TS + rr, blockIdx.x*TS + 4*k, 0), v);
+      const long long id = cidx<2> (g, blockIdx.y*TS + rr, blockIdx.x*TS + 4*k, 0);
+      store_quad (out + id, v);
+      if (acor) {
+        Quad<double> av = load_quad (acor + id);
+        av.x = av.x + v.x; av.y = av.y + v.y; av.z = av.z + v.z; av.w = av.w + v.w;
+        store_quad (acor + id, av);
+      }
     }
     return;
   }
@@ -1286,15 +1312,21 @@ k_relax_tile2d_x4 (bmg_geom g, double * __restrict__ out, const double * __restr
     if (oi >= n || oj >= n) continue;
     const int pp = rr + H, q = s + H;
     const double v = sa[((base + pp + q) & 1)*WM + pp*M + (q >> 1)];
-    out[cidx<2> (g, oi, oj, 0)] = v;
+    const long long id = cidx<2> (g, oi, oj, 0);
+    out[id] = v;
     ghosts_homog<2, double> (out, g, oi, oj, 0, v, bc);
+    if (acor) {
+      const double an = acor[id] + v;
+      acor[id] = an;
+      ghosts_inhomog<2> (acor, g, oi, oj, 0, an, abc);
+    }
   }
 }
 
 template <bool LAM>
 int launch_tile_x4 (bmg_geom g, void * out, const void * in, const void * res,
                     const bmg_coef * alpha, bmg_coef lambda, double Delta, BCH h, int nsweeps,
-                    cudaStream_t s)
+                    double * acor, const bmg_bcdesc & abc, cudaStream_t s)
 {
   using namespace tx4;
   constexpr int TS = 48;
@@ -1312,14 +1344,14 @@ int launch_tile_x4 (bmg_geom g, void * out, const void * in, const void * res,
   return (int) cudaLaunchKernelEx (&cfg, k_relax_tile2d_x4<TS, LAM>, g, (double *) out,
                                    (const double *) in, (const double *) res,
                                    coef_of<double> (alpha[0]), coef_of<double> (alpha[1]),
-                                   coef_of<double> (lambda), Delta, h, nsweeps);
+                                   coef_of<double> (lambda), Delta, h, nsweeps, acor, abc);
 }
 
 
 template <int TS, bool LAM>
 int launch_tile_w (bmg_geom g, void * out, const void * in, const void * res,
                    const bmg_coef * alpha, bmg_coef lambda, double Delta, BCH h, int nsweeps,
-                   cudaStream_t s)
+                   double * acor, bmg_geom ga, const bmg_bcdesc & abc, cudaStream_t s)
 {
   using namespace tw;
   cudaLaunchConfig_t cfg;
@@ -1336,7 +1368,7 @@ int launch_tile_w (bmg_geom g, void * out, const void * in, const void * res,
   return (int) cudaLaunchKernelEx (&cfg, k_relax_tile2d_w<TS, LAM>, g, (float *) out, (const float *) in,
                                    (const float *) res, coef_of<float> (alpha[0]),
                                    coef_of<float> (alpha[1]), coef_of<float> (lambda),
-                                   (float) Delta, h, nsweeps);
+                                   (float) Delta, h, nsweeps, acor, ga, abc);
 }
 
 /* ---------------------------------------------------------------- */
@@ -1990,12 +2022,22 @@ int bmg_tile_sweeps (int st, int n)
   return st == BMG_ST_F32 && n == BMG_DEEP_TILE_N ? 8 : 4;
 }
 
+int bmg_tile_corrects (int st, int n)
+{
+  return n > BMG_SMALL_TILE_N;
+}
+
 int bmg_launch_relax_tile (int dim, int st, bmg_geom g, void * out, const void * in,
                            const void * res, const bmg_coef * alpha, bmg_coef lambda,
-                           double Delta, const bmg_bcdesc * bc, int nsweeps, cudaStream_t s)
+                           double Delta, const bmg_bcdesc * bc, int nsweeps, double * acor,
+                           bmg_geom ga, const bmg_bcdesc * abc, cudaStream_t s)
 {
   if (dim != 2 || nsweeps < 1 || nsweeps > bmg_tile_sweeps (st, g.n)) return (int) cudaErrorInvalidValue;
+  if (acor && (!abc || !bmg_tile_corrects (st, g.n))) return (int) cudaErrorInvalidValue;
   BCH h = bch_of (bc);
+  bmg_bcdesc abc0;
+  memset (&abc0, 0, sizeof abc0);
+  const bmg_bcdesc & ab = abc ? *abc : abc0;
   int e;
   /* small levels: 16 x 16 tiles (more CTAs, a shorter critical path per
      CTA); large levels: big tiles (less halo recomputation).  A deeper halo
@@ -2004,15 +2046,15 @@ int bmg_launch_relax_tile (int dim, int st, bmg_geom g, void * out, const void *
   const bool small = g.n <= BMG_SMALL_TILE_N;
   if (st == BMG_ST_F64)
     e = small ? launch_tile<double, 16, 4, 8, 32> (g, out, in, res, alpha, lambda, Delta, h, nsweeps, s)
-      : lambda.p ? launch_tile_x4<true> (g, out, in, res, alpha, lambda, Delta, h, nsweeps, s)
-      : launch_tile_x4<false> (g, out, in, res, alpha, lambda, Delta, h, nsweeps, s);
+      : lambda.p ? launch_tile_x4<true> (g, out, in, res, alpha, lambda, Delta, h, nsweeps, acor, ab, s)
+      : launch_tile_x4<false> (g, out, in, res, alpha, lambda, Delta, h, nsweeps, acor, ab, s);
   else
     e = small ? launch_tile<float, 16, 4, 8, 32> (g, out, in, res, alpha, lambda, Delta, h, nsweeps, s)
       : g.n == BMG_DEEP_TILE_N ?
-        (lambda.p ? launch_tile_w<32, true> (g, out, in, res, alpha, lambda, Delta, h, nsweeps, s)
-                  : launch_tile_w<32, false> (g, out, in, res, alpha, lambda, Delta, h, nsweeps, s))
-      : lambda.p ? launch_tile_w<48, true> (g, out, in, res, alpha, lambda, Delta, h, nsweeps, s)
-      : launch_tile_w<48, false> (g, out, in, res, alpha, lambda, Delta, h, nsweeps, s);
+        (lambda.p ? launch_tile_w<32, true> (g, out, in, res, alpha, lambda, Delta, h, nsweeps, acor, ga, ab, s)
+                  : launch_tile_w<32, false> (g, out, in, res, alpha, lambda, Delta, h, nsweeps, acor, ga, ab, s))
+      : lambda.p ? launch_tile_w<48, true> (g, out, in, res, alpha, lambda, Delta, h, nsweeps, acor, ga, ab, s)
+      : launch_tile_w<48, false> (g, out, in, res, alpha, lambda, Delta, h, nsweeps, acor, ga, ab, s);
   if (e) return e;
   cudaError_t r = cudaGetLastError ();
   return r == cudaSuccess ? 0 : (int) r;

@@ -744,6 +744,34 @@ static int residual_max (bmg_grid * g, field_t * a, const double * b, const coef
   return BMG_OK;
 }
 
+/* the residual of an mg_solve iteration: on 2D grids fused with the
+   restriction of res into the level below, which the next cycle then
+   skips (returns 1 when it restricted) */
+static int fused_tail (const bmg_grid * g) { return g->dim == 2 && g->depth >= 1; }
+
+static int residual_tail (bmg_grid * g, field_t * a, const double * b, const coefs_t * c,
+                          const levels_t * lv, double * maxres, int sync, work_t * w)
+{
+  const int L = g->depth;
+  if (!fused_tail (g))
+    return residual_max (g, a, b, c, lv->res[L], lv->st[L], maxres, sync, w);
+  CK (cudaMemsetAsync (g->d_maxres, 0, sizeof (unsigned long long), g->stream));
+  CL (bmg_launch_residual_restrict (lv->st[L], lv->st[L - 1], g->g64[L], geom_st (g, L, lv->st[L]),
+                                    geom_st (g, L - 1, lv->st[L - 1]), a->lv[L], b,
+                                    c->alpha64[L], c->lambda64[L], delta_of (g, L),
+                                    lv->res[L], lv->res[L - 1], g->d_maxres, g->stream));
+  w->launches += 1;
+  w->bytes += ncells (g, L)*(8.*(2. + (c->alpha_stored ? g->dim : 0) +
+                                 (c->lambda_stored ? 1 : 0)) + es_of (lv->st[L])) +
+    ncells (g, L - 1)*es_of (lv->st[L - 1]);
+  if (sync) {
+    CK (cudaMemcpyAsync (g->h_pinned, g->d_maxres, sizeof (double), cudaMemcpyDeviceToHost, g->stream));
+    CK (cudaStreamSynchronize (g->stream));
+    *maxres = g->h_pinned[0];
+  }
+  return BMG_OK;
+}
+
 /* an event on stream s: a graph node of its own while s is being captured
    (the external flag), a plain record otherwise (the flag is refused
    outside a capture) */
@@ -804,12 +832,15 @@ static int use_cluster (const bmg_grid * g, const levels_t * lv, int l, int minl
    the da and da2 buffers). */
 static int cycle_launches (bmg_grid * g, field_t * a, const levels_t * lv, const coefs_t * c,
                            const bmg_bcdesc * dabc, int nrelax, int minlevel, int maxlevel,
-                           void ** fin, work_t * w)
+                           int top_restricted, void ** fin, work_t * w)
 {
   const int dim = g->dim, L = g->depth;
   cudaStream_t s = g->stream;
   double bytes = 0.;
   long long launches = 0, sweeps = 0;
+  bmg_bcdesc abc;                   /* the boundary conditions of a */
+  bcdesc_of (g, a, &abc);
+  int corrected = 0;
   /* restriction (res) down to minlevel (multigrid-common.h:368-404); on the
      red-black path the levels of the bottom solve are restricted inside it */
   int rlow = minlevel;
@@ -817,7 +848,9 @@ static int cycle_launches (bmg_grid * g, field_t * a, const levels_t * lv, const
     bmg_bottom_level bl[BMG_MAXLEVEL + 1];
     rlow = bottom_top (g, lv, c, minlevel, maxlevel, bl) + 1;
   }
-  for (int l = L - 1; l >= rlow; l--) {
+  /* (res of level L - 1 may already be the restriction of the finest
+     residual, made by the residual that ended the previous iteration) */
+  for (int l = top_restricted ? L - 2 : L - 1; l >= rlow; l--) {
     CL (bmg_launch_restrict (dim, lv->st[l + 1], lv->st[l], geom_st (g, l + 1, lv->st[l + 1]),
                              geom_st (g, l, lv->st[l]), lv->res[l + 1], lv->res[l], s));
     bytes += ncells (g, l + 1)*es_of (lv->st[l + 1]) + ncells (g, l)*es_of (lv->st[l]);
@@ -885,15 +918,24 @@ static int cycle_launches (bmg_grid * g, field_t * a, const levels_t * lv, const
     const int timed = g->timing && l == L && maxlevel == L;
     if (timed) CK (record_event (g->evr0, s));
     if (g->relax == BMG_RELAX_RBGS && dim == 2) {
-      /* several complete red-black sweeps per launch, ping-pong buffers */
+      /* several complete red-black sweeps per launch, ping-pong buffers;
+         the last launch of the finest level also applies a += da */
       const int S = bmg_tile_sweeps (st, gl.n);
+      const int fuse = l == L && maxlevel == L && bmg_tile_corrects (st, gl.n);
       for (int done = 0; done < nrelax; ) {
         const int k = nrelax - done < S ? nrelax - done : S;
+        const int last = fuse && done + k >= nrelax;
         CL (bmg_launch_relax_tile (dim, st, gl, oth[l], cur[l], lv->res[l], al, la,
-                                   delta_of (g, l), dabc, k, s));
+                                   delta_of (g, l), dabc, k, last ? a->lv[L] : NULL,
+                                   g->g64[L], last ? &abc : NULL, s));
         void * t = cur[l]; cur[l] = oth[l]; oth[l] = t;
         launches++;
         done += k;
+      }
+      if (fuse) {
+        corrected = 1;
+        bytes += ncells (g, L)*16.;
+        if (timed) w->relax_bytes += ncells (g, L)*16.;
       }
     }
     else
@@ -920,10 +962,9 @@ static int cycle_launches (bmg_grid * g, field_t * a, const levels_t * lv, const
       w->relax_sweeps += nrelax;
     }
   }
-  /* a += da on the finest level, with the BCs of a (poisson.h:84-89) */
-  {
-    bmg_bcdesc abc;
-    bcdesc_of (g, a, &abc);
+  /* a += da on the finest level, with the BCs of a (poisson.h:84-89),
+     unless the finest level's last tile launch applied it */
+  if (!corrected) {
     const int st = lv->st[L];
     CL (bmg_launch_correct (dim, st, g->g64[L], geom_st (g, L, st), a->lv[L], cur[L], &abc, s));
     bytes += ncells (g, L)*(16. + es_of (st));
@@ -982,9 +1023,10 @@ static int run_cycle (bmg_grid * g, field_t * a, const double * bdata, const lev
       cudaGraph_t graph;
       memset (&victim->w, 0, sizeof victim->w);
       CK (cudaStreamBeginCapture (g->stream, cudaStreamCaptureModeThreadLocal));
-      int r = cycle_launches (g, a, lv, c, dabc, nrelax, minlevel, L, fin, &victim->w);
+      int r = cycle_launches (g, a, lv, c, dabc, nrelax, minlevel, L, fused_tail (g), fin,
+                              &victim->w);
       double dummy;
-      if (!r) r = residual_max (g, a, bdata, c, lv->res[L], lv->st[L], &dummy, 0, &victim->w);
+      if (!r) r = residual_tail (g, a, bdata, c, lv, &dummy, 0, &victim->w);
       cudaError_t me = cudaMemcpyAsync (g->h_pinned, g->d_maxres, sizeof (double),
                                         cudaMemcpyDeviceToHost, g->stream);
 
@@ -1006,10 +1048,10 @@ static int run_cycle (bmg_grid * g, field_t * a, const double * bdata, const lev
     w = e->w;
   }
   else {
-    int r = cycle_launches (g, a, lv, c, dabc, nrelax, minlevel, L, fin, &w);
+    int r = cycle_launches (g, a, lv, c, dabc, nrelax, minlevel, L, fused_tail (g), fin, &w);
     if (r) return r;
     double dummy;
-    r = residual_max (g, a, bdata, c, lv->res[L], lv->st[L], &dummy, 0, &w);
+    r = residual_tail (g, a, bdata, c, lv, &dummy, 0, &w);
     if (r) return r;
     CK (cudaMemcpyAsync (g->h_pinned, g->d_maxres, sizeof (double), cudaMemcpyDeviceToHost,
                          g->stream));
@@ -1081,7 +1123,7 @@ static int solve (bmg_grid * g, field_t * a, field_t * b, coefs_t * c, int nrela
 
   double resb;
   work_t w0 = {0., 0, 0, 0., 0};
-  r = residual_max (g, a, bdata, c, lv.res[L], lv.st[L], &s.resb, 1, &w0);
+  r = residual_tail (g, a, bdata, c, &lv, &s.resb, 1, &w0);
   if (r) return r;
   resb = s.resa = s.resb;
   if (tolerance == 0.)
@@ -1348,7 +1390,7 @@ void mg_cycle (bmg_scalar * al, bmg_scalar * resl, bmg_scalar * dal,
   bcdesc_of (g, da, &dabc);
   void * fin[BMG_MAXLEVEL + 1];
   work_t w = {0., 0, 0, 0., 0};
-  if (cycle_launches (g, a, &lv, &c, &dabc, nrelax, minlevel, maxlevel, fin, &w)) return;
+  if (cycle_launches (g, a, &lv, &c, &dabc, nrelax, minlevel, maxlevel, 0, fin, &w)) return;
   /* Jacobi may leave a level's final iterate in the workspace partner */
   for (int l = minlevel; l <= maxlevel; l++)
     if (fin[l] != da->lv[l])

@@ -288,6 +288,52 @@ __global__ void k_residual (bmg_geom g, bmg_geom gr, const double * __restrict__
   block_max_atomic (m, maxres);
 }
 
+/* the residual of the finest 2D level fused with its restriction into the
+   level below (multigrid-common.h:368-404): each thread computes the four
+   residuals of one coarse cell's children with k_residual's expression and
+   order, stores them, and stores their mean in k_restrict's order (children
+   in foreach_child order, from the stored values), so the results are
+   bit-identical to k_residual followed by k_restrict */
+template <typename TR, typename TC, bool POW2>
+__global__ void k_residual_restrict2d (bmg_geom g, bmg_geom gr, bmg_geom gc,
+                                       const double * __restrict__ a,
+                                       const double * __restrict__ b, Coef<double> ax,
+                                       Coef<double> ay, Coef<double> lam, double Delta,
+                                       TR * __restrict__ res, TC * __restrict__ resc,
+                                       unsigned long long * maxres)
+{
+  pdl_wait ();
+  pdl_trigger ();
+  const int cj = blockIdx.x*blockDim.x + threadIdx.x, ci = blockIdx.y*blockDim.y + threadIdx.y;
+  double m = 0.;
+  const double rD = 1./Delta;
+  if (ci < gc.n && cj < gc.n) {
+    TC sum = TC(0);
+#pragma unroll
+    for (int u = 0; u < 2; u++)
+#pragma unroll
+      for (int v = 0; v < 2; v++) {
+        const int i = 2*ci + u, j = 2*cj + v;
+        const long long id = cidx<2> (g, i, j, 0);
+        const double ac = a[id];
+        double r = b[id] - lam.at (id)*ac;
+        {
+          const long long s = g.P;
+          r += over_delta<POW2> (ax.at (id)*over_delta<POW2> (ac - a[id - s], Delta, rD) -
+                                 ax.at (id + s)*over_delta<POW2> (a[id + s] - ac, Delta, rD), Delta, rD);
+        }
+        r += over_delta<POW2> (ay.at (id)*over_delta<POW2> (ac - a[id - 1], Delta, rD) -
+                               ay.at (id + 1)*over_delta<POW2> (a[id + 1] - ac, Delta, rD), Delta, rD);
+        const TR rs = (TR) r;
+        res[cidx<2> (gr, i, j, 0)] = rs;
+        sum += (TC) rs;
+        m = nanmax (m, fabs (r));
+      }
+    resc[cidx<2> (gc, ci, cj, 0)] = sum/TC(4);
+  }
+  block_max_atomic (m, maxres);
+}
+
 /* ---------------------------------------------------------------- */
 /* correction a += da, boundary conditions                           */
 /* ---------------------------------------------------------------- */
@@ -570,6 +616,25 @@ void residual_dim (int st, bmg_geom g, bmg_geom gr, const double * a, const doub
     if (pow2) pdl_launch (k_residual<DIM, float, true>, gb, bb, 0, s, g, gr, a, b, ax, ay, az, lam, Delta, (float *) res, maxres);
     else pdl_launch (k_residual<DIM, float, false>, gb, bb, 0, s, g, gr, a, b, ax, ay, az, lam, Delta, (float *) res, maxres);
   }
+}
+
+template <typename TR, typename TC>
+void residual_restrict_2d (bmg_geom g, bmg_geom gr, bmg_geom gc, const double * a,
+                           const double * b, const bmg_coef * alpha, bmg_coef lambda,
+                           double Delta, void * res, void * resc, unsigned long long * maxres,
+                           cudaStream_t s)
+{
+  Coef<double> ax = coef_of<double> (alpha[0]), ay = coef_of<double> (alpha[1]),
+    lam = coef_of<double> (lambda);
+  const dim3 bb (32, 8, 1), gb ((gc.n + 31)/32, (gc.n + 7)/8, 1);
+  int ex;
+  const bool pow2 = Delta > 0. && frexp (Delta, &ex) == 0.5 && ex > -1000 && ex < 1000;
+  if (pow2)
+    pdl_launch (k_residual_restrict2d<TR, TC, true>, gb, bb, 0, s, g, gr, gc, a, b, ax, ay, lam,
+                Delta, (TR *) res, (TC *) resc, maxres);
+  else
+    pdl_launch (k_residual_restrict2d<TR, TC, false>, gb, bb, 0, s, g, gr, gc, a, b, ax, ay, lam,
+                Delta, (TR *) res, (TC *) resc, maxres);
 }
 
 template <int DIM>
@@ -1013,6 +1078,25 @@ int bmg_launch_residual (int dim, int st_res, bmg_geom g, bmg_geom gres, const d
 {
   DISPATCH_DIM (dim, residual_dim, st_res, g, gres, a, b, alpha, lambda, Delta, res, maxres, s);
   return status_of_launch ();
+}
+
+int bmg_launch_residual_restrict (int st_res, int st_coarse, bmg_geom g, bmg_geom gres,
+                                  bmg_geom gcoarse, const double * a, const double * b,
+                                  const bmg_coef * alpha, bmg_coef lambda, double Delta,
+                                  void * res, void * coarse, unsigned long long * maxres,
+                                  cudaStream_t s)
+{
+  if (g.n < 2 || gcoarse.n*2 != g.n) return (int) cudaErrorInvalidValue;
+  if (st_res == BMG_ST_F64 && st_coarse == BMG_ST_F64)
+    residual_restrict_2d<double, double> (g, gres, gcoarse, a, b, alpha, lambda, Delta, res, coarse, maxres, s);
+  else if (st_res == BMG_ST_F32 && st_coarse == BMG_ST_F32)
+    residual_restrict_2d<float, float> (g, gres, gcoarse, a, b, alpha, lambda, Delta, res, coarse, maxres, s);
+  else if (st_res == BMG_ST_F32 && st_coarse == BMG_ST_F64)
+    residual_restrict_2d<float, double> (g, gres, gcoarse, a, b, alpha, lambda, Delta, res, coarse, maxres, s);
+  else
+    residual_restrict_2d<double, float> (g, gres, gcoarse, a, b, alpha, lambda, Delta, res, coarse, maxres, s);
+  cudaError_t r = cudaGetLastError ();
+  return r == cudaSuccess ? 0 : (int) r;
 }
 
 int bmg_launch_correct (int dim, int st_da, bmg_geom g, bmg_geom gda, double * a,

@@ -80,6 +80,16 @@ int bmg_launch_residual (int dim, int st_res, bmg_geom g, bmg_geom gres,
                          void * res, unsigned long long * maxres,
                          cudaStream_t s);
 
+/* the 2D residual of the finest level (as bmg_launch_residual, max into
+   maxres) fused with its restriction into the level below (coarse, storage
+   st_coarse, geometry gcoarse): bit-identical to bmg_launch_residual then
+   bmg_launch_restrict */
+int bmg_launch_residual_restrict (int st_res, int st_coarse, bmg_geom g, bmg_geom gres,
+                                  bmg_geom gcoarse, const double * a, const double * b,
+                                  const bmg_coef * alpha, bmg_coef lambda, double Delta,
+                                  void * res, void * coarse, unsigned long long * maxres,
+                                  cudaStream_t s);
+
 int bmg_launch_correct (int dim, int st_da, bmg_geom g, bmg_geom gda, double * a,
                         const void * da, const bmg_bcdesc * bc, cudaStream_t s);
 
@@ -114,9 +124,15 @@ int bmg_launch_face_wrap (int dim, bmg_geom g, int face_dim, double * f, cudaStr
 
 /* fused red-black relaxation (mg_fused.cu) */
 int bmg_tile_sweeps (int st, int n);   /* sweeps one tile launch can do on an n x n level */
+/* whether the tile launch of an n x n level can apply the correction: with
+   acor != NULL (the FP64 finest level of a, geometry ga, boundary conditions
+   abc) the launch also does a += out on every cell it writes, with the
+   ghost images of a (poisson.h:84-89) */
+int bmg_tile_corrects (int st, int n);
 int bmg_launch_relax_tile (int dim, int st, bmg_geom g, void * out, const void * in,
                            const void * res, const bmg_coef * alpha, bmg_coef lambda,
-                           double Delta, const bmg_bcdesc * bc, int nsweeps, cudaStream_t s);
+                           double Delta, const bmg_bcdesc * bc, int nsweeps, double * acor,
+                           bmg_geom ga, const bmg_bcdesc * abc, cudaStream_t s);
 
 /* all nrelax red-black sweeps of a 128^2 or 256^2 FP32 2D level in one
    launch of one thread-block cluster, the bilinear prolongation of coarse
