@@ -1323,6 +1323,289 @@ k_relax_tile2d_x4 (bmg_geom g, double * __restrict__ out, const double * __restr
   }
 }
 
+/* The plain FP64 form of k_level_cluster, for the 64^2 and 128^2 levels:
+   the same strips, exchanges and barriers, eight cells per thread (four
+   of each colour) whose exact coefficients and -Delta^2 b stay in
+   registers, and every update in relax_value's expression and order with
+   the IEEE division (as k_relax_tile2d_x4), so that the result is
+   bit-identical to the single-CTA bottom and the tile launches it
+   replaces; the fused prolongation is bilinear's expression in FP64. */
+namespace clx {
+template <int N, int C> struct Shape {
+  static constexpr int R = N/C, H = 8, S = 4;
+  static constexpr int BYR = R + 2*H, BX = N/8, NT = BX*BYR, RW = 32/BX;
+  static constexpr int OFS = 4, MP = N/2 + 8;
+  static constexpr int SAW = BYR*MP, OWW = R*MP;
+  static constexpr size_t bytes = sizeof (double)*(2*SAW + 4*OWW);
+  static_assert (R >= H && 32 % BX == 0 && BYR % (2*RW) == 0 && NT <= 1024, "cluster level shape");
+};
+}
+
+template <int N, int C, bool LAM>
+__global__ void __launch_bounds__ (clx::Shape<N, C>::NT, 1)
+k_level_cluster_x (bmg_geom g, double * __restrict__ out, const double * __restrict__ res,
+                   Coef<double> ax, Coef<double> ay, Coef<double> lam, double Delta, BCH bc,
+                   int nrelax, bmg_geom gc, const double * __restrict__ coarse)
+{
+  typedef clx::Shape<N, C> Sh;
+  constexpr int R = Sh::R, H = Sh::H, S = Sh::S, BYR = Sh::BYR, BX = Sh::BX, RW = Sh::RW;
+  constexpr int OFS = Sh::OFS, MP = Sh::MP, SAW = Sh::SAW, OWW = Sh::OWW;
+  extern __shared__ __align__ (16) double xsm[];
+  double * sa = xsm, * own = xsm + 2*SAW;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int p = 2*RW*(ty/(2*RW)) + 2*(ty % RW) + ((ty/RW) & 1);
+  const int rank = (int) cluster_rank ();
+  const int px = bc.periodic[0], py = bc.periodic[1];
+  const int gi = rank*R - H + p, ri = real_index (gi, N, px);
+  const bool rowok = ri >= 0;
+  const int ce = gi & 1, q0 = 8*tx, m0 = 4*tx;
+  const double D2 = Delta*Delta;
+  pdl_trigger ();
+
+  /* the exact coefficients of the thread's eight cells */
+  double cxl[2][4], cxu[2][4], cyl[2][4], cyr[2][4], cnb[2][4], cdl[2][LAM ? 4 : 1];
+  {
+    double r8[8], xl8[8], xu8[8], yl8[9], l8[8];
+#pragma unroll
+    for (int q = 0; q < 8; q++) { r8[q] = xl8[q] = xu8[q] = yl8[q] = l8[q] = 0.; }
+    yl8[8] = 0.;
+    if (rowok) {
+      const int flo = real_face (gi, N, px), fhi = real_face (gi + 1, N, px);
+      const long long id = cidx<2> (g, ri, q0, 0);
+      const Quad<double> r0 = load_quad (res + id), r1 = load_quad (res + id + 4);
+      r8[0] = r0.x; r8[1] = r0.y; r8[2] = r0.z; r8[3] = r0.w;
+      r8[4] = r1.x; r8[5] = r1.y; r8[6] = r1.z; r8[7] = r1.w;
+      if (ax.p) {
+        const long long il = cidx<2> (g, flo, q0, 0), iu = cidx<2> (g, fhi, q0, 0);
+        const Quad<double> a0 = load_quad (ax.p + il), a1 = load_quad (ax.p + il + 4);
+        const Quad<double> b0 = load_quad (ax.p + iu), b1 = load_quad (ax.p + iu + 4);
+        xl8[0] = a0.x; xl8[1] = a0.y; xl8[2] = a0.z; xl8[3] = a0.w;
+        xl8[4] = a1.x; xl8[5] = a1.y; xl8[6] = a1.z; xl8[7] = a1.w;
+        xu8[0] = b0.x; xu8[1] = b0.y; xu8[2] = b0.z; xu8[3] = b0.w;
+        xu8[4] = b1.x; xu8[5] = b1.y; xu8[6] = b1.z; xu8[7] = b1.w;
+      }
+      else
+#pragma unroll
+        for (int q = 0; q < 8; q++) xl8[q] = xu8[q] = ax.c;
+      if (ay.p) {
+        const Quad<double> a0 = load_quad (ay.p + id), a1 = load_quad (ay.p + id + 4);
+        yl8[0] = a0.x; yl8[1] = a0.y; yl8[2] = a0.z; yl8[3] = a0.w;
+        yl8[4] = a1.x; yl8[5] = a1.y; yl8[6] = a1.z; yl8[7] = a1.w;
+        yl8[8] = ay.p[cidx<2> (g, ri, real_face (q0 + 8, N, py), 0)];
+      }
+      else
+#pragma unroll
+        for (int q = 0; q < 9; q++) yl8[q] = ay.c;
+      if (LAM) {
+        const Quad<double> a0 = load_quad (lam.p + id), a1 = load_quad (lam.p + id + 4);
+        l8[0] = a0.x; l8[1] = a0.y; l8[2] = a0.z; l8[3] = a0.w;
+        l8[4] = a1.x; l8[5] = a1.y; l8[6] = a1.z; l8[7] = a1.w;
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < 2; c++)
+#pragma unroll
+      for (int e = 0; e < 4; e++) {
+        const bool odd = (c ^ ce) & 1;
+        cxl[c][e] = odd ? xl8[2*e + 1] : xl8[2*e]; cxu[c][e] = odd ? xu8[2*e + 1] : xu8[2*e];
+        cyl[c][e] = odd ? yl8[2*e + 1] : yl8[2*e]; cyr[c][e] = odd ? yl8[2*e + 2] : yl8[2*e + 1];
+        cnb[c][e] = (-D2)*(odd ? r8[2*e + 1] : r8[2*e]);
+        if (LAM) cdl[c][LAM ? e : 0] = (-(odd ? l8[2*e + 1] : l8[2*e]))*D2;
+      }
+  }
+  const double dlc = (-lam.c)*D2;
+
+  const bool rowghost_lo = !px && gi == 0 && p >= 1, rowghost_hi = !px && gi == N - 1 && p <= BYR - 2;
+  const double frow = rowghost_lo ? (double) bc.fac[1] : (double) bc.fac[0];
+  const double fbot = (double) bc.fac[3], ftop = (double) bc.fac[2];
+  const bool first_col = tx == 0, last_col = tx == BX - 1;
+  auto put_ghosts = [&] (int c, const double * nv) {
+    if (rowghost_lo || rowghost_hi) {
+      double * gr = sa + (c ^ 1)*SAW + (rowghost_lo ? p - 1 : p + 1)*MP + OFS + m0;
+#pragma unroll
+      for (int e = 0; e < 4; e++) gr[e] = nv[e]*frow;
+    }
+    const int o = c ^ ce;
+    if (first_col && o == 0) {
+      if (py) sa[c*SAW + p*MP + OFS + N/2] = nv[0];
+      else sa[(c ^ 1)*SAW + p*MP + OFS - 1] = nv[0]*fbot;
+    }
+    if (last_col && o == 1) {
+      if (py) sa[c*SAW + p*MP + OFS - 1] = nv[3];
+      else sa[(c ^ 1)*SAW + p*MP + OFS + N/2] = nv[3]*ftop;
+    }
+  };
+  auto stage_ghosts = [&] () {
+    if (!rowok) return;
+    const int c0 = ce, cl = ce ^ 1;
+    if (first_col) {
+      const double v = sa[c0*SAW + p*MP + OFS];
+      if (py) sa[c0*SAW + p*MP + OFS + N/2] = v;
+      else sa[(c0 ^ 1)*SAW + p*MP + OFS - 1] = v*fbot;
+    }
+    if (last_col) {
+      const double v = sa[cl*SAW + p*MP + OFS + N/2 - 1];
+      if (py) sa[cl*SAW + p*MP + OFS - 1] = v;
+      else sa[(cl ^ 1)*SAW + p*MP + OFS + N/2] = v*ftop;
+    }
+    if (rowghost_lo || rowghost_hi) {
+      const int pg = rowghost_lo ? p - 1 : p + 1;
+#pragma unroll
+      for (int c = 0; c < 2; c++)
+#pragma unroll
+        for (int e = 0; e < 4; e++)
+          sa[(c ^ 1)*SAW + pg*MP + OFS + m0 + e] = sa[c*SAW + p*MP + OFS + m0 + e]*frow;
+    }
+  };
+
+  const unsigned sbase = (unsigned) __cvta_generic_to_shared (sa);
+  const int nblk = (nrelax + S - 1)/S;
+  const int up = rank > 0 ? rank - 1 : (px ? C - 1 : -1);
+  const int dn = rank < C - 1 ? rank + 1 : (px ? 0 : -1);
+  grid_dependency_wait ();
+
+  for (int blk = 0; blk < nblk; blk++) {
+    const int ks = nrelax - blk*S < S ? nrelax - blk*S : S;
+    if (blk == 0) {
+      double v8[8];
+      if (rowok) {
+        const int ci = ri >> 1, cx = (ri & 1) ? 1 : -1, cj0 = (q0 >> 1) - 1;
+        const long long b0 = cidx<2> (gc, ci, cj0, 0), b1 = cidx<2> (gc, ci + cx, cj0, 0);
+        double r0[6], r1[6];
+#pragma unroll
+        for (int u = 0; u < 6; u++) { r0[u] = coarse[b0 + u]; r1[u] = coarse[b1 + u]; }
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+          const int u = 1 + (q >> 1), cy = (q & 1) ? 1 : -1;
+          v8[q] = (9.*r0[u] + 3.*(r1[u] + r0[u + cy]) + r1[u + cy])/16.;
+        }
+      }
+      else
+#pragma unroll
+        for (int q = 0; q < 8; q++) v8[q] = 0.;
+      double * se = sa + ce*SAW + p*MP + OFS + m0, * so = sa + (ce ^ 1)*SAW + p*MP + OFS + m0;
+      *(double2 *) se = make_double2 (v8[0], v8[2]); *(double2 *) (se + 2) = make_double2 (v8[4], v8[6]);
+      *(double2 *) so = make_double2 (v8[1], v8[3]); *(double2 *) (so + 2) = make_double2 (v8[5], v8[7]);
+    }
+    else {
+      const int src = (blk - 1) & 1;
+      int u = rank, r = p - H;
+      if (p < H) { u = up; r = R - H + p; }
+      else if (p >= H + R) { u = dn; r = p - H - R; }
+      const double * ob = own + src*2*OWW;
+      const double * q = u < 0 ? NULL : (u == rank ? ob : cluster_map (ob, (unsigned) u));
+#pragma unroll
+      for (int c = 0; c < 2; c++) {
+        double2 v0 = make_double2 (0., 0.), v1 = v0;
+        if (q) {
+          v0 = *(const double2 *) (q + c*OWW + r*MP + OFS + m0);
+          v1 = *(const double2 *) (q + c*OWW + r*MP + OFS + m0 + 2);
+        }
+        *(double2 *) (sa + c*SAW + p*MP + OFS + m0) = v0;
+        *(double2 *) (sa + c*SAW + p*MP + OFS + m0 + 2) = v1;
+      }
+    }
+    __syncthreads ();
+    stage_ghosts ();
+    __syncthreads ();
+
+    for (int sw = 0; sw < ks; sw++)
+#pragma unroll
+      for (int c = 0; c < 2; c++) {
+        const int k = 2*sw + c;
+        if (rowok && p >= k + 1 && p < BYR - k - 1) {
+          const int o = c ^ ce;
+          const unsigned aup = sbase + 8u*((c ^ 1)*SAW + (p - 1)*MP + OFS + m0);
+          const double2 u0 = lds_d2<0> (aup), u1 = lds_d2<16> (aup);
+          const double2 mA = lds_d2<8*MP> (aup), mB = lds_d2<8*MP + 16> (aup);
+          const double2 d0 = lds_d2<16*MP> (aup), d1 = lds_d2<16*MP + 16> (aup);
+          double v[5];
+          if (o == 0) { v[0] = lds_d1<8*MP - 8> (aup); v[1] = mA.x; v[2] = mA.y; v[3] = mB.x; v[4] = mB.y; }
+          else { v[0] = mA.x; v[1] = mA.y; v[2] = mB.x; v[3] = mB.y; v[4] = lds_d1<8*MP + 32> (aup); }
+          const double upv[4] = {u0.x, u0.y, u1.x, u1.y}, dnv[4] = {d0.x, d0.y, d1.x, d1.y};
+          double nv[4];
+#pragma unroll
+          for (int e = 0; e < 4; e++) {
+            /* relax_value's expression and order (poisson.h:303-319) */
+            double d = LAM ? cdl[c][LAM ? e : 0] : dlc;
+            d += cxu[c][e] + cxl[c][e];
+            d += cyr[c][e] + cyl[c][e];
+            double nn = cnb[c][e] + (cxu[c][e]*dnv[e] + cxl[c][e]*upv[e]);
+            nn = nn + (cyr[c][e]*v[e + 1] + cyl[c][e]*v[e]);
+            nv[e] = nn/d;
+          }
+          const unsigned aw = sbase + 8u*(c*SAW + p*MP + OFS + m0);
+          sts_d2 (aw, make_double2 (nv[0], nv[1]));
+          sts_d2 (aw + 16, make_double2 (nv[2], nv[3]));
+          put_ghosts (c, nv);
+        }
+        __syncthreads ();
+      }
+    if (p >= H && p < H + R) {
+      double * ob = own + (blk & 1)*2*OWW;
+#pragma unroll
+      for (int c = 0; c < 2; c++) {
+        *(double2 *) (ob + c*OWW + (p - H)*MP + OFS + m0) =
+          *(const double2 *) (sa + c*SAW + p*MP + OFS + m0);
+        *(double2 *) (ob + c*OWW + (p - H)*MP + OFS + m0 + 2) =
+          *(const double2 *) (sa + c*SAW + p*MP + OFS + m0 + 2);
+      }
+    }
+    cluster_barrier ();
+  }
+
+  if (p >= H && p < H + R) {
+    const double * se = sa + ce*SAW + p*MP + OFS + m0, * so = sa + (ce ^ 1)*SAW + p*MP + OFS + m0;
+    const double v8[8] = {se[0], so[0], se[1], so[1], se[2], so[2], se[3], so[3]};
+    double * o8 = out + cidx<2> (g, gi, q0, 0);
+    *(double2 *) o8 = make_double2 (v8[0], v8[1]); *(double2 *) (o8 + 2) = make_double2 (v8[2], v8[3]);
+    *(double2 *) (o8 + 4) = make_double2 (v8[4], v8[5]); *(double2 *) (o8 + 6) = make_double2 (v8[6], v8[7]);
+    if (gi == 0 || gi == N - 1 || q0 == 0 || q0 + 8 == N)
+#pragma unroll
+      for (int q = 0; q < 8; q++)
+        ghosts_homog<2, double> (out, g, gi, q0 + q, 0, v8[q], bc);
+  }
+}
+
+template <int N, int C, bool LAM>
+int launch_level_cluster_x (bmg_geom g, double * out, const double * res, const bmg_coef * alpha,
+                            bmg_coef lambda, double Delta, BCH h, int nrelax, bmg_geom gc,
+                            const double * coarse, cudaStream_t s)
+{
+  typedef clx::Shape<N, C> Sh;
+  auto kern = k_level_cluster_x<N, C, LAM>;
+  static int ok[64];
+  int dev = 0;
+  cudaGetDevice (&dev);
+  if (dev < 0 || dev >= 64) return (int) cudaErrorInvalidDevice;
+  cudaLaunchConfig_t cfg;
+  memset (&cfg, 0, sizeof cfg);
+  cfg.gridDim = dim3 (C, 1, 1);
+  cfg.blockDim = dim3 (Sh::BX, Sh::BYR, 1);
+  cfg.dynamicSmemBytes = Sh::bytes;
+  cfg.stream = s;
+  cudaLaunchAttribute at[2];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = C; at[0].val.clusterDim.y = 1; at[0].val.clusterDim.z = 1;
+  at[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[1].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 2;
+  if (!ok[dev]) {
+    cudaError_t e = cudaFuncSetAttribute (kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) Sh::bytes);
+    if (e == cudaSuccess && C > 8)
+      e = cudaFuncSetAttribute (kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    int nc = 0;
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveClusters (&nc, kern, &cfg);
+    cudaGetLastError ();
+    ok[dev] = e == cudaSuccess && nc >= 1 ? 1 : -1;
+  }
+  if (ok[dev] < 0) return -1;
+  return (int) cudaLaunchKernelEx (&cfg, kern, g, out, res, coef_of<double> (alpha[0]),
+                                   coef_of<double> (alpha[1]), coef_of<double> (lambda),
+                                   Delta, h, nrelax, gc, coarse);
+}
+
 template <bool LAM>
 int launch_tile_x4 (bmg_geom g, void * out, const void * in, const void * res,
                     const bmg_coef * alpha, bmg_coef lambda, double Delta, BCH h, int nsweeps,
@@ -2062,15 +2345,29 @@ int bmg_launch_relax_tile (int dim, int st, bmg_geom g, void * out, const void *
 
 int bmg_level_cluster_ok (int st, int n)
 {
-  return st == BMG_ST_F32 && (n == 64 || n == 128 || n == 256);
+  if (st == BMG_ST_F64) return n == 64 || n == 128;
+  return n == 64 || n == 128 || n == 256;
 }
 
-int bmg_launch_level_cluster (bmg_geom g, void * out, const void * res, const bmg_coef * alpha,
-                              bmg_coef lambda, double Delta, const bmg_bcdesc * bc, int nrelax,
-                              bmg_geom gc, const void * coarse, cudaStream_t s)
+int bmg_launch_level_cluster (int st, bmg_geom g, void * out, const void * res,
+                              const bmg_coef * alpha, bmg_coef lambda, double Delta,
+                              const bmg_bcdesc * bc, int nrelax, bmg_geom gc, const void * coarse,
+                              cudaStream_t s)
 {
-  if (nrelax < 1 || !bmg_level_cluster_ok (BMG_ST_F32, g.n)) return -1;
+  if (nrelax < 1 || !bmg_level_cluster_ok (st, g.n)) return -1;
   BCH h = bch_of (bc);
+  if (st == BMG_ST_F64) {
+    double * o = (double *) out;
+    const double * r = (const double *) res, * c = (const double *) coarse;
+    int e = g.n == 128 ?
+      (lambda.p ? launch_level_cluster_x<128, 16, true> (g, o, r, alpha, lambda, Delta, h, nrelax, gc, c, s)
+                : launch_level_cluster_x<128, 16, false> (g, o, r, alpha, lambda, Delta, h, nrelax, gc, c, s))
+      : lambda.p ? launch_level_cluster_x<64, 8, true> (g, o, r, alpha, lambda, Delta, h, nrelax, gc, c, s)
+      : launch_level_cluster_x<64, 8, false> (g, o, r, alpha, lambda, Delta, h, nrelax, gc, c, s);
+    if (e) return e;
+    cudaError_t q = cudaGetLastError ();
+    return q == cudaSuccess ? 0 : (int) q;
+  }
   float * o = (float *) out;
   const float * r = (const float *) res, * c = (const float *) coarse;
   int e;

@@ -816,14 +816,14 @@ static int bottom_top (const bmg_grid * g, const levels_t * lv, const coefs_t * 
 }
 
 /* whether level l of a cycle is relaxed by the cluster level kernel: a
-   128^2 or 256^2 (or, below the tile levels, 64^2) FP32 level of the mixed
-   form's red-black cycle above minlevel, whose coarse level is FP32 too;
-   not the finest level while its sweeps are being timed */
+   level of a red-black 2D cycle above minlevel that has such a kernel in
+   its storage type (FP32: 64^2 to 256^2; FP64: 64^2 and 128^2), whose
+   coarse level has the same storage type; not the finest level while its
+   sweeps are being timed */
 static int use_cluster (const bmg_grid * g, const levels_t * lv, int l, int minlevel, int maxlevel)
 {
   return g->cluster_levels && g->relax == BMG_RELAX_RBGS && g->dim == 2 && l > minlevel &&
-    lv->st[l] == BMG_ST_F32 && lv->st[l - 1] == BMG_ST_F32 &&
-    bmg_level_cluster_ok (BMG_ST_F32, 1 << l) &&
+    lv->st[l] == lv->st[l - 1] && bmg_level_cluster_ok (lv->st[l], 1 << l) &&
     !(g->timing && l == g->depth && maxlevel == g->depth);
 }
 
@@ -889,9 +889,11 @@ static int cycle_launches (bmg_grid * g, field_t * a, const levels_t * lv, const
     /* a middle level of the mixed form: prolongation and all nrelax sweeps
        in one thread-block cluster (falls through when it does not apply) */
     if (use_cluster (g, lv, l, minlevel, maxlevel)) {
-      const int e = bmg_launch_level_cluster (gl, lv->da[l], lv->res[l], c->alpha32[l],
-                                              c->lambda32[l], delta_of (g, l), dabc, nrelax,
-                                              geom_st (g, l - 1, BMG_ST_F32), cur[l - 1], s);
+      const int e = bmg_launch_level_cluster (st, gl, lv->da[l], lv->res[l],
+                                              st == BMG_ST_F64 ? c->alpha64[l] : c->alpha32[l],
+                                              st == BMG_ST_F64 ? c->lambda64[l] : c->lambda32[l],
+                                              delta_of (g, l), dabc, nrelax,
+                                              geom_st (g, l - 1, st), cur[l - 1], s);
       if (e > 0) CL (e);
       if (e == 0) {
         bytes += ncells (g, l - 1)*es_of (BMG_ST_F32) + ncells (g, l)*es_of (st);

@@ -134,16 +134,18 @@ int bmg_launch_relax_tile (int dim, int st, bmg_geom g, void * out, const void *
                            double Delta, const bmg_bcdesc * bc, int nsweeps, double * acor,
                            bmg_geom ga, const bmg_bcdesc * abc, cudaStream_t s);
 
-/* all nrelax red-black sweeps of a 128^2 or 256^2 FP32 2D level in one
-   launch of one thread-block cluster, the bilinear prolongation of coarse
-   (FP32, the level below, ghosts included) fused in; the final iterate,
-   with its ghost images, goes to out.  bmg_level_cluster_ok () tells
-   whether a level has such a kernel.  Returns 0, -1 when the device cannot
-   schedule the cluster (use tile launches), or a CUDA error. */
+/* all nrelax red-black sweeps of a 2D level (FP32: 64^2 to 256^2; FP64,
+   bit-identical: 64^2 and 128^2) in one launch of one thread-block
+   cluster, the bilinear prolongation of coarse (the level below, same
+   storage type, ghosts included) fused in; the final iterate, with its
+   ghost images, goes to out.  bmg_level_cluster_ok () tells whether a
+   level has such a kernel.  Returns 0, -1 when the device cannot schedule
+   the cluster (use tile launches), or a CUDA error. */
 int bmg_level_cluster_ok (int st, int n);
-int bmg_launch_level_cluster (bmg_geom g, void * out, const void * res, const bmg_coef * alpha,
-                              bmg_coef lambda, double Delta, const bmg_bcdesc * bc, int nrelax,
-                              bmg_geom gc, const void * coarse, cudaStream_t s);
+int bmg_launch_level_cluster (int st, bmg_geom g, void * out, const void * res,
+                              const bmg_coef * alpha, bmg_coef lambda, double Delta,
+                              const bmg_bcdesc * bc, int nrelax, bmg_geom gc, const void * coarse,
+                              cudaStream_t s);
 
 /* one level of the single-CTA bottom solve */
 typedef struct {

@@ -83,3 +83,36 @@ def test_cluster_level_finest(depth):
     st, at, _ = solve_mixed(prob, False, 1e-6)
     assert sp["resa"] <= 1e-6 and abs(sp["i"] - st["i"]) <= 2, (sp, st)
     assert np.abs(ap - at).max() <= 1e-3 * np.abs(at).max()
+
+
+def solve_fp64(prob, cluster, tol):
+    from helpers import gpu_grid
+    if not cluster:
+        os.environ["BMG_NO_CLUSTER"] = "1"
+    try:
+        g, a, b, alpha, lam = gpu_grid(prob, relax="rbgs")
+    finally:
+        os.environ.pop("BMG_NO_CLUSTER", None)
+    st = g.poisson(a, b, alpha=alpha, lambda_=lam, tolerance=tol)
+    sol = a.get()
+    g.close()
+    return st, sol
+
+
+@pytest.mark.parametrize("name", ["two_phase_512", "periodic_256", "neumann_lambda_field_512",
+                                  "mixed_bc_128"])
+def test_fp64_cluster_levels_bit_identical(name):
+    """The plain FP64 form's cluster kernel (64^2 and 128^2 levels, relax_value's
+    order with the IEEE division) gives the tile / single-CTA path's solve and
+    the oracle's bit for bit."""
+    from helpers import oracle_grid
+    prob = cases()[name]
+    sc, ac = solve_fp64(prob, True, 1e-8)
+    st, at = solve_fp64(prob, False, 1e-8)
+    for k in ("i", "nrelax", "resb", "resa"):
+        assert sc[k] == st[k], (k, sc, st)
+    assert np.array_equal(ac, at)
+    o = oracle_grid(prob, relax=oracle.RELAX_RBGS, threads=os.cpu_count() or 1)
+    so = o.poisson(tolerance=1e-8)
+    assert so["i"] == sc["i"] and so["resa"] == sc["resa"], (so, sc)
+    assert np.array_equal(o.get_a(), ac)
