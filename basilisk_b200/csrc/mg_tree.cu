@@ -15,6 +15,7 @@
  */
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <string.h>
 #include "basilisk_mg.h"
 #include "mg_device.cuh"
 #include "mg_tree.h"
@@ -43,6 +44,15 @@ __device__ __forceinline__ double coef (const bmg_tree_coef & c, long long id)
   return c.p ? c.p[id] : c.c;
 }
 
+/* a field value: a plain load in the one-operation kernels, an L2 load
+   (ld.global.cg) in the interpreter, whose fields other CTAs write during
+   the launch (L1 is not coherent across SMs) */
+template <bool CG>
+__device__ __forceinline__ double ldf (const double * p)
+{
+  return CG ? __ldcg (p) : *p;
+}
+
 #define GRID_STRIDE(k, n) \
   for (long k = (long) blockIdx.x*blockDim.x + threadIdx.x; k < (n); k += (long) gridDim.x*blockDim.x)
 
@@ -59,14 +69,15 @@ __global__ void k_set (const uint32_t * __restrict__ list, long n, TL T, double 
 
 /* bilinear (multigrid-common.h:124-140) of child (i, j) of level l from
    level l - 1 */
+template <bool CG = false>
 __device__ __forceinline__ double bilinear (const TL & T, const double * s, int l, int i, int j)
 {
   const int pi = i >> 1, pj = j >> 1, cx = (i & 1) ? 1 : -1, cy = (j & 1) ? 1 : -1;
   const double * c = s + T.off[l - 1];
   const bmg_geom & gc = T.g[l - 1];
-  return (9.*c[cidx<2> (gc, pi, pj, 0)] +
-          3.*(c[cidx<2> (gc, pi + cx, pj, 0)] + c[cidx<2> (gc, pi, pj + cy, 0)]) +
-          c[cidx<2> (gc, pi + cx, pj + cy, 0)])/16.;
+  return (9.*ldf<CG> (c + cidx<2> (gc, pi, pj, 0)) +
+          3.*(ldf<CG> (c + cidx<2> (gc, pi + cx, pj, 0)) + ldf<CG> (c + cidx<2> (gc, pi, pj + cy, 0))) +
+          ldf<CG> (c + cidx<2> (gc, pi + cx, pj + cy, 0)))/16.;
 }
 
 /* foreach_level (l) s[] = bilinear (point, s) (poisson.h:64-68) */
@@ -83,12 +94,13 @@ __global__ void k_prolong (const uint32_t * __restrict__ list, long n, TL T, dou
 
 /* refine_bilinear of the halo children of prolongation leaves: one thread
    per child */
+template <bool CG = false>
 __device__ __forceinline__ void halo_child (const uint32_t * list, long k, const TL & T, double * s)
 {
   int l, i, j;
   unpack (list[k >> 2], l, i, j);
   const int ci = 2*i + (int) ((k >> 1) & 1), cj = 2*j + (int) (k & 1);
-  s[gidx (T, l + 1, ci, cj)] = bilinear (T, s, l + 1, ci, cj);
+  s[gidx (T, l + 1, ci, cj)] = bilinear<CG> (T, s, l + 1, ci, cj);
 }
 
 __global__ void k_halo (const uint32_t * __restrict__ list, long n, TL T, double * s)
@@ -101,6 +113,7 @@ __global__ void k_halo (const uint32_t * __restrict__ list, long n, TL T, double
 
 /* restriction_average (multigrid-common.h:26-32), children in foreach_child
    order */
+template <bool CG = false>
 __device__ __forceinline__ void restrict_cell (const uint32_t * list, long k, const TL & T, double * s)
 {
   int l, i, j;
@@ -108,10 +121,10 @@ __device__ __forceinline__ void restrict_cell (const uint32_t * list, long k, co
   const double * f = s + T.off[l + 1];
   const bmg_geom & gf = T.g[l + 1];
   double sum = 0.;
-  sum += f[cidx<2> (gf, 2*i, 2*j, 0)];
-  sum += f[cidx<2> (gf, 2*i, 2*j + 1, 0)];
-  sum += f[cidx<2> (gf, 2*i + 1, 2*j, 0)];
-  sum += f[cidx<2> (gf, 2*i + 1, 2*j + 1, 0)];
+  sum += ldf<CG> (f + cidx<2> (gf, 2*i, 2*j, 0));
+  sum += ldf<CG> (f + cidx<2> (gf, 2*i, 2*j + 1, 0));
+  sum += ldf<CG> (f + cidx<2> (gf, 2*i + 1, 2*j, 0));
+  sum += ldf<CG> (f + cidx<2> (gf, 2*i + 1, 2*j + 1, 0));
   s[gidx (T, l, i, j)] = sum/(1 << 2);
 }
 
@@ -167,6 +180,7 @@ __device__ __forceinline__ double bc_of (const bmg_tree_bc & bc, int side, int l
   return homog ? sn : Delta*val + sn;
 }
 
+template <bool CG = false>
 __device__ __forceinline__ void ghost_value (const bmg_tree_rule & r, const TL & T, double * s,
                                              const bmg_tree_bc & bc, int homog)
 {
@@ -174,7 +188,7 @@ __device__ __forceinline__ void ghost_value (const bmg_tree_rule & r, const TL &
   unpack (r.ghost, l, gi, gj);
   unpack (r.inner, l2, a, b);
   const long long nid = gidx (T, l, a, b);
-  const double sn = s[nid], D = T.Delta[l];
+  const double sn = ldf<CG> (s + nid), D = T.Delta[l];
   const int s1 = r.kind_sides & 15, s2 = (r.kind_sides >> 4) & 15, kind = r.kind_sides >> 8;
   const int t1 = r.tidx & 0xFFFF, t2 = r.tidx >> 16;
   double v = bc_of (bc, s1, l, t1, sn, D, homog);
@@ -209,27 +223,36 @@ __global__ void k_stage (const uint32_t * __restrict__ list, long n, int op,
   }
 }
 
-/* relax (poisson.h:303-320); x is the first index (stride P), y the second */
+/* relax (poisson.h:303-320) of one listed cell; x is the first index
+   (stride P), y the second */
+template <bool CG = false>
+__device__ __forceinline__ void relax_item (uint32_t e, const TL & T, const double * a,
+                                            const double * b, const bmg_tree_coef & ax,
+                                            const bmg_tree_coef & ay, const bmg_tree_coef & lam,
+                                            double * out)
+{
+  int l, i, j;
+  unpack (e, l, i, j);
+  const long long id = gidx (T, l, i, j), P = T.g[l].P;
+  const double Delta = T.Delta[l];
+  double nn = - (Delta*Delta)*ldf<CG> (b + id), d = - coef (lam, id)*(Delta*Delta);
+  const double x1 = coef (ax, id + P), x0 = coef (ax, id);
+  nn += x1*ldf<CG> (a + id + P) + x0*ldf<CG> (a + id - P);
+  d += x1 + x0;
+  const double y1 = coef (ay, id + 1), y0 = coef (ay, id);
+  nn += y1*ldf<CG> (a + id + 1) + y0*ldf<CG> (a + id - 1);
+  d += y1 + y0;
+  out[id] = nn/d;
+}
+
 __global__ void k_relax (const uint32_t * __restrict__ list, long n, TL T,
                          const double * a, const double * __restrict__ b,
                          bmg_tree_coef ax, bmg_tree_coef ay, bmg_tree_coef lam, double * out)
 {
   pdl_wait ();
   pdl_trigger ();
-  GRID_STRIDE (k, n) {
-    int l, i, j;
-    unpack (list[k], l, i, j);
-    const long long id = gidx (T, l, i, j), P = T.g[l].P;
-    const double Delta = T.Delta[l];
-    double nn = - (Delta*Delta)*b[id], d = - coef (lam, id)*(Delta*Delta);
-    const double x1 = coef (ax, id + P), x0 = coef (ax, id);
-    nn += x1*a[id + P] + x0*a[id - P];
-    d += x1 + x0;
-    const double y1 = coef (ay, id + 1), y0 = coef (ay, id);
-    nn += y1*a[id + 1] + y0*a[id - 1];
-    d += y1 + y0;
-    out[id] = nn/d;
-  }
+  GRID_STRIDE (k, n)
+    relax_item (list[k], T, a, b, ax, ay, lam, out);
 }
 
 /* weighted Jacobi (poisson.h:325-328) */
@@ -247,18 +270,20 @@ __global__ void k_jacobi (const uint32_t * __restrict__ list, long n, TL T, doub
 }
 
 /* g.x = alpha.x face_gradient_x (a, 0) on the left face of (i, j) */
+template <bool CG = false>
 __device__ __forceinline__ double gx (const TL & T, const double * a, const bmg_tree_coef & ax,
                                       int l, int i, int j)
 {
   const long long id = gidx (T, l, i, j);
-  return coef (ax, id)*((a[id] - a[id - T.g[l].P])/T.Delta[l]);
+  return coef (ax, id)*((ldf<CG> (a + id) - ldf<CG> (a + id - T.g[l].P))/T.Delta[l]);
 }
 
+template <bool CG = false>
 __device__ __forceinline__ double gy (const TL & T, const double * a, const bmg_tree_coef & ay,
                                       int l, int i, int j)
 {
   const long long id = gidx (T, l, i, j);
-  return coef (ay, id)*((a[id] - a[id - 1])/T.Delta[l]);
+  return coef (ay, id)*((ldf<CG> (a + id) - ldf<CG> (a + id - 1))/T.Delta[l]);
 }
 
 /* atomicMax on the bits of a non-negative double (NaN sorts above inf) */
@@ -269,6 +294,35 @@ __device__ __forceinline__ void max_bits (unsigned long long * m, double v)
 
 /* residual, tree branch (poisson.h:355-372): a leaf face shared with a
    refined neighbour carries the mean of the two fine fluxes (halo_face) */
+template <bool CG = false>
+__device__ __forceinline__ double residual_item (uint32_t e, const TL & T, const unsigned char * fl,
+                                                 const double * a, const double * b,
+                                                 const bmg_tree_coef & ax, const bmg_tree_coef & ay,
+                                                 const bmg_tree_coef & lam, double * res)
+{
+  int l, i, j;
+  unpack (e, l, i, j);
+  const long long id = gidx (T, l, i, j);
+  const double Delta = T.Delta[l];
+  const double gl = refined_at (T, fl, l, i - 1, j) ?
+    (gx<CG> (T, a, ax, l + 1, 2*i, 2*j) + gx<CG> (T, a, ax, l + 1, 2*i, 2*j + 1))/2. :
+    gx<CG> (T, a, ax, l, i, j);
+  const double gr = refined_at (T, fl, l, i + 1, j) ?
+    (gx<CG> (T, a, ax, l + 1, 2*i + 2, 2*j) + gx<CG> (T, a, ax, l + 1, 2*i + 2, 2*j + 1))/2. :
+    gx<CG> (T, a, ax, l, i + 1, j);
+  const double gb = refined_at (T, fl, l, i, j - 1) ?
+    (gy<CG> (T, a, ay, l + 1, 2*i, 2*j) + gy<CG> (T, a, ay, l + 1, 2*i + 1, 2*j))/2. :
+    gy<CG> (T, a, ay, l, i, j);
+  const double gt = refined_at (T, fl, l, i, j + 1) ?
+    (gy<CG> (T, a, ay, l + 1, 2*i, 2*j + 2) + gy<CG> (T, a, ay, l + 1, 2*i + 1, 2*j + 2))/2. :
+    gy<CG> (T, a, ay, l, i, j + 1);
+  double r = b[id] - coef (lam, id)*ldf<CG> (a + id);
+  r -= (gr - gl)/Delta;
+  r -= (gt - gb)/Delta;
+  res[id] = r;
+  return r;
+}
+
 __global__ void k_residual (const uint32_t * __restrict__ list, long n, TL T,
                             const unsigned char * __restrict__ fl, const double * __restrict__ a,
                             const double * __restrict__ b, bmg_tree_coef ax, bmg_tree_coef ay,
@@ -278,25 +332,7 @@ __global__ void k_residual (const uint32_t * __restrict__ list, long n, TL T,
   pdl_trigger ();
   double m = 0.;
   GRID_STRIDE (k, n) {
-    int l, i, j;
-    unpack (list[k], l, i, j);
-    const long long id = gidx (T, l, i, j);
-    const double Delta = T.Delta[l];
-    const double gl = refined_at (T, fl, l, i - 1, j) ?
-      (gx (T, a, ax, l + 1, 2*i, 2*j) + gx (T, a, ax, l + 1, 2*i, 2*j + 1))/2. : gx (T, a, ax, l, i, j);
-    const double gr = refined_at (T, fl, l, i + 1, j) ?
-      (gx (T, a, ax, l + 1, 2*i + 2, 2*j) + gx (T, a, ax, l + 1, 2*i + 2, 2*j + 1))/2. :
-      gx (T, a, ax, l, i + 1, j);
-    const double gb = refined_at (T, fl, l, i, j - 1) ?
-      (gy (T, a, ay, l + 1, 2*i, 2*j) + gy (T, a, ay, l + 1, 2*i + 1, 2*j))/2. : gy (T, a, ay, l, i, j);
-    const double gt = refined_at (T, fl, l, i, j + 1) ?
-      (gy (T, a, ay, l + 1, 2*i, 2*j + 2) + gy (T, a, ay, l + 1, 2*i + 1, 2*j + 2))/2. :
-      gy (T, a, ay, l, i, j + 1);
-    double r = b[id] - coef (lam, id)*a[id];
-    r -= (gr - gl)/Delta;
-    r -= (gt - gb)/Delta;
-    res[id] = r;
-    const double ar = fabs (r);
+    const double ar = fabs (residual_item (list[k], T, fl, a, b, ax, ay, lam, res));
     if (m == m && !(ar <= m)) m = ar;       /* a NaN sticks */
   }
   /* warp maximum, then one atomic per warp */
@@ -355,6 +391,164 @@ __global__ void k_sum_final (const double * __restrict__ partials, int np, doubl
     __syncthreads ();
   }
   if (threadIdx.x == 0) *out = sh[0];
+}
+
+/* ---------------------------------------------------------------- */
+/* the schedule interpreter                                          */
+/* ---------------------------------------------------------------- */
+
+/* One mg_solve iteration on a tree (the cycle and the residual) is a fixed
+   sequence of a few thousand small list operations, each of which depends
+   on the one before.  k_tree_interp runs such a sequence (bmg_tree_op
+   records, built on the host in the order of the launches they replace)
+   in one launch of one thread-block cluster: every operation's items are
+   spread over the cluster's threads, and the cluster barrier
+   (release/acquire at cluster scope) separates an operation from the next;
+   field values are loaded from L2, since other CTAs of the cluster wrote
+   them.  Every item is computed by the function the one-operation kernel
+   uses, so the results are bit-identical.  The residual's maximum is
+   reduced per warp into maxres (zeroed before the launch). */
+template <int C>
+__global__ void __launch_bounds__ (1024, 1)
+k_tree_interp (const bmg_tree_op * __restrict__ ops, int nops, TL Tp, double * fa, double * fda,
+               double * fres, double * ftmp, const double * __restrict__ b,
+               const unsigned char * __restrict__ fl, bmg_tree_coef ax, bmg_tree_coef ay,
+               bmg_tree_coef lam, bmg_tree_bc bc0, bmg_tree_bc bc1, unsigned long long * maxres)
+{
+  constexpr int CH = 256;                       /* operations staged per chunk */
+  __shared__ TL T;
+  __shared__ bmg_tree_bc B[2];
+  __shared__ bmg_tree_op sops[CH];
+  if (threadIdx.x == 0) { T = Tp; B[0] = bc0; B[1] = bc1; }
+  unsigned rank;
+  asm volatile ("mov.u32 %0, %%cluster_ctarank;" : "=r"(rank));
+  const long gt = (long) rank*blockDim.x + threadIdx.x, gs = (long) C*blockDim.x;
+  double * const F[4] = {fa, fda, fres, ftmp};
+  double m = 0.;
+  /* the list entry of the thread's first item of the current operation,
+     loaded while the previous one waited at the barrier */
+  uint32_t first = 0;
+  for (int o = 0; o < nops; o++) {
+    if (o % CH == 0) {
+      /* the next chunk of operations into shared memory (after the
+         barrier that ended the last chunk's operation) */
+      __syncthreads ();
+      const int nc = nops - o < CH ? nops - o : CH;
+      const int words = nc*(int) (sizeof (bmg_tree_op)/8);
+      const unsigned long long * src = (const unsigned long long *) (ops + o);
+      unsigned long long * dst = (unsigned long long *) sops;
+      for (int w = threadIdx.x; w < words; w += blockDim.x) dst[w] = src[w];
+      __syncthreads ();
+      if (gt < sops[0].n && sops[0].list) first = sops[0].list[gt];
+    }
+    const bmg_tree_op & op = sops[o % CH];
+    double * s = F[op.field];
+    const uint32_t * list = op.list;
+#define ENTRY(k) ((k) == gt ? first : list[k])
+    switch (op.type) {
+    case BMG_TI_SET:
+      for (long k = gt; k < op.n; k += gs) {
+        int l, i, j;
+        unpack (ENTRY (k), l, i, j);
+        s[gidx (T, l, i, j)] = op.v;
+      }
+      break;
+    case BMG_TI_PROLONG:
+      for (long k = gt; k < op.n; k += gs) {
+        int l, i, j;
+        unpack (ENTRY (k), l, i, j);
+        s[gidx (T, l, i, j)] = bilinear<true> (T, s, l, i, j);
+      }
+      break;
+    case BMG_TI_RESTRICT:
+      for (long k = gt; k < op.n; k += gs)
+        restrict_cell<true> (list, k, T, s);
+      break;
+    case BMG_TI_STAGE: {
+      const long w = op.sub == BMG_T_OP_HALO ? 4*op.n : op.sub == BMG_T_OP_RESTRICT ? op.n : 0;
+      for (long k = gt; k < w + op.nr; k += gs) {
+        if (k >= w) ghost_value<true> (op.rules[k - w], T, s, B[op.bcsel], op.homog);
+        else if (op.sub == BMG_T_OP_HALO) halo_child<true> (list, k, T, s);
+        else restrict_cell<true> (list, k, T, s);
+      }
+      break;
+    }
+    case BMG_TI_RELAX:
+      for (long k = gt; k < op.n; k += gs)
+        relax_item<true> (ENTRY (k), T, fda, fres, ax, ay, lam, op.sub ? ftmp : fda);
+      break;
+    case BMG_TI_JACOBI:
+      for (long k = gt; k < op.n; k += gs) {
+        int l, i, j;
+        unpack (ENTRY (k), l, i, j);
+        const long long id = gidx (T, l, i, j);
+        fda[id] = (ldf<true> (fda + id) + 2.*ldf<true> (ftmp + id))/3.;
+      }
+      break;
+    case BMG_TI_ADD:
+      for (long k = gt; k < op.n; k += gs) {
+        int l, i, j;
+        unpack (ENTRY (k), l, i, j);
+        const long long id = gidx (T, l, i, j);
+        fa[id] = ldf<true> (fa + id) + ldf<true> (fda + id);
+      }
+      break;
+    case BMG_TI_RESIDUAL:
+      for (long k = gt; k < op.n; k += gs) {
+        const double ar = fabs (residual_item<true> (ENTRY (k), T, fl, fa, b, ax, ay, lam, fres));
+        if (m == m && !(ar <= m)) m = ar;   /* a NaN sticks */
+      }
+      break;
+    }
+#undef ENTRY
+    /* the next operation's first list entry of this thread (the lists are
+       constant during the launch), then the barrier */
+    if (o + 1 < nops && (o + 1) % CH != 0) {
+      const bmg_tree_op & nx = sops[(o + 1) % CH];
+      if (gt < nx.n && nx.list) first = nx.list[gt];
+    }
+    asm volatile ("barrier.cluster.arrive.release.aligned;\n"
+                  "barrier.cluster.wait.acquire.aligned;\n" ::: "memory");
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    const double v = __shfl_down_sync (0xffffffffu, m, o);
+    if (m == m && !(v <= m)) m = v;
+  }
+  if ((threadIdx.x & 31) == 0 && m != 0.)
+    max_bits (maxres, m);
+}
+
+template <int C>
+int launch_interp (const bmg_tree_op * ops, int nops, const TL & T, double * const * f,
+                   const double * b, const unsigned char * fl, const bmg_tree_coef * co,
+                   const bmg_tree_bc * bc, unsigned long long * maxres, cudaStream_t st)
+{
+  auto kern = k_tree_interp<C>;
+  static int ok[64];
+  int dev = 0;
+  cudaGetDevice (&dev);
+  if (dev < 0 || dev >= 64) return (int) cudaErrorInvalidDevice;
+  cudaLaunchConfig_t cfg;
+  memset (&cfg, 0, sizeof cfg);
+  cfg.gridDim = dim3 (C, 1, 1);
+  cfg.blockDim = dim3 (1024, 1, 1);
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = C; at[0].val.clusterDim.y = 1; at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  if (!ok[dev]) {
+    cudaError_t e = cudaSuccess;
+    if (C > 8) e = cudaFuncSetAttribute (kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    int nc = 0;
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveClusters (&nc, kern, &cfg);
+    cudaGetLastError ();
+    ok[dev] = e == cudaSuccess && nc >= 1 ? 1 : -1;
+  }
+  if (ok[dev] < 0) return -1;
+  return (int) cudaLaunchKernelEx (&cfg, kern, ops, nops, T, f[0], f[1], f[2], f[3], b, fl,
+                                   co[0], co[1], co[2], bc[0], bc[1], maxres);
 }
 
 const int NT = 256;
@@ -468,6 +662,46 @@ int bmg_tree_launch_add (const uint32_t * leaves, long n, const bmg_tree_levels 
 {
   if (n <= 0) return 0;
   pdl_launch (k_add, dim3 (blocks_for (n)), dim3 (NT), 0, st, leaves, n, *T, a, da);
+  return status ();
+}
+
+int bmg_tree_interp_available (void)
+{
+  /* a cluster of 16 or 8 CTAs of 1024 threads can be scheduled */
+  int dev = 0;
+  if (cudaGetDevice (&dev) != cudaSuccess) { cudaGetLastError (); return 0; }
+  for (int C = 16; C >= 8; C /= 2) {
+    cudaLaunchConfig_t cfg;
+    memset (&cfg, 0, sizeof cfg);
+    cfg.gridDim = dim3 (C, 1, 1);
+    cfg.blockDim = dim3 (1024, 1, 1);
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = C; at[0].val.clusterDim.y = 1; at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    int nc = 0;
+    cudaError_t e = C > 8 ?
+      cudaFuncSetAttribute (k_tree_interp<16>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) :
+      cudaSuccess;
+    if (e == cudaSuccess)
+      e = C > 8 ? cudaOccupancyMaxActiveClusters (&nc, k_tree_interp<16>, &cfg)
+                : cudaOccupancyMaxActiveClusters (&nc, k_tree_interp<8>, &cfg);
+    cudaGetLastError ();
+    if (e == cudaSuccess && nc >= 1) return 1;
+  }
+  return 0;
+}
+
+int bmg_tree_launch_interp (const bmg_tree_op * ops, int nops, const bmg_tree_levels * T,
+                            double * const * fields, const double * b, const unsigned char * flags,
+                            const bmg_tree_coef * coefs, const bmg_tree_bc * bcs,
+                            unsigned long long * maxres, cudaStream_t st)
+{
+  if (nops < 1) return 0;
+  int e = launch_interp<16> (ops, nops, *T, fields, b, flags, coefs, bcs, maxres, st);
+  if (e == -1) e = launch_interp<8> (ops, nops, *T, fields, b, flags, coefs, bcs, maxres, st);
+  if (e) return e;
   return status ();
 }
 

@@ -93,6 +93,33 @@ int bmg_tree_launch_residual (const uint32_t * leaves, long n, const bmg_tree_le
                               double * res, unsigned long long * maxres, cudaStream_t st);
 int bmg_tree_launch_add (const uint32_t * leaves, long n, const bmg_tree_levels * T,
                          double * a, const double * da, cudaStream_t st);
+/* one operation of the schedule interpreter: the one-operation launch it
+   stands for (type), its cell list and ghost rules, the field it works on
+   (0 a, 1 da, 2 res, 3 the Jacobi temporary), the boundary conditions of a
+   ghost rule (bcsel: 0 those of a, 1 those of da) and whether they are
+   homogeneous; sub is a stage's operation, or for a relaxation 1 when it
+   writes the Jacobi temporary; v is the value of a set */
+enum { BMG_TI_SET = 0, BMG_TI_PROLONG, BMG_TI_RESTRICT, BMG_TI_STAGE, BMG_TI_RELAX,
+       BMG_TI_JACOBI, BMG_TI_ADD, BMG_TI_RESIDUAL };
+typedef struct {
+  const uint32_t * list;
+  long long n;
+  const bmg_tree_rule * rules;
+  long long nr;
+  int type, sub, field, bcsel, homog, pad_;
+  double v;
+} bmg_tree_op;
+/* the operations ops[0..nops) in order, in one launch of one thread-block
+   cluster (16 CTAs, or 8 where 16 cannot be scheduled): fields = {a, da,
+   res, tmp}, b the right-hand side, coefs = {alpha_x, alpha_y, lambda},
+   bcs = {those of a, those of da}; the residual operations' maximum goes
+   to maxres */
+int bmg_tree_interp_available (void);
+int bmg_tree_launch_interp (const bmg_tree_op * ops, int nops, const bmg_tree_levels * T,
+                            double * const * fields, const double * b, const unsigned char * flags,
+                            const bmg_tree_coef * coefs, const bmg_tree_bc * bcs,
+                            unsigned long long * maxres, cudaStream_t st);
+
 /* deterministic sum over the listed cells: per-block partials, then one
    block; npartials at most 1024 */
 int bmg_tree_launch_sum (const uint32_t * list, long n, const bmg_tree_levels * T,

@@ -56,6 +56,8 @@ struct tgraph {
   tkey key;
   cudaGraphExec_t exec;
   long long launches;
+  bmg_tree_op * dops;     /* the interpreter's operations of the iteration */
+  long nops;
 };
 
 struct bmg_tree {
@@ -80,6 +82,7 @@ struct bmg_tree {
   int npart;
   struct tgraph graphs[NTGRAPH];
   unsigned long long clock;
+  int interp;                         /* run solve iterations through the interpreter */
 };
 
 #define FAIL(s) bmg_i_fail (s)
@@ -103,11 +106,18 @@ static inline uint32_t pack (int l, int i, int j)
 /* building the tree                                                   */
 /* ------------------------------------------------------------------ */
 
+static void graph_drop (struct tgraph * q)
+{
+  if (q->valid) cudaGraphExecDestroy (q->exec);
+  cudaFree (q->dops);
+  q->dops = NULL; q->nops = 0;
+  q->valid = 0;
+}
+
 static void tree_release (struct bmg_tree * t)
 {
   if (!t) return;
-  for (int i = 0; i < NTGRAPH; i++)
-    if (t->graphs[i].valid) cudaGraphExecDestroy (t->graphs[i].exec);
+  for (int i = 0; i < NTGRAPH; i++) graph_drop (&t->graphs[i]);
   for (int l = 0; l <= TMAX; l++) { free (t->fl[l]); free (t->nb[l]); }
   cudaFree (t->dflags); cudaFree (t->dlist); cudaFree (t->drules); cudaFree (t->dpart);
   cudaFree (t->dsrules);
@@ -125,11 +135,7 @@ void bmg_tree_free (bmg_grid * g)
 void bmg_tree_graphs_clear (bmg_grid * g)
 {
   if (!g || !g->tree) return;
-  for (int i = 0; i < NTGRAPH; i++)
-    if (g->tree->graphs[i].valid) {
-      cudaGraphExecDestroy (g->tree->graphs[i].exec);
-      g->tree->graphs[i].valid = 0;
-    }
+  for (int i = 0; i < NTGRAPH; i++) graph_drop (&g->tree->graphs[i]);
 }
 
 /* refine_cell (tree-common.h:22-55): the leaves among the parent's
@@ -505,6 +511,7 @@ int bmg_tree_refine (bmg_grid * g, bmg_refine_cond cond, void * data)
       if (!t->fl[l] || !t->nb[l]) { tree_release (t); return FAIL (BMG_ENOMEM); }
     }
     t->fl[0][HX (0, 0, 0)] = BMG_T_ACTIVE | BMG_T_LEAF;     /* init_grid (1) */
+    t->interp = getenv ("BMG_NO_TREE_INTERP") == NULL && bmg_tree_interp_available ();
     g->tree = t;
   }
   long count = 0, pass;
@@ -663,6 +670,92 @@ static int t_residual (bmg_grid * g, struct bmg_tree * t, double * a, const doub
   return BMG_OK;
 }
 
+/* ------------------------------------------------------------------ */
+/* the iteration as interpreter operations                             */
+/* ------------------------------------------------------------------ */
+
+/* the same operations, in the same order, as the launches of t_cycle and
+   t_residual (an empty operation, which those skip, is left out) */
+typedef struct { bmg_tree_op * v; long n, cap; int err; } opvec;
+enum { F_A = 0, F_DA = 1, F_RES = 2, F_TMP = 3 };
+
+static void r_push (opvec * o, int type, int field, int sub, int homog, const uint32_t * list,
+                    long n, const bmg_tree_rule * rules, long nr, double v)
+{
+  if (o->err) return;
+  if (o->n == o->cap) {
+    long cap = 2*o->cap + 256;
+    bmg_tree_op * nv = realloc (o->v, cap*sizeof (bmg_tree_op));
+    if (!nv) { o->err = 1; return; }
+    o->v = nv; o->cap = cap;
+  }
+  bmg_tree_op * q = &o->v[o->n++];
+  memset (q, 0, sizeof *q);
+  q->type = type; q->field = field; q->sub = sub; q->homog = homog; q->bcsel = 0;
+  q->list = list; q->n = n; q->rules = rules; q->nr = nr; q->v = v;
+}
+
+static void r_boundary (struct bmg_tree * t, opvec * o, int field, int l, int homog, int kind)
+{
+  if (t->full) {
+    if (t->ghost[l].n)
+      r_push (o, BMG_TI_STAGE, field, BMG_T_OP_NONE, homog, NULL, 0,
+              t->drules + t->ghost[l].off, t->ghost[l].n, 0.);
+    return;
+  }
+  const span_t sp = t->sched[kind][l];
+  for (long k = 0; k < sp.n; k++) {
+    const tstage * sg = &t->stages[sp.off + k];
+    const long w = (sg->op == BMG_T_OP_HALO ? 4*sg->list.n : sg->op == BMG_T_OP_RESTRICT ?
+                    sg->list.n : 0) + sg->rules.n;
+    if (w <= 0) continue;
+    r_push (o, BMG_TI_STAGE, field, sg->op, homog, t->dlist + sg->list.off, sg->list.n,
+            t->dsrules + sg->rules.off, sg->rules.n, 0.);
+  }
+}
+
+static void r_relax (bmg_grid * g, struct bmg_tree * t, opvec * o, int l)
+{
+  const span_t all = t->rl[l];
+  if (g->relax == BMG_RELAX_JACOBI) {
+    if (all.n) {
+      r_push (o, BMG_TI_RELAX, F_DA, 1, 0, t->dlist + all.off, all.n, NULL, 0, 0.);
+      r_push (o, BMG_TI_JACOBI, F_DA, 0, 0, t->dlist + all.off, all.n, NULL, 0, 0.);
+    }
+    return;
+  }
+  const span_t red = {all.off, t->rl1[l]}, black = {all.off + t->rl1[l], all.n - t->rl1[l]};
+  if (red.n) r_push (o, BMG_TI_RELAX, F_DA, 0, 0, t->dlist + red.off, red.n, NULL, 0, 0.);
+  r_boundary (t, o, F_DA, l, 1, SCHED_PRUNED);
+  if (black.n) r_push (o, BMG_TI_RELAX, F_DA, 0, 0, t->dlist + black.off, black.n, NULL, 0, 0.);
+}
+
+static void r_iteration (bmg_grid * g, struct bmg_tree * t, opvec * o, int nrelax, int minlevel,
+                         int maxlevel)
+{
+  for (int m = t->depth - 1; m >= 0; m--)
+    if (t->ref[m].n)
+      r_push (o, BMG_TI_RESTRICT, F_RES, 0, 0, t->dlist + t->ref[m].off, t->ref[m].n, NULL, 0, 0.);
+  for (int l = minlevel; l <= maxlevel; l++) {
+    if (l == minlevel) {
+      if (t->rl[l].n)
+        r_push (o, BMG_TI_SET, F_DA, 0, 0, t->dlist + t->rl[l].off, t->rl[l].n, NULL, 0, 0.);
+    }
+    else if (t->act[l].n)
+      r_push (o, BMG_TI_PROLONG, F_DA, 0, 0, t->dlist + t->act[l].off, t->act[l].n, NULL, 0, 0.);
+    r_boundary (t, o, F_DA, l, 1, SCHED_PRUNED);
+    for (int i = 0; i < nrelax; i++) {
+      r_relax (g, t, o, l);
+      r_boundary (t, o, F_DA, l, 1, SCHED_PRUNED);
+    }
+  }
+  if (t->leaves.n)
+    r_push (o, BMG_TI_ADD, F_A, 0, 0, t->dlist + t->leaves.off, t->leaves.n, NULL, 0, 0.);
+  r_boundary (t, o, F_A, t->depth, 0, SCHED_FULL);
+  if (t->leaves.n)
+    r_push (o, BMG_TI_RESIDUAL, F_RES, 0, 0, t->dlist + t->leaves.off, t->leaves.n, NULL, 0, 0.);
+}
+
 static int read_max (bmg_grid * g, double * m)
 {
   CKT (cudaMemcpyAsync (g->h_pinned, g->d_maxres, sizeof (double), cudaMemcpyDeviceToHost, g->stream));
@@ -692,8 +785,52 @@ static int t_iteration (bmg_grid * g, struct bmg_tree * t, const tkey * key, dou
     if (q->valid && !memcmp (&q->key, key, sizeof *key)) { e = q; break; }
     if (!q->valid || q->stamp < victim->stamp) victim = q;
   }
+  if (!e && t->interp) {
+    /* the iteration as one interpreter launch, its operations uploaded once */
+    graph_drop (victim);
+    opvec o = {NULL, 0, 0, 0};
+    r_iteration (g, t, &o, key->nrelax, key->minlevel, key->maxlevel);
+    if (o.err) { free (o.v); return FAIL (BMG_ENOMEM); }
+    if (cudaMalloc ((void **) &victim->dops, (o.n + 1)*sizeof (bmg_tree_op)) != cudaSuccess ||
+        (o.n && cudaMemcpy (victim->dops, o.v, o.n*sizeof (bmg_tree_op), cudaMemcpyHostToDevice)
+         != cudaSuccess)) {
+      free (o.v);
+      cudaGetLastError ();
+      graph_drop (victim);
+      return FAIL (BMG_ENOMEM);
+    }
+    victim->nops = o.n;
+    free (o.v);
+    double * fields[4] = {a, da, res, tmp};
+    const bmg_tree_coef co[3] = {c->ax, c->ay, c->lam};
+    const bmg_tree_bc bcs[2] = {*abc, *abc};
+    cudaGraph_t graph;
+    CKT (cudaStreamBeginCapture (g->stream, cudaStreamCaptureModeThreadLocal));
+    cudaError_t me = cudaMemsetAsync (g->d_maxres, 0, sizeof (unsigned long long), g->stream);
+    int r = me == cudaSuccess ?
+      bmg_tree_launch_interp (victim->dops, (int) victim->nops, &t->T, fields, b, t->dflags, co,
+                              bcs, g->d_maxres, g->stream) : (int) me;
+    me = cudaMemcpyAsync (g->h_pinned, g->d_maxres, sizeof (double), cudaMemcpyDeviceToHost,
+                          g->stream);
+    cudaError_t ee = cudaStreamEndCapture (g->stream, &graph);
+    if (r) {
+      if (ee == cudaSuccess) cudaGraphDestroy (graph);
+      fprintf (stderr, "bmg: tree interpreter launch failed (%d)\n", r);
+      graph_drop (victim);
+      return FAIL (BMG_ECUDA);
+    }
+    CKT (me);
+    CKT (ee);
+    cudaError_t ie = cudaGraphInstantiate (&victim->exec, graph, 0);
+    cudaGraphDestroy (graph);
+    CKT (ie);
+    victim->key = *key;
+    victim->launches = 1;
+    victim->valid = 1;
+    e = victim;
+  }
   if (!e) {
-    if (victim->valid) { cudaGraphExecDestroy (victim->exec); victim->valid = 0; }
+    graph_drop (victim);
     cudaGraph_t graph;
     CKT (cudaStreamBeginCapture (g->stream, cudaStreamCaptureModeThreadLocal));
     int r = t_cycle (g, t, a, da, res, tmp, c, abc, key->nrelax, key->minlevel, key->maxlevel, nl);

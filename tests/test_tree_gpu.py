@@ -114,3 +114,30 @@ def test_tree_poisson_matches_oracle(relax):
     np.testing.assert_array_equal(leaf_values(tg, ot.A), leaf_values(tc, ot.A))
     for t in made["gpu"]:
         t.close()
+
+
+@pytest.mark.parametrize("relax", ["rbgs", "jacobi"])
+def test_tree_interpreter_matches_launch_path(relax):
+    """poisson () on the band tree with the iterations run by the schedule
+    interpreter (one cluster launch per iteration) and by one launch per
+    operation (the tree is built with BMG_NO_TREE_INTERP set): the same
+    statistics and leaf values bit for bit, with fewer launches."""
+    out = {}
+    for interp in (True, False):
+        if not interp:
+            os.environ["BMG_NO_TREE_INTERP"] = "1"
+        try:
+            t = GpuTree(9, (0.0, 0.0), relax=relax)
+            t.refine(gd.band_refinement(9, 4))
+        finally:
+            os.environ.pop("BMG_NO_TREE_INTERP", None)
+        gd.two_phase_tree(t, seed=11)
+        t.g.reset_counters()
+        st = t.poisson(tolerance=1e-6, nrelax=4, minlevel=1)
+        out[interp] = (st, leaf_values(t, ot.A), t.g.counters())
+        t.close()
+    (si, ai, ci), (sl, al, cl) = out[True], out[False]
+    for k in ("i", "nrelax", "resb", "resa"):
+        assert si[k] == sl[k], (k, si, sl)
+    np.testing.assert_array_equal(ai, al)
+    assert ci["launches"] < cl["launches"], (ci, cl)
