@@ -1208,13 +1208,13 @@ int bmg_poisson (bmg_grid * g, struct Poisson p, mgstats * out)
   if (r) return r;
   r = restrict_coefs (g, &c);
   if (r) return r;
-  /* TOLERANCE override and restore (poisson.h:426-438) */
-  double defaultol = TOLERANCE;
-  if (p.tolerance)
-    TOLERANCE = p.tolerance;
-  r = solve (g, a, b, &c, p.nrelax, res, p.minlevel > 1 ? p.minlevel : 1, 0., out);
-  if (p.tolerance)
-    TOLERANCE = defaultol;
+  /* the reference sets TOLERANCE to p.tolerance for the duration of the
+     solve and restores it (poisson.h:426-438); mg_solve then reads it.
+     Here the solve is given that tolerance directly, which is the same
+     solve and leaves the global untouched, so that solves on different
+     grids can run from different host threads at once. */
+  r = solve (g, a, b, &c, p.nrelax, res, p.minlevel > 1 ? p.minlevel : 1,
+             p.tolerance ? p.tolerance : TOLERANCE, out);
   return fail (r);
 }
 

@@ -58,6 +58,7 @@ struct tgraph {
   long long launches;
   bmg_tree_op * dops;     /* the interpreter's operations of the iteration */
   long nops;
+  double bytes;           /* algorithmic bytes of the iteration */
 };
 
 struct bmg_tree {
@@ -676,8 +677,28 @@ static int t_residual (bmg_grid * g, struct bmg_tree * t, double * a, const doub
 
 /* the same operations, in the same order, as the launches of t_cycle and
    t_residual (an empty operation, which those skip, is left out) */
-typedef struct { bmg_tree_op * v; long n, cap; int err; } opvec;
+typedef struct { bmg_tree_op * v; long n, cap; int err; double bytes; int astored, lstored; } opvec;
 enum { F_A = 0, F_DA = 1, F_RES = 2, F_TMP = 3 };
+
+/* algorithmic bytes of one item of an operation: each array value it
+   reads or writes once (8 B), its list index (4 B) or ghost rule (16 B);
+   alpha and lambda only when they are stored */
+static double item_bytes (const opvec * o, int type, int sub, int rule)
+{
+  const double ax = o->astored ? 8. : 0., lam = o->lstored ? 8. : 0.;
+  if (rule) return 16. + 8. + 8.;                     /* rule, interior value, ghost */
+  switch (type) {
+  case BMG_TI_SET: return 4. + 8.;
+  case BMG_TI_PROLONG: return 4. + 4*8. + 8.;
+  case BMG_TI_RESTRICT: return 4. + 4*8. + 8.;
+  case BMG_TI_STAGE: return sub == BMG_T_OP_HALO ? 1. + 4*8. + 8. : 4. + 4*8. + 8.;
+  case BMG_TI_RELAX: return 4. + 8. + 4*8. + 4*ax + lam + 8.;
+  case BMG_TI_JACOBI: return 4. + 2*8. + 8.;
+  case BMG_TI_ADD: return 4. + 2*8. + 8.;
+  case BMG_TI_RESIDUAL: return 4. + 8. + 5*8. + 4*ax + lam + 8. + 4.;
+  }
+  return 0.;
+}
 
 static void r_push (opvec * o, int type, int field, int sub, int homog, const uint32_t * list,
                     long n, const bmg_tree_rule * rules, long nr, double v)
@@ -689,6 +710,8 @@ static void r_push (opvec * o, int type, int field, int sub, int homog, const ui
     if (!nv) { o->err = 1; return; }
     o->v = nv; o->cap = cap;
   }
+  const long items = type == BMG_TI_STAGE ? (sub == BMG_T_OP_HALO ? 4*n : sub == BMG_T_OP_RESTRICT ? n : 0) : n;
+  o->bytes += items*item_bytes (o, type, sub, 0) + nr*item_bytes (o, type, sub, 1);
   bmg_tree_op * q = &o->v[o->n++];
   memset (q, 0, sizeof *q);
   q->type = type; q->field = field; q->sub = sub; q->homog = homog; q->bcsel = 0;
@@ -788,8 +811,9 @@ static int t_iteration (bmg_grid * g, struct bmg_tree * t, const tkey * key, dou
   if (!e && t->interp) {
     /* the iteration as one interpreter launch, its operations uploaded once */
     graph_drop (victim);
-    opvec o = {NULL, 0, 0, 0};
+    opvec o = {NULL, 0, 0, 0, 0., c->ax.p != NULL, c->lam.p != NULL};
     r_iteration (g, t, &o, key->nrelax, key->minlevel, key->maxlevel);
+    victim->bytes = o.bytes;
     if (o.err) { free (o.v); return FAIL (BMG_ENOMEM); }
     if (cudaMalloc ((void **) &victim->dops, (o.n + 1)*sizeof (bmg_tree_op)) != cudaSuccess ||
         (o.n && cudaMemcpy (victim->dops, o.v, o.n*sizeof (bmg_tree_op), cudaMemcpyHostToDevice)
@@ -831,6 +855,13 @@ static int t_iteration (bmg_grid * g, struct bmg_tree * t, const tkey * key, dou
   }
   if (!e) {
     graph_drop (victim);
+    {
+      /* the same iteration's algorithmic bytes, from its operation list */
+      opvec o = {NULL, 0, 0, 0, 0., c->ax.p != NULL, c->lam.p != NULL};
+      r_iteration (g, t, &o, key->nrelax, key->minlevel, key->maxlevel);
+      victim->bytes = o.bytes;
+      free (o.v);
+    }
     cudaGraph_t graph;
     CKT (cudaStreamBeginCapture (g->stream, cudaStreamCaptureModeThreadLocal));
     int r = t_cycle (g, t, a, da, res, tmp, c, abc, key->nrelax, key->minlevel, key->maxlevel, nl);
@@ -852,6 +883,7 @@ static int t_iteration (bmg_grid * g, struct bmg_tree * t, const tkey * key, dou
   e->stamp = ++t->clock;
   CKT (cudaGraphLaunch (e->exec, g->stream));
   g->counters.launches += e->launches;
+  g->counters.bytes += e->bytes;
   return BMG_OK;
 }
 
@@ -963,12 +995,10 @@ int bmg_tree_poisson (bmg_grid * g, struct Poisson p, mgstats * out)
   if (r) return r;
   r = t_restrict_coefs (g, g->tree, &c);
   if (r) return r;
-  const double defaultol = TOLERANCE;
-  if (p.tolerance)
-    TOLERANCE = p.tolerance;
-  r = t_solve (g, a, b, &c, p.nrelax, res, p.minlevel > 1 ? p.minlevel : 1, 0., out);
-  if (p.tolerance)
-    TOLERANCE = defaultol;
+  /* p.tolerance for this solve, without touching the global TOLERANCE
+     (see bmg_poisson) */
+  r = t_solve (g, a, b, &c, p.nrelax, res, p.minlevel > 1 ? p.minlevel : 1,
+               p.tolerance ? p.tolerance : TOLERANCE, out);
   return FAIL (r);
 }
 

@@ -329,9 +329,11 @@ def run_workload(args, ws, rank, local):
     elif args.workload == "random_field_batch":
         from basilisk_b200.autograd import Problem, solve as dsolve
         B, depth = 16, 9
-        pr = Problem(2, depth, periodic=(0, 1), tolerance=1e-8, precision=args.precision)
+        pr = Problem(2, depth, periodic=(0, 1), tolerance=1e-8, precision=args.precision,
+                     lanes=args.lanes)
         g = pr.grid
-        g.set_stream(torch.cuda.current_stream().cuda_stream)
+        if args.lanes == 1:
+            g.set_stream(torch.cuda.current_stream().cuda_stream)
         inst = [problems.random_field_2d(depth, seed=3 + rank, instance=k) for k in range(2*B)]
         dev = lambda x: torch.tensor(np.stack(x), dtype=torch.float64, device="cuda")
         kappa = dev([d["kappa"] for d in inst[:B]])
@@ -369,6 +371,7 @@ def run_workload(args, ws, rank, local):
                               "w.r.t. kappa, tolerance 1e-8",
                   "grid": "16 x 512^2 (depth 9)", "form": args.precision,
                   "relax": "red-black Gauss-Seidel",
+                  "lanes": "%d grids on their own streams, one host thread each" % args.lanes,
                   "parallelism": "replicas" if ws > 1 else "1 gpu"}
     elif args.workload == "viscosity_2d":
         depth = 11
@@ -424,14 +427,17 @@ def run_workload(args, ws, rank, local):
                   "grid": "256^3 (depth 8)", "form": args.precision,
                   "relax": "red-black Gauss-Seidel",
                   "parallelism": "replicas" if ws > 1 else "1 gpu"}
-    g.set_timing(True)
+    grids = [ln.grid for ln in pr.lanes] if args.workload == "random_field_batch" else [g]
+    for gg in grids:
+        gg.set_timing(True)
     clocks.start()
     for _ in range(args.warmup):
         reset()
         solve()
     torch.cuda.synchronize()
     barrier(ws)
-    g.reset_counters()
+    for gg in grids:
+        gg.reset_counters()
     times, st = [], None
     t_begin = time.monotonic()
     for _ in range(args.steps):
@@ -447,7 +453,8 @@ def run_workload(args, ws, rank, local):
     clocks.window(t_begin, time.monotonic())
     clk = clocks.stop()
     barrier(ws)
-    c = g.counters()
+    cs = [gg.counters() for gg in grids]
+    c = {k: sum(x[k] for x in cs) for k in cs[0]}
     ms = max_over_ranks(ws, sum(times) / len(times))
     if rank != 0:
         return
@@ -463,6 +470,68 @@ def run_workload(args, ws, rank, local):
                        "vcycle_gbs": c["bytes"] / (c["cycle_ms"] * 1e-3) / 1e9
                        if c["cycle_ms"] and c["bytes"] else None},
             "clocks": clk, "gpu_launches": int(c["launches"])}
+    # the whole step's algorithmic bytes (every V-cycle kernel, each array
+    # pass once at its storage precision; on the tree plus 4 B per list
+    # index) over its device time
+    peak, peak_kind = load_peaks()
+    if c["bytes"]:
+        ach = c["bytes"] / args.steps / (ms * 1e-3) / 1e9
+        line["roofline"] = {"bound": "hbm", "kernel": "whole step (all V-cycle kernels)",
+                            "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                            "traffic": None, "peak_kind": peak_kind,
+                            "note": "algorithmic bytes of the step over its CUDA-event time; "
+                                    "no ncu capture of this workload, so no DRAM traffic"}
+    if not args.no_cpu and args.workload == "helmholtz_3d":
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        from oracle import oracle
+        from helpers import oracle_grid
+        threads = os.cpu_count()
+        o = oracle_grid(prob, relax=oracle.RELAX_GS, threads=threads)
+        t0 = time.perf_counter()
+        cst = o.poisson(tolerance=tol)
+        dt = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": 1.0 / dt, "unit": "solves/s", "cores": threads,
+                                "kind": "port",
+                                "sample": "1 full solve of the same problem (%d V-cycles), "
+                                          "lexicographic GS, %d OpenMP threads" % (cst["i"], threads)}
+    if not args.no_cpu and args.workload == "random_field_batch":
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        from oracle import oracle
+        threads = os.cpu_count()
+        kq = [d["kappa"] for d in inst[:2]]
+        bq = b[:2].cpu().numpy()
+        obs = a_obs[:2].cpu().numpy()
+        n = 1 << depth
+        t_cpu = 0.0
+        for k in range(2):
+            kk = np.asarray(kq[k])
+            kx = np.concatenate([kk[-1:], kk, kk[:1]], axis=0)
+            ky = np.concatenate([kk[:, -1:], kk, kk[:, :1]], axis=1)
+            alpha = [np.exp((kx[:-1] + kx[1:]) / 2), np.exp((ky[:, :-1] + ky[:, 1:]) / 2)]
+            for rhs_kind in ("forward", "adjoint"):
+                o = oracle.Grid(2, depth, relax=oracle.RELAX_GS, threads=threads)
+                o.set_periodic(0); o.set_periodic(1)
+                o.set_alpha(alpha)
+                o.set_lambda_const(0.0)
+                if rhs_kind == "forward":
+                    rhs = bq[k]
+                else:
+                    rhs = a_fwd - obs[k]
+                    rhs = rhs - rhs.mean()
+                o.set_b(rhs)
+                o.set_a(np.zeros((n, n)))
+                t0 = time.perf_counter()
+                o.poisson(tolerance=tol)
+                t_cpu += time.perf_counter() - t0
+                if rhs_kind == "forward":
+                    a_fwd = o.get_a() - o.get_a().mean()
+        step = t_cpu * B / 2
+        line["cpu_baseline"] = {"value": 1.0 / step, "unit": unit, "cores": threads,
+                                "kind": "port",
+                                "sample": "the forward and adjoint solves of 2 of the 16 "
+                                          "instances (lexicographic GS, %d OpenMP threads, %.1f s), "
+                                          "scaled to 16; the face gradients are not timed"
+                                          % (threads, t_cpu)}
     if not args.no_cpu and args.workload == "two_phase_tree":
         sys.path.insert(0, os.path.join(ROOT, "tests"))
         from oracle import tree as otree
@@ -529,6 +598,8 @@ def main():
                     help="two_phase_2d: the headline; the others print their own line")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64",
                     help="form of the helmholtz_3d and random_field_batch workloads")
+    ap.add_argument("--lanes", type=int, default=8,
+                    help="random_field_batch: grids solving instances concurrently")
     args = ap.parse_args()
     ws, rank, local = dist_init()
     if args.impl == "bmg" and args.workload != "two_phase_2d":

@@ -255,3 +255,30 @@ def test_checkpointed_chain():
         grads.append(torch.autograd.grad(loss, x)[0])
     assert torch.allclose(grads[0], grads[1], rtol=0, atol=1e-12 * grads[0].abs().max().item())
     prob.close()
+
+
+def test_lanes_give_the_single_lane_results():
+    """A batch of 6 periodic instances on a Problem with 3 lanes (three grids,
+    three streams, three host threads) gives the single-lane solutions and
+    gradients bit for bit."""
+    import torch
+    from basilisk_b200.autograd import solve
+    depth, n, B = 6, 64, 6
+    g = torch.Generator(device="cpu").manual_seed(12)
+    b = torch.randn(B, n, n, generator=g, dtype=torch.float64).cuda()
+    kx = torch.randn(B, n + 1, n, generator=g, dtype=torch.float64).cuda() * 0.3
+    ky = torch.randn(B, n, n + 1, generator=g, dtype=torch.float64).cuda() * 0.3
+    kx[:, n] = kx[:, 0]; ky[:, :, n] = ky[:, :, 0]
+    aobs = torch.randn(B, n, n, generator=g, dtype=torch.float64).cuda()
+    out = {}
+    for lanes in (1, 3):
+        from basilisk_b200.autograd import Problem
+        prob = Problem(2, depth, periodic=(0, 1), tolerance=1e-12, alpha=True, lanes=lanes)
+        ins = [t.clone().requires_grad_(True) for t in (b, kx, ky)]
+        a = solve(prob, ins[0], alpha=[torch.exp(ins[1]), torch.exp(ins[2])])
+        loss = 0.5 * ((a - aobs) ** 2).sum()
+        out[lanes] = (a.detach(), torch.autograd.grad(loss, ins))
+        prob.close()
+    assert torch.equal(out[1][0], out[3][0])
+    for k in range(3):
+        assert torch.equal(out[1][1][k], out[3][1][k]), k
