@@ -153,6 +153,13 @@ SIGNATURES = {
     "bmg_set_timing": (I, [P, I]),
     "bmg_set_graphs": (I, [P, I]),
     "bmg_sum_noalloc": (I, [P, SZ, P, P]),
+    "bmg_shard_new": (I, [ctypes.POINTER(P), ctypes.POINTER(P), ctypes.POINTER(I),
+                          ctypes.POINTER(I)]),
+    "bmg_shard_free": (None, [P]),
+    "bmg_shard_poisson": (I, [P, Poisson, ctypes.POINTER(mgstats)]),
+    "bmg_shard_dims": (I, [I, I, ctypes.POINTER(I)]),
+    "bmg_shard_neighbours": (I, [I, ctypes.POINTER(I), ctypes.POINTER(I), I,
+                                 ctypes.POINTER(I)]),
     "bmg_adjoint_gradients": (I, [P, bmg_scalar, bmg_scalar, ctypes.POINTER(P), P, I]),
 }
 GLOBALS = {"NITERMAX": ctypes.c_int, "NITERMIN": ctypes.c_int, "TOLERANCE": ctypes.c_double}

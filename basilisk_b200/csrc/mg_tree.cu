@@ -47,10 +47,16 @@ __device__ __forceinline__ double coef (const bmg_tree_coef & c, long long id)
 /* a field value: a plain load in the one-operation kernels, an L2 load
    (ld.global.cg) in the interpreter, whose fields other CTAs write during
    the launch (L1 is not coherent across SMs) */
-template <bool CG>
-__device__ __forceinline__ double ldf (const double * p)
+template <bool CG, typename R>
+__device__ __forceinline__ R ldf (const R * p)
 {
   return CG ? __ldcg (p) : *p;
+}
+
+/* a coefficient of the mixed form's FP32 cycle */
+__device__ __forceinline__ float coef (const bmg_tree_coef32 & c, long long id)
+{
+  return c.p ? c.p[id] : (float) c.c;
 }
 
 #define GRID_STRIDE(k, n) \
@@ -69,15 +75,15 @@ __global__ void k_set (const uint32_t * __restrict__ list, long n, TL T, double 
 
 /* bilinear (multigrid-common.h:124-140) of child (i, j) of level l from
    level l - 1 */
-template <bool CG = false>
-__device__ __forceinline__ double bilinear (const TL & T, const double * s, int l, int i, int j)
+template <bool CG = false, typename R = double>
+__device__ __forceinline__ R bilinear (const TL & T, const R * s, int l, int i, int j)
 {
   const int pi = i >> 1, pj = j >> 1, cx = (i & 1) ? 1 : -1, cy = (j & 1) ? 1 : -1;
-  const double * c = s + T.off[l - 1];
+  const R * c = s + T.off[l - 1];
   const bmg_geom & gc = T.g[l - 1];
-  return (9.*ldf<CG> (c + cidx<2> (gc, pi, pj, 0)) +
-          3.*(ldf<CG> (c + cidx<2> (gc, pi + cx, pj, 0)) + ldf<CG> (c + cidx<2> (gc, pi, pj + cy, 0))) +
-          ldf<CG> (c + cidx<2> (gc, pi + cx, pj + cy, 0)))/16.;
+  return ((R) 9*ldf<CG> (c + cidx<2> (gc, pi, pj, 0)) +
+          (R) 3*(ldf<CG> (c + cidx<2> (gc, pi + cx, pj, 0)) + ldf<CG> (c + cidx<2> (gc, pi, pj + cy, 0))) +
+          ldf<CG> (c + cidx<2> (gc, pi + cx, pj + cy, 0)))/(R) 16;
 }
 
 /* foreach_level (l) s[] = bilinear (point, s) (poisson.h:64-68) */
@@ -94,8 +100,8 @@ __global__ void k_prolong (const uint32_t * __restrict__ list, long n, TL T, dou
 
 /* refine_bilinear of the halo children of prolongation leaves: one thread
    per child */
-template <bool CG = false>
-__device__ __forceinline__ void halo_child (const uint32_t * list, long k, const TL & T, double * s)
+template <bool CG = false, typename R = double>
+__device__ __forceinline__ void halo_child (const uint32_t * list, long k, const TL & T, R * s)
 {
   int l, i, j;
   unpack (list[k >> 2], l, i, j);
@@ -113,19 +119,19 @@ __global__ void k_halo (const uint32_t * __restrict__ list, long n, TL T, double
 
 /* restriction_average (multigrid-common.h:26-32), children in foreach_child
    order */
-template <bool CG = false>
-__device__ __forceinline__ void restrict_cell (const uint32_t * list, long k, const TL & T, double * s)
+template <bool CG = false, typename R = double>
+__device__ __forceinline__ void restrict_cell (const uint32_t * list, long k, const TL & T, R * s)
 {
   int l, i, j;
   unpack (list[k], l, i, j);
-  const double * f = s + T.off[l + 1];
+  const R * f = s + T.off[l + 1];
   const bmg_geom & gf = T.g[l + 1];
-  double sum = 0.;
+  R sum = 0.;
   sum += ldf<CG> (f + cidx<2> (gf, 2*i, 2*j, 0));
   sum += ldf<CG> (f + cidx<2> (gf, 2*i, 2*j + 1, 0));
   sum += ldf<CG> (f + cidx<2> (gf, 2*i + 1, 2*j, 0));
   sum += ldf<CG> (f + cidx<2> (gf, 2*i + 1, 2*j + 1, 0));
-  s[gidx (T, l, i, j)] = sum/(1 << 2);
+  s[gidx (T, l, i, j)] = sum/(R) (1 << 2);
 }
 
 __global__ void k_restrict (const uint32_t * __restrict__ list, long n, TL T, double * s)
@@ -180,8 +186,8 @@ __device__ __forceinline__ double bc_of (const bmg_tree_bc & bc, int side, int l
   return homog ? sn : Delta*val + sn;
 }
 
-template <bool CG = false>
-__device__ __forceinline__ void ghost_value (const bmg_tree_rule & r, const TL & T, double * s,
+template <bool CG = false, typename R = double>
+__device__ __forceinline__ void ghost_value (const bmg_tree_rule & r, const TL & T, R * s,
                                              const bmg_tree_bc & bc, int homog)
 {
   int l, gi, gj, l2, a, b;
@@ -194,7 +200,7 @@ __device__ __forceinline__ void ghost_value (const bmg_tree_rule & r, const TL &
   double v = bc_of (bc, s1, l, t1, sn, D, homog);
   if (kind == BMG_T_DIAGONAL)
     v = (v + bc_of (bc, s2, l, t2, sn, D, homog) - sn);
-  s[gidx (T, l, gi, gj)] = v;
+  s[gidx (T, l, gi, gj)] = (R) v;
 }
 
 __global__ void k_bc (const bmg_tree_rule * __restrict__ rules, long n, TL T, double * s,
@@ -225,21 +231,20 @@ __global__ void k_stage (const uint32_t * __restrict__ list, long n, int op,
 
 /* relax (poisson.h:303-320) of one listed cell; x is the first index
    (stride P), y the second */
-template <bool CG = false>
-__device__ __forceinline__ void relax_item (uint32_t e, const TL & T, const double * a,
-                                            const double * b, const bmg_tree_coef & ax,
-                                            const bmg_tree_coef & ay, const bmg_tree_coef & lam,
-                                            double * out)
+template <bool CG = false, typename R = double, typename CO = bmg_tree_coef>
+__device__ __forceinline__ void relax_item (uint32_t e, const TL & T, const R * a,
+                                            const R * b, const CO & ax, const CO & ay,
+                                            const CO & lam, R * out)
 {
   int l, i, j;
   unpack (e, l, i, j);
   const long long id = gidx (T, l, i, j), P = T.g[l].P;
-  const double Delta = T.Delta[l];
-  double nn = - (Delta*Delta)*ldf<CG> (b + id), d = - coef (lam, id)*(Delta*Delta);
-  const double x1 = coef (ax, id + P), x0 = coef (ax, id);
+  const R Delta = (R) T.Delta[l];
+  R nn = - (Delta*Delta)*ldf<CG> (b + id), d = - coef (lam, id)*(Delta*Delta);
+  const R x1 = coef (ax, id + P), x0 = coef (ax, id);
   nn += x1*ldf<CG> (a + id + P) + x0*ldf<CG> (a + id - P);
   d += x1 + x0;
-  const double y1 = coef (ay, id + 1), y0 = coef (ay, id);
+  const R y1 = coef (ay, id + 1), y0 = coef (ay, id);
   nn += y1*ldf<CG> (a + id + 1) + y0*ldf<CG> (a + id - 1);
   d += y1 + y0;
   out[id] = nn/d;
@@ -294,11 +299,11 @@ __device__ __forceinline__ void max_bits (unsigned long long * m, double v)
 
 /* residual, tree branch (poisson.h:355-372): a leaf face shared with a
    refined neighbour carries the mean of the two fine fluxes (halo_face) */
-template <bool CG = false>
+template <bool CG = false, typename R = double>
 __device__ __forceinline__ double residual_item (uint32_t e, const TL & T, const unsigned char * fl,
                                                  const double * a, const double * b,
                                                  const bmg_tree_coef & ax, const bmg_tree_coef & ay,
-                                                 const bmg_tree_coef & lam, double * res)
+                                                 const bmg_tree_coef & lam, R * res)
 {
   int l, i, j;
   unpack (e, l, i, j);
@@ -319,7 +324,7 @@ __device__ __forceinline__ double residual_item (uint32_t e, const TL & T, const
   double r = b[id] - coef (lam, id)*ldf<CG> (a + id);
   r -= (gr - gl)/Delta;
   r -= (gt - gb)/Delta;
-  res[id] = r;
+  res[id] = (R) r;
   return r;
 }
 
@@ -408,12 +413,70 @@ __global__ void k_sum_final (const double * __restrict__ partials, int np, doubl
    them.  Every item is computed by the function the one-operation kernel
    uses, so the results are bit-identical.  The residual's maximum is
    reduced per warp into maxres (zeroed before the launch). */
-template <int C>
+/* The list operations that work on one field s of the scalar type S: a
+   set, prolongation, restriction or boundary stage (the interpreter's
+   field 0, a, is FP64; the cycle's fields have the cycle's type) */
+template <typename S>
+__device__ __forceinline__ void field_op (const bmg_tree_op & op, long gt, long gs, uint32_t first,
+                                          const TL & T, S * s, const bmg_tree_bc & bc)
+{
+  const uint32_t * list = op.list;
+#define ENTRY(k) ((k) == gt ? first : list[k])
+  switch (op.type) {
+  case BMG_TI_SET:
+    for (long k = gt; k < op.n; k += gs) {
+      int l, i, j;
+      unpack (ENTRY (k), l, i, j);
+      s[gidx (T, l, i, j)] = (S) op.v;
+    }
+    break;
+  case BMG_TI_PROLONG:
+    for (long k = gt; k < op.n; k += gs) {
+      int l, i, j;
+      unpack (ENTRY (k), l, i, j);
+      s[gidx (T, l, i, j)] = bilinear<true> (T, s, l, i, j);
+    }
+    break;
+  case BMG_TI_RESTRICT:
+    for (long k = gt; k < op.n; k += gs)
+      restrict_cell<true> (list, k, T, s);
+    break;
+  case BMG_TI_STAGE: {
+    const long w = op.sub == BMG_T_OP_HALO ? 4*op.n : op.sub == BMG_T_OP_RESTRICT ? op.n : 0;
+    for (long k = gt; k < w + op.nr; k += gs) {
+      if (k >= w) ghost_value<true> (op.rules[k - w], T, s, bc, op.homog);
+      else if (op.sub == BMG_T_OP_HALO) halo_child<true> (list, k, T, s);
+      else restrict_cell<true> (list, k, T, s);
+    }
+    break;
+  }
+  }
+#undef ENTRY
+}
+
+/* One mg_solve iteration on a tree (the cycle and the residual) is a fixed
+   sequence of a few thousand small list operations, each of which depends
+   on the one before.  k_tree_interp runs such a sequence (bmg_tree_op
+   records, built on the host in the order of the launches they replace)
+   in one launch of one thread-block cluster: every operation's items are
+   spread over the cluster's threads, and the cluster barrier
+   (release/acquire at cluster scope) separates an operation from the next;
+   field values are loaded from L2, since other CTAs of the cluster wrote
+   them.  Every item is computed by the function the one-operation kernel
+   uses, so the results are bit-identical.  The residual's maximum is
+   reduced per warp into maxres (zeroed before the launch).
+   R is the cycle's type: double for the plain form; float for the mixed
+   form, whose correction da, restricted residual res and Jacobi temporary
+   are FP32 with FP32 coefficients (rax, ray, rlam), while a, b and the
+   residual itself (ax, ay, lam) stay FP64 and res receives the FP64
+   residual rounded to FP32. */
+template <int C, typename R, typename CO>
 __global__ void __launch_bounds__ (1024, 1)
-k_tree_interp (const bmg_tree_op * __restrict__ ops, int nops, TL Tp, double * fa, double * fda,
-               double * fres, double * ftmp, const double * __restrict__ b,
+k_tree_interp (const bmg_tree_op * __restrict__ ops, int nops, TL Tp, double * fa, R * fda,
+               R * fres, R * ftmp, const double * __restrict__ b,
                const unsigned char * __restrict__ fl, bmg_tree_coef ax, bmg_tree_coef ay,
-               bmg_tree_coef lam, bmg_tree_bc bc0, bmg_tree_bc bc1, unsigned long long * maxres)
+               bmg_tree_coef lam, CO rax, CO ray, CO rlam, bmg_tree_bc bc0, bmg_tree_bc bc1,
+               unsigned long long * maxres)
 {
   constexpr int CH = 256;                       /* operations staged per chunk */
   __shared__ TL T;
@@ -423,7 +486,7 @@ k_tree_interp (const bmg_tree_op * __restrict__ ops, int nops, TL Tp, double * f
   unsigned rank;
   asm volatile ("mov.u32 %0, %%cluster_ctarank;" : "=r"(rank));
   const long gt = (long) rank*blockDim.x + threadIdx.x, gs = (long) C*blockDim.x;
-  double * const F[4] = {fa, fda, fres, ftmp};
+  R * const F[4] = {NULL, fda, fres, ftmp};
   double m = 0.;
   /* the list entry of the thread's first item of the current operation,
      loaded while the previous one waited at the barrier */
@@ -442,47 +505,27 @@ k_tree_interp (const bmg_tree_op * __restrict__ ops, int nops, TL Tp, double * f
       if (gt < sops[0].n && sops[0].list) first = sops[0].list[gt];
     }
     const bmg_tree_op & op = sops[o % CH];
-    double * s = F[op.field];
     const uint32_t * list = op.list;
 #define ENTRY(k) ((k) == gt ? first : list[k])
     switch (op.type) {
     case BMG_TI_SET:
-      for (long k = gt; k < op.n; k += gs) {
-        int l, i, j;
-        unpack (ENTRY (k), l, i, j);
-        s[gidx (T, l, i, j)] = op.v;
-      }
-      break;
     case BMG_TI_PROLONG:
-      for (long k = gt; k < op.n; k += gs) {
-        int l, i, j;
-        unpack (ENTRY (k), l, i, j);
-        s[gidx (T, l, i, j)] = bilinear<true> (T, s, l, i, j);
-      }
-      break;
     case BMG_TI_RESTRICT:
-      for (long k = gt; k < op.n; k += gs)
-        restrict_cell<true> (list, k, T, s);
+    case BMG_TI_STAGE:
+      if (op.field == 0) field_op (op, gt, gs, first, T, fa, B[op.bcsel]);
+      else field_op (op, gt, gs, first, T, F[op.field], B[op.bcsel]);
       break;
-    case BMG_TI_STAGE: {
-      const long w = op.sub == BMG_T_OP_HALO ? 4*op.n : op.sub == BMG_T_OP_RESTRICT ? op.n : 0;
-      for (long k = gt; k < w + op.nr; k += gs) {
-        if (k >= w) ghost_value<true> (op.rules[k - w], T, s, B[op.bcsel], op.homog);
-        else if (op.sub == BMG_T_OP_HALO) halo_child<true> (list, k, T, s);
-        else restrict_cell<true> (list, k, T, s);
-      }
-      break;
-    }
     case BMG_TI_RELAX:
       for (long k = gt; k < op.n; k += gs)
-        relax_item<true> (ENTRY (k), T, fda, fres, ax, ay, lam, op.sub ? ftmp : fda);
+        relax_item<true> (ENTRY (k), T, (const R *) fda, (const R *) fres, rax, ray, rlam,
+                          op.sub ? ftmp : fda);
       break;
     case BMG_TI_JACOBI:
       for (long k = gt; k < op.n; k += gs) {
         int l, i, j;
         unpack (ENTRY (k), l, i, j);
         const long long id = gidx (T, l, i, j);
-        fda[id] = (ldf<true> (fda + id) + 2.*ldf<true> (ftmp + id))/3.;
+        fda[id] = (ldf<true> (fda + id) + (R) 2*ldf<true> (ftmp + id))/(R) 3;
       }
       break;
     case BMG_TI_ADD:
@@ -490,7 +533,7 @@ k_tree_interp (const bmg_tree_op * __restrict__ ops, int nops, TL Tp, double * f
         int l, i, j;
         unpack (ENTRY (k), l, i, j);
         const long long id = gidx (T, l, i, j);
-        fa[id] = ldf<true> (fa + id) + ldf<true> (fda + id);
+        fa[id] = ldf<true> (fa + id) + (double) ldf<true> (fda + id);
       }
       break;
     case BMG_TI_RESIDUAL:
@@ -518,12 +561,13 @@ k_tree_interp (const bmg_tree_op * __restrict__ ops, int nops, TL Tp, double * f
     max_bits (maxres, m);
 }
 
-template <int C>
-int launch_interp (const bmg_tree_op * ops, int nops, const TL & T, double * const * f,
+template <int C, typename R, typename CO>
+int launch_interp (const bmg_tree_op * ops, int nops, const TL & T, double * fa, R * const * f,
                    const double * b, const unsigned char * fl, const bmg_tree_coef * co,
-                   const bmg_tree_bc * bc, unsigned long long * maxres, cudaStream_t st)
+                   const CO * rco, const bmg_tree_bc * bc, unsigned long long * maxres,
+                   cudaStream_t st)
 {
-  auto kern = k_tree_interp<C>;
+  auto kern = k_tree_interp<C, R, CO>;
   static int ok[64];
   int dev = 0;
   cudaGetDevice (&dev);
@@ -547,8 +591,18 @@ int launch_interp (const bmg_tree_op * ops, int nops, const TL & T, double * con
     ok[dev] = e == cudaSuccess && nc >= 1 ? 1 : -1;
   }
   if (ok[dev] < 0) return -1;
-  return (int) cudaLaunchKernelEx (&cfg, kern, ops, nops, T, f[0], f[1], f[2], f[3], b, fl,
-                                   co[0], co[1], co[2], bc[0], bc[1], maxres);
+  return (int) cudaLaunchKernelEx (&cfg, kern, ops, nops, T, fa, f[0], f[1], f[2], b, fl,
+                                   co[0], co[1], co[2], rco[0], rco[1], rco[2], bc[0], bc[1],
+                                   maxres);
+}
+
+/* double -> float of n consecutive values (the mixed form's FP32 copies
+   of the coefficients and of the initial residual, all levels at once) */
+__global__ void k_to_f32 (const double * __restrict__ src, float * __restrict__ dst, long long n)
+{
+  for (long long k = (long long) blockIdx.x*blockDim.x + threadIdx.x; k < n;
+       k += (long long) gridDim.x*blockDim.x)
+    dst[k] = (float) src[k];
 }
 
 const int NT = 256;
@@ -682,11 +736,12 @@ int bmg_tree_interp_available (void)
     cfg.numAttrs = 1;
     int nc = 0;
     cudaError_t e = C > 8 ?
-      cudaFuncSetAttribute (k_tree_interp<16>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) :
+      cudaFuncSetAttribute (k_tree_interp<16, double, bmg_tree_coef>,
+                            cudaFuncAttributeNonPortableClusterSizeAllowed, 1) :
       cudaSuccess;
     if (e == cudaSuccess)
-      e = C > 8 ? cudaOccupancyMaxActiveClusters (&nc, k_tree_interp<16>, &cfg)
-                : cudaOccupancyMaxActiveClusters (&nc, k_tree_interp<8>, &cfg);
+      e = C > 8 ? cudaOccupancyMaxActiveClusters (&nc, k_tree_interp<16, double, bmg_tree_coef>, &cfg)
+                : cudaOccupancyMaxActiveClusters (&nc, k_tree_interp<8, double, bmg_tree_coef>, &cfg);
     cudaGetLastError ();
     if (e == cudaSuccess && nc >= 1) return 1;
   }
@@ -699,9 +754,34 @@ int bmg_tree_launch_interp (const bmg_tree_op * ops, int nops, const bmg_tree_le
                             unsigned long long * maxres, cudaStream_t st)
 {
   if (nops < 1) return 0;
-  int e = launch_interp<16> (ops, nops, *T, fields, b, flags, coefs, bcs, maxres, st);
-  if (e == -1) e = launch_interp<8> (ops, nops, *T, fields, b, flags, coefs, bcs, maxres, st);
+  double * const f[3] = {fields[1], fields[2], fields[3]};
+  int e = launch_interp<16> (ops, nops, *T, fields[0], f, b, flags, coefs, coefs, bcs, maxres, st);
+  if (e == -1)
+    e = launch_interp<8> (ops, nops, *T, fields[0], f, b, flags, coefs, coefs, bcs, maxres, st);
   if (e) return e;
+  return status ();
+}
+
+int bmg_tree_launch_interp_mixed (const bmg_tree_op * ops, int nops, const bmg_tree_levels * T,
+                                  double * a, float * const * fields32, const double * b,
+                                  const unsigned char * flags, const bmg_tree_coef * coefs,
+                                  const bmg_tree_coef32 * coefs32, const bmg_tree_bc * bcs,
+                                  unsigned long long * maxres, cudaStream_t st)
+{
+  if (nops < 1) return 0;
+  int e = launch_interp<16> (ops, nops, *T, a, fields32, b, flags, coefs, coefs32, bcs, maxres, st);
+  if (e == -1)
+    e = launch_interp<8> (ops, nops, *T, a, fields32, b, flags, coefs, coefs32, bcs, maxres, st);
+  if (e) return e;
+  return status ();
+}
+
+int bmg_tree_launch_to_f32 (const double * src, float * dst, long long n, cudaStream_t st)
+{
+  if (n <= 0) return 0;
+  long long nb = (n + NT - 1)/NT;
+  if (nb > 148*8) nb = 148*8;
+  k_to_f32<<<(int) nb, NT, 0, st>>> (src, dst, n);
   return status ();
 }
 

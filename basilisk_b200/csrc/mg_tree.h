@@ -51,6 +51,13 @@ typedef struct {
   double c;
 } bmg_tree_coef;
 
+/* a coefficient of the mixed form's FP32 cycle: an all-level FP32 array
+   (the same element layout as the FP64 one), or a constant */
+typedef struct {
+  const float * p;
+  double c;
+} bmg_tree_coef32;
+
 /* box conditions of one cell field, per level (NULL values: the constant) */
 typedef struct {
   int type[4];
@@ -119,6 +126,19 @@ int bmg_tree_launch_interp (const bmg_tree_op * ops, int nops, const bmg_tree_le
                             double * const * fields, const double * b, const unsigned char * flags,
                             const bmg_tree_coef * coefs, const bmg_tree_bc * bcs,
                             unsigned long long * maxres, cudaStream_t st);
+
+/* the same operations in the mixed form: the cycle's fields
+   fields32 = {da, res, tmp} and its coefficients coefs32 are FP32 (same
+   element layout as the FP64 arrays), a, b and the residual (coefs) FP64;
+   the residual operation stores the FP64 residual rounded to FP32 into
+   res, and the correction adds the FP32 da to the FP64 a */
+int bmg_tree_launch_interp_mixed (const bmg_tree_op * ops, int nops, const bmg_tree_levels * T,
+                                  double * a, float * const * fields32, const double * b,
+                                  const unsigned char * flags, const bmg_tree_coef * coefs,
+                                  const bmg_tree_coef32 * coefs32, const bmg_tree_bc * bcs,
+                                  unsigned long long * maxres, cudaStream_t st);
+/* dst[k] = (float) src[k], 0 <= k < n */
+int bmg_tree_launch_to_f32 (const double * src, float * dst, long long n, cudaStream_t st);
 
 /* deterministic sum over the listed cells: per-block partials, then one
    block; npartials at most 1024 */

@@ -19,7 +19,14 @@
  *
  * The red-black smoother relaxes the red cells of every level of the set,
  * refreshes the tree boundary, then the black cells; the Jacobi smoother is
- * the reference's JACOBI branch.  The tree path computes in FP64.
+ * the reference's JACOBI branch.
+ *
+ * Two forms, as on uniform grids: the plain form computes in FP64; the
+ * mixed form (grid precision BMG_MIXED) runs the cycle -- restriction of
+ * the residual, prolongation, relaxation and the tree boundaries of the
+ * correction -- in FP32, and keeps FP64 for a, b, the residual r = b - L a
+ * (its boundary of a included) and the accumulation a += da, so that every
+ * iteration is an FP64 iterative-refinement step.
  */
 #include <stdio.h>
 #include <stdlib.h>
@@ -42,7 +49,7 @@ enum { SCHED_FULL = 0, SCHED_PRUNED = 1 };
 
 /* everything a captured solve iteration depends on */
 typedef struct {
-  int nrelax, minlevel, maxlevel, relax;
+  int nrelax, minlevel, maxlevel, relax, mixed;
   const void * a, * b, * da, * res, * tmp;
   bmg_tree_coef ax, ay, lam;
   bmg_tree_bc abc;
@@ -84,7 +91,10 @@ struct bmg_tree {
   struct tgraph graphs[NTGRAPH];
   unsigned long long clock;
   int interp;                         /* run solve iterations through the interpreter */
+  float * ws32;                       /* mixed form: da, res, tmp, alpha x, alpha y, lambda in
+                                         FP32, each an all-level array in the FP64 element layout */
 };
+enum { W32_DA = 0, W32_RES, W32_TMP, W32_AX, W32_AY, W32_LAM, W32_N };
 
 #define FAIL(s) bmg_i_fail (s)
 #define CKT(call) do { cudaError_t e_ = (call); if (e_ != cudaSuccess) { \
@@ -121,7 +131,7 @@ static void tree_release (struct bmg_tree * t)
   for (int i = 0; i < NTGRAPH; i++) graph_drop (&t->graphs[i]);
   for (int l = 0; l <= TMAX; l++) { free (t->fl[l]); free (t->nb[l]); }
   cudaFree (t->dflags); cudaFree (t->dlist); cudaFree (t->drules); cudaFree (t->dpart);
-  cudaFree (t->dsrules);
+  cudaFree (t->dsrules); cudaFree (t->ws32);
   free (t->stages);
   free (t);
 }
@@ -677,25 +687,32 @@ static int t_residual (bmg_grid * g, struct bmg_tree * t, double * a, const doub
 
 /* the same operations, in the same order, as the launches of t_cycle and
    t_residual (an empty operation, which those skip, is left out) */
-typedef struct { bmg_tree_op * v; long n, cap; int err; double bytes; int astored, lstored; } opvec;
+typedef struct {
+  bmg_tree_op * v; long n, cap; int err; double bytes; int astored, lstored;
+  double vb;            /* bytes of a value of the cycle's fields: 8, or 4 (mixed form) */
+} opvec;
 enum { F_A = 0, F_DA = 1, F_RES = 2, F_TMP = 3 };
 
 /* algorithmic bytes of one item of an operation: each array value it
-   reads or writes once (8 B), its list index (4 B) or ghost rule (16 B);
-   alpha and lambda only when they are stored */
-static double item_bytes (const opvec * o, int type, int sub, int rule)
+   reads or writes once at its storage precision (a, b and the residual's
+   coefficients 8 B, the cycle's fields and coefficients o->vb), its list
+   index (4 B) or ghost rule (16 B); alpha and lambda only when they are
+   stored */
+static double item_bytes (const opvec * o, int type, int sub, int rule, int field)
 {
-  const double ax = o->astored ? 8. : 0., lam = o->lstored ? 8. : 0.;
-  if (rule) return 16. + 8. + 8.;                     /* rule, interior value, ghost */
+  const double w = field == F_A ? 8. : o->vb;
+  const double ax = o->astored ? o->vb : 0., lam = o->lstored ? o->vb : 0.;
+  const double ax8 = o->astored ? 8. : 0., lam8 = o->lstored ? 8. : 0.;
+  if (rule) return 16. + w + w;                       /* rule, interior value, ghost */
   switch (type) {
-  case BMG_TI_SET: return 4. + 8.;
-  case BMG_TI_PROLONG: return 4. + 4*8. + 8.;
-  case BMG_TI_RESTRICT: return 4. + 4*8. + 8.;
-  case BMG_TI_STAGE: return sub == BMG_T_OP_HALO ? 1. + 4*8. + 8. : 4. + 4*8. + 8.;
-  case BMG_TI_RELAX: return 4. + 8. + 4*8. + 4*ax + lam + 8.;
-  case BMG_TI_JACOBI: return 4. + 2*8. + 8.;
-  case BMG_TI_ADD: return 4. + 2*8. + 8.;
-  case BMG_TI_RESIDUAL: return 4. + 8. + 5*8. + 4*ax + lam + 8. + 4.;
+  case BMG_TI_SET: return 4. + w;
+  case BMG_TI_PROLONG: return 4. + 4*w + w;
+  case BMG_TI_RESTRICT: return 4. + 4*w + w;
+  case BMG_TI_STAGE: return sub == BMG_T_OP_HALO ? 1. + 4*w + w : 4. + 4*w + w;
+  case BMG_TI_RELAX: return 4. + w + 4*w + 4*ax + lam + w;
+  case BMG_TI_JACOBI: return 4. + 2*w + w;
+  case BMG_TI_ADD: return 4. + 2*8. + o->vb;
+  case BMG_TI_RESIDUAL: return 4. + 8. + 5*8. + 4*ax8 + lam8 + o->vb + 4.;
   }
   return 0.;
 }
@@ -711,7 +728,7 @@ static void r_push (opvec * o, int type, int field, int sub, int homog, const ui
     o->v = nv; o->cap = cap;
   }
   const long items = type == BMG_TI_STAGE ? (sub == BMG_T_OP_HALO ? 4*n : sub == BMG_T_OP_RESTRICT ? n : 0) : n;
-  o->bytes += items*item_bytes (o, type, sub, 0) + nr*item_bytes (o, type, sub, 1);
+  o->bytes += items*item_bytes (o, type, sub, 0, field) + nr*item_bytes (o, type, sub, 1, field);
   bmg_tree_op * q = &o->v[o->n++];
   memset (q, 0, sizeof *q);
   q->type = type; q->field = field; q->sub = sub; q->homog = homog; q->bcsel = 0;
@@ -811,7 +828,7 @@ static int t_iteration (bmg_grid * g, struct bmg_tree * t, const tkey * key, dou
   if (!e && t->interp) {
     /* the iteration as one interpreter launch, its operations uploaded once */
     graph_drop (victim);
-    opvec o = {NULL, 0, 0, 0, 0., c->ax.p != NULL, c->lam.p != NULL};
+    opvec o = {NULL, 0, 0, 0, 0., c->ax.p != NULL, c->lam.p != NULL, 8.};
     r_iteration (g, t, &o, key->nrelax, key->minlevel, key->maxlevel);
     victim->bytes = o.bytes;
     if (o.err) { free (o.v); return FAIL (BMG_ENOMEM); }
@@ -857,7 +874,7 @@ static int t_iteration (bmg_grid * g, struct bmg_tree * t, const tkey * key, dou
     graph_drop (victim);
     {
       /* the same iteration's algorithmic bytes, from its operation list */
-      opvec o = {NULL, 0, 0, 0, 0., c->ax.p != NULL, c->lam.p != NULL};
+      opvec o = {NULL, 0, 0, 0, 0., c->ax.p != NULL, c->lam.p != NULL, 8.};
       r_iteration (g, t, &o, key->nrelax, key->minlevel, key->maxlevel);
       victim->bytes = o.bytes;
       free (o.v);
@@ -887,14 +904,90 @@ static int t_iteration (bmg_grid * g, struct bmg_tree * t, const tkey * key, dou
   return BMG_OK;
 }
 
+/* one iteration of the mixed form: the operations of r_iteration run by
+   the FP32 interpreter (bmg_tree_launch_interp_mixed), captured once per
+   key with the upload of its operations, and replayed */
+static int t_iteration_mixed (bmg_grid * g, struct bmg_tree * t, const tkey * key, double * a,
+                              const double * b, float * const * f32, const tcoefs * c,
+                              const bmg_tree_coef32 * c32, const bmg_tree_bc * abc)
+{
+  struct tgraph * e = NULL, * victim = &t->graphs[0];
+  for (int i = 0; i < NTGRAPH; i++) {
+    struct tgraph * q = &t->graphs[i];
+    if (q->valid && !memcmp (&q->key, key, sizeof *key)) { e = q; break; }
+    if (!q->valid || q->stamp < victim->stamp) victim = q;
+  }
+  if (!e) {
+    graph_drop (victim);
+    opvec o = {NULL, 0, 0, 0, 0., c->ax.p != NULL, c->lam.p != NULL, 4.};
+    r_iteration (g, t, &o, key->nrelax, key->minlevel, key->maxlevel);
+    victim->bytes = o.bytes;
+    if (o.err) { free (o.v); return FAIL (BMG_ENOMEM); }
+    if (cudaMalloc ((void **) &victim->dops, (o.n + 1)*sizeof (bmg_tree_op)) != cudaSuccess ||
+        (o.n && cudaMemcpy (victim->dops, o.v, o.n*sizeof (bmg_tree_op), cudaMemcpyHostToDevice)
+         != cudaSuccess)) {
+      free (o.v);
+      cudaGetLastError ();
+      graph_drop (victim);
+      return FAIL (BMG_ENOMEM);
+    }
+    victim->nops = o.n;
+    free (o.v);
+    const bmg_tree_coef co[3] = {c->ax, c->ay, c->lam};
+    const bmg_tree_bc bcs[2] = {*abc, *abc};
+    cudaGraph_t graph;
+    CKT (cudaStreamBeginCapture (g->stream, cudaStreamCaptureModeThreadLocal));
+    cudaError_t me = cudaMemsetAsync (g->d_maxres, 0, sizeof (unsigned long long), g->stream);
+    int r = me == cudaSuccess ?
+      bmg_tree_launch_interp_mixed (victim->dops, (int) victim->nops, &t->T, a, f32, b,
+                                    t->dflags, co, c32, bcs, g->d_maxres, g->stream) : (int) me;
+    me = cudaMemcpyAsync (g->h_pinned, g->d_maxres, sizeof (double), cudaMemcpyDeviceToHost,
+                          g->stream);
+    cudaError_t ee = cudaStreamEndCapture (g->stream, &graph);
+    if (r) {
+      if (ee == cudaSuccess) cudaGraphDestroy (graph);
+      fprintf (stderr, "bmg: tree interpreter launch (mixed) failed (%d)\n", r);
+      graph_drop (victim);
+      return FAIL (BMG_ECUDA);
+    }
+    CKT (me);
+    CKT (ee);
+    cudaError_t ie = cudaGraphInstantiate (&victim->exec, graph, 0);
+    cudaGraphDestroy (graph);
+    CKT (ie);
+    victim->key = *key;
+    victim->launches = 1;
+    victim->valid = 1;
+    e = victim;
+  }
+  e->stamp = ++t->clock;
+  CKT (cudaGraphLaunch (e->exec, g->stream));
+  g->counters.launches += e->launches;
+  g->counters.bytes += e->bytes;
+  return BMG_OK;
+}
+
+/* the mixed form's FP32 workspace, allocated on its first solve */
+static int t_workspace32 (bmg_grid * g, struct bmg_tree * t)
+{
+  if (t->ws32) return BMG_OK;
+  const size_t n = g->off64[g->depth + 1];
+  CKT (cudaMalloc ((void **) &t->ws32, (size_t) W32_N*n*sizeof (float)));
+  CKT (cudaMemsetAsync (t->ws32, 0, (size_t) W32_N*n*sizeof (float), g->stream));
+  return BMG_OK;
+}
+
 /* mg_solve (poisson.h:139-235) on the tree, Poisson callbacks */
 static int t_solve (bmg_grid * g, field_t * a, field_t * b, const tcoefs * c, int nrelax,
                     field_t * resout, int minlevel, double tolerance, mgstats * out)
 {
   struct bmg_tree * t = g->tree;
-  if (g->precision != BMG_FP64) return FAIL (BMG_EUNSUPPORTED);
+  const int mixed = g->precision == BMG_MIXED;
+  /* the mixed form runs its iterations through the interpreter only */
+  if (mixed && !t->interp) return FAIL (BMG_EUNSUPPORTED);
   int r = bmg_i_workspace (g);
   if (r) return r;
+  if (mixed && (r = t_workspace32 (g, t))) return r;
   if (minlevel > t->depth) minlevel = t->depth;
   if (minlevel < 0) minlevel = 0;
   double * da = bmg_i_ws64 (g, BMG_WS_DA, 0), * tmp = bmg_i_ws64 (g, BMG_WS_DA2, 0);
@@ -912,6 +1005,23 @@ static int t_solve (bmg_grid * g, field_t * a, field_t * b, const tcoefs * c, in
   s.nrelax = nrelax > 0 ? nrelax : 4;
   r = t_residual (g, t, a->buf, b->buf, res, c, &abc, nl);
   if (r) return r;
+  /* mixed form: FP32 copies of the initial residual and of the
+     coefficients the cycle reads (all levels) */
+  const long long n32 = (long long) g->off64[g->depth + 1];
+  float * const f32[3] = {t->ws32 ? t->ws32 + (size_t) W32_DA*n32 : NULL,
+                          t->ws32 ? t->ws32 + (size_t) W32_RES*n32 : NULL,
+                          t->ws32 ? t->ws32 + (size_t) W32_TMP*n32 : NULL};
+  bmg_tree_coef32 c32[3] = {{NULL, c->ax.c}, {NULL, c->ay.c}, {NULL, c->lam.c}};
+  if (mixed) {
+    LT (bmg_tree_launch_to_f32 (res, f32[1], n32, g->stream));
+    const bmg_tree_coef * c64[3] = {&c->ax, &c->ay, &c->lam};
+    for (int k = 0; k < 3; k++)
+      if (c64[k]->p) {
+        float * dst = t->ws32 + (size_t) (W32_AX + k)*n32;
+        LT (bmg_tree_launch_to_f32 (c64[k]->p, dst, n32, g->stream));
+        c32[k].p = dst;
+      }
+  }
   r = read_max (g, &s.resb);
   if (r) return r;
   g->counters.launches += launches;
@@ -920,15 +1030,19 @@ static int t_solve (bmg_grid * g, field_t * a, field_t * b, const tcoefs * c, in
     tolerance = TOLERANCE;
   tkey key;
   memset (&key, 0, sizeof key);
-  key.minlevel = minlevel; key.maxlevel = t->depth; key.relax = g->relax;
-  key.a = a->buf; key.b = b->buf; key.da = da; key.res = res; key.tmp = tmp;
+  key.minlevel = minlevel; key.maxlevel = t->depth; key.relax = g->relax; key.mixed = mixed;
+  key.a = a->buf; key.b = b->buf;
+  key.da = mixed ? (const void *) f32[0] : da;
+  key.res = mixed ? (const void *) f32[1] : res;
+  key.tmp = mixed ? (const void *) f32[2] : tmp;
   key.ax = c->ax; key.ay = c->ay; key.lam = c->lam; key.abc = abc;
   key.stream = g->stream; key.maxres = g->d_maxres; key.pinned = g->h_pinned;
   int status = BMG_OK;
   for (s.i = 0; s.i < NITERMAX && (s.i < NITERMIN || s.resa > tolerance); s.i++) {
     key.nrelax = s.nrelax;
     if (g->timing) CKT (cudaEventRecord (g->ev0, g->stream));
-    r = t_iteration (g, t, &key, a->buf, b->buf, da, res, tmp, c, &abc);
+    r = mixed ? t_iteration_mixed (g, t, &key, a->buf, b->buf, f32, c, c32, &abc)
+              : t_iteration (g, t, &key, a->buf, b->buf, da, res, tmp, c, &abc);
     if (r) return r;
     if (g->timing) CKT (cudaEventRecord (g->ev1, g->stream));
     CKT (cudaStreamSynchronize (g->stream));
@@ -956,9 +1070,17 @@ static int t_solve (bmg_grid * g, field_t * a, field_t * b, const tcoefs * c, in
              s.i, s.resa, s.sum, s.nrelax), fflush (stderr);
     if (status == BMG_OK) status = BMG_ENOTCONV;
   }
-  if (resout && !resout->is_const && resout->face_dim < 0)
+  if (resout && !resout->is_const && resout->face_dim < 0) {
+    if (mixed) {
+      /* the FP64 residual of the final a (the iterations kept it in FP32) */
+      launches = 0;
+      r = t_residual (g, t, a->buf, b->buf, res, c, &abc, nl);
+      if (r) return r;
+      g->counters.launches += launches;
+    }
     CKT (cudaMemcpyAsync (resout->buf, res, g->off64[g->depth + 1]*sizeof (double),
                           cudaMemcpyDeviceToDevice, g->stream));
+  }
   CKT (cudaStreamSynchronize (g->stream));
   *out = s;
   return FAIL (status);

@@ -458,10 +458,13 @@ class TreeGrid(Grid):
     ``get(level=l)``); the solver reads the leaves, whose mask
     ``leaf_mask(l)`` gives.  ``poisson``, ``mg_solve``, ``mg_cycle``,
     ``residual`` and ``restriction`` follow the reference's tree branch.
+    ``precision="mixed"`` runs the solve's cycles in FP32 inside FP64
+    iterative refinement (the residual, a and b stay FP64).
     """
 
-    def __init__(self, maxdepth, L0=1.0, origin=(0.0, 0.0), relax="rbgs", graphs=True):
-        super().__init__(2, maxdepth, L0=L0, origin=origin, relax=relax, precision="fp64",
+    def __init__(self, maxdepth, L0=1.0, origin=(0.0, 0.0), relax="rbgs", graphs=True,
+                 precision="fp64"):
+        super().__init__(2, maxdepth, L0=L0, origin=origin, relax=relax, precision=precision,
                          graphs=graphs)
         self.maxdepth = maxdepth
 

@@ -307,12 +307,12 @@ def run_workload(args, ws, rank, local):
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     clocks = ClockSampler(local)
     if args.workload == "two_phase_tree":
-        g = bmg.TreeGrid(11, relax="rbgs")
+        g = bmg.TreeGrid(11, relax="rbgs", precision=args.precision)
         g.set_stream(torch.cuda.current_stream().cuda_stream)
         a, b, alpha = problems.setup_tree(g, 11, 5, seed=1 + rank)
         zeros = [torch.zeros((1 << l, 1 << l), dtype=torch.float64, device="cuda")
                  for l in range(g.tree_depth + 1)]
-        tol, dtype = TOL, "f64"
+        tol, dtype = TOL, "f64" if args.precision == "fp64" else "f32+f64"
 
         def reset():
             for l, z in enumerate(zeros):
@@ -324,7 +324,8 @@ def run_workload(args, ws, rank, local):
                               "everywhere and cells within 4 cells of r = 0.25 refined up to "
                               "level 11 (%d leaves), tolerance 1e-6, at most 100 V-cycles"
                               % g.leaves,
-                  "grid": "quadtree levels 5-11", "relax": "red-black Gauss-Seidel",
+                  "grid": "quadtree levels 5-11", "form": args.precision,
+                  "relax": "red-black Gauss-Seidel",
                   "parallelism": "replicas" if ws > 1 else "1 gpu"}
     elif args.workload == "random_field_batch":
         from basilisk_b200.autograd import Problem, solve as dsolve
@@ -536,6 +537,28 @@ def run_workload(args, ws, rank, local):
         sys.path.insert(0, os.path.join(ROOT, "tests"))
         from oracle import tree as otree
         import golden_drivers as gd
+        # the error of this form's solution (tolerance 1e-6) against the tree
+        # oracle (red-black, FP64) driven to 1e-9 on the same tree
+        tf = otree.Tree(11, 1.0, (0.0, 0.0))
+        tf.set_relax(otree.RELAX_RBGS)
+        tf.refine(problems.band_refinement(11, 5))
+        gd.two_phase_tree(tf, seed=1)
+        otree.set_niter(nitermax=300)
+        try:
+            fst = tf.poisson(tolerance=1e-9, nrelax=4, minlevel=1)
+        finally:
+            otree.set_niter(nitermax=100)
+        dev_a, ref_a = [], []
+        for l in range(tf.depth + 1):
+            leaf = (tf.flags(l) & otree.LEAF) != 0
+            ref_a.append(tf.get_level(otree.A, l)[leaf])
+            dev_a.append(a.get(level=l)[leaf])
+        ref_a, dev_a = np.concatenate(ref_a), np.concatenate(dev_a)
+        line["error_vs_oracle"] = {
+            args.precision: float(np.abs(dev_a - ref_a).max() / np.abs(ref_a).max()),
+            "oracle_residual": fst["resa"], "oracle_cycles": fst["i"],
+            "note": "max over leaves |a - a_oracle| / max |a_oracle|, this form at residual "
+                    "1e-6, the tree oracle (red-black, FP64) driven to 1e-9"}
         t = otree.Tree(11, 1.0, (0.0, 0.0))
         t.set_relax(otree.RELAX_GS)
         t.refine(problems.band_refinement(11, 5))

@@ -273,6 +273,39 @@ int bmg_dump (bmg_grid * grid, const char * file, const bmg_scalar * list,
 int bmg_restore (bmg_grid * grid, const char * file, const bmg_scalar * list,
                  const char * const * names, double * t, int * iter);
 
+/* ---- decomposition into blocks: grid/multigrid-mpi.h ----------------- */
+
+/* A domain of dims[0] x dims[1] (x dims[2]) blocks, each a grid of the same
+   dimension and depth (the reference's per-rank multigrid, multigrid-mpi.h:
+   94-130): block b sits at Cartesian coordinates c with
+   b = (c0 dims[1] + c1) dims[2] + c2 (MPI_Cart_create's row-major order),
+   and covers cells c_e 2^depth .. (c_e + 1) 2^depth - 1 along direction e;
+   set each block's origin and size accordingly (bmg_origin, bmg_size).
+   periodic[e] makes the domain periodic along e: a direction of a single
+   block is then periodic on that block (bmg_periodic), a direction of
+   several blocks wraps its neighbours and must not be periodic on the
+   blocks.  Blocks may live on different CUDA devices (each created with its
+   device current); the decomposition puts the blocks of a device on one
+   stream of its own, and gives them their own streams back when it is
+   freed.  Every block must create its fields in the same order, so that a
+   field has the same handle in every block.  The solve is FP64. */
+typedef struct bmg_shard bmg_shard;
+int bmg_shard_new (bmg_shard ** shard, bmg_grid * const * blocks, const int * dims,
+                   const int * periodic);
+void bmg_shard_free (bmg_shard * shard);
+/* poisson () (poisson.h:402-441) over the blocks: mg_solve with the
+   boundary exchange of mpi_boundary_level (multigrid-mpi.h:52-85) after
+   every pass, the sum of b and the residual maximum reduced over the
+   blocks (the MPI_Allreduce of common.h:681-718).  Field handles of p are
+   those of every block; minlevel counts a block's levels (at least 1). */
+int bmg_shard_poisson (bmg_shard * shard, struct Poisson p, mgstats * out);
+/* MPI_Dims_create (n, dimension, dims) with all dims free */
+int bmg_shard_dims (int n, int dimension, int * dims);
+/* MPI_Cart_shift of block b: out[side] is the neighbouring block on each
+   side (BMG_RIGHT .. BMG_BACK), -1 on a box side */
+int bmg_shard_neighbours (int dimension, const int * dims, const int * periodic, int b,
+                          int * out);
+
 /* ---- differentiation ----------------------------------------------- */
 
 /* Gradients of a loss l(a) with respect to the coefficients of the solve

@@ -70,6 +70,15 @@ def lib():
     return L
 
 
+def set_niter(nitermax=None, nitermin=None):
+    """The tree oracle's NITERMAX / NITERMIN (poisson.h:102)."""
+    L = lib()
+    if nitermax is not None:
+        ctypes.c_int.in_dll(L, "ot_NITERMAX").value = nitermax
+    if nitermin is not None:
+        ctypes.c_int.in_dll(L, "ot_NITERMIN").value = nitermin
+
+
 def _dp(a):
     return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
 

@@ -101,11 +101,13 @@ class GpuTree:
     ``TreeGrid``, so that the tree programs of ``golden_drivers`` run on
     both; the field ids are the oracle's."""
 
-    def __init__(self, maxdepth, origin=(0.0, 0.0), relax="rbgs", L0=1.0, graphs=True):
+    def __init__(self, maxdepth, origin=(0.0, 0.0), relax="rbgs", L0=1.0, graphs=True,
+                 precision="fp64"):
         import basilisk_b200 as bmg
         from oracle import tree as ot
         self.ot = ot
-        self.g = bmg.TreeGrid(maxdepth, L0=L0, origin=origin, relax=relax, graphs=graphs)
+        self.g = bmg.TreeGrid(maxdepth, L0=L0, origin=origin, relax=relax, graphs=graphs,
+                              precision=precision)
         self.L0, self.X0, self.Y0 = float(L0), float(origin[0]), float(origin[1])
         self.f = {ot.A: self.g.scalar(), ot.B: self.g.scalar(), ot.RES: self.g.scalar(),
                   ot.DA: self.g.scalar()}

@@ -141,3 +141,46 @@ def test_tree_interpreter_matches_launch_path(relax):
         assert si[k] == sl[k], (k, si, sl)
     np.testing.assert_array_equal(ai, al)
     assert ci["launches"] < cl["launches"], (ci, cl)
+
+
+def test_tree_mixed_form_against_the_oracle():
+    """The mixed form on the band tree (FP32 cycles inside FP64 iterative
+    refinement): it reaches the tolerance, its error against the tree
+    oracle driven to 1e-9 (124 cycles) is no worse than a small multiple of
+    the FP64 form's at the same tolerance (1e-6), and driven on to 1e-9 it
+    is close to the oracle's solution."""
+    import basilisk_b200 as bmg
+    depth, base = 8, 4
+    ot.set_niter(nitermax=400)
+    try:
+        tc = c4_problem(lambda d, o: _cpu_rbgs(d, o), depth, base)
+        sc = tc.poisson(tolerance=1e-9, nrelax=4, minlevel=1)
+    finally:
+        ot.set_niter(nitermax=100)
+    assert sc["resa"] <= 1e-9, sc
+    ref = leaf_values(tc, ot.A)
+    errs = {}
+    for prec in ("fp64", "mixed"):
+        tg = c4_problem(lambda d, o: GpuTree(d, o, relax="rbgs", precision=prec), depth, base)
+        st = tg.poisson(tolerance=1e-6, nrelax=4, minlevel=1)
+        assert st["resa"] <= 1e-6, (prec, st)
+        errs[prec] = float(np.abs(leaf_values(tg, ot.A) - ref).max() / np.abs(ref).max())
+        if prec == "mixed":
+            bmg.set_niter(nitermax=400)
+            try:
+                st = tg.poisson(tolerance=1e-9, nrelax=4, minlevel=1)
+            finally:
+                bmg.set_niter(nitermax=100)
+            assert st["resa"] <= 1e-9, st
+            errs["mixed_1e-9"] = float(np.abs(leaf_values(tg, ot.A) - ref).max()
+                                       / np.abs(ref).max())
+        tg.close()
+    print("tree errors against the oracle:", errs)
+    assert errs["mixed"] <= 4 * errs["fp64"] + 1e-12, errs
+    assert errs["mixed_1e-9"] <= 1e-6, errs
+
+
+def _cpu_rbgs(depth, origin):
+    t = ot.Tree(depth, 1.0, origin)
+    t.set_relax(ot.RELAX_RBGS)
+    return t
