@@ -50,8 +50,6 @@ struct bmg_grid {
   unsigned long long * d_maxres;
   int cluster_levels;   /* cluster kernels for the middle levels of the mixed form
                            (on unless BMG_NO_CLUSTER is set in the environment) */
-  int fused3d;          /* one launch per red-black sweep on 3D levels (on when
-                           BMG_FUSED3D is set in the environment) */
   double * d_sum, * d_partials;
   int npartials;
   double * h_pinned;

@@ -170,7 +170,6 @@ int bmg_grid_new (bmg_grid ** out, int dim, int depth)
   g->nfields = 1;   /* handle 0 means "unset" */
   CK (cudaMalloc ((void **) &g->d_maxres, 2*sizeof (unsigned long long)));
   g->cluster_levels = getenv ("BMG_NO_CLUSTER") == NULL;
-  g->fused3d = getenv ("BMG_FUSED3D") != NULL;
   g->npartials = bmg_sum_partials (dim, g->g64[depth]);
   CK (cudaMalloc ((void **) &g->d_partials, (g->npartials + 1)*sizeof (double)));
   CK (cudaMalloc ((void **) &g->d_sum, 2*sizeof (double)));
@@ -941,14 +940,6 @@ static int cycle_launches (bmg_grid * g, field_t * a, const levels_t * lv, const
         if (timed) w->relax_bytes += ncells (g, L)*16.;
       }
     }
-    else if (g->relax == BMG_RELAX_RBGS && dim == 3 && g->fused3d && bmg_relax3d_rb_ok (gl.n))
-      /* a complete red-black sweep per launch, ping-pong buffers */
-      for (int i = 0; i < nrelax; i++) {
-        CL (bmg_launch_relax3d_rb (st, gl, oth[l], cur[l], lv->res[l], al, la, delta_of (g, l),
-                                   dabc, s));
-        void * t = cur[l]; cur[l] = oth[l]; oth[l] = t;
-        launches++;
-      }
     else
       for (int i = 0; i < nrelax; i++) {
         if (g->relax == BMG_RELAX_JACOBI) {

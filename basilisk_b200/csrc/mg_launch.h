@@ -147,14 +147,6 @@ int bmg_launch_level_cluster (int st, bmg_geom g, void * out, const void * res,
                               const bmg_bcdesc * bc, int nrelax, bmg_geom gc, const void * coarse,
                               cudaStream_t s);
 
-/* one complete red-black sweep of a 3D level (n >= 16, a multiple of 16)
-   in one launch (mg_fused3d.cu): reads in, writes out (out != in) with its
-   ghost images; bit-identical to a red then a black bmg_launch_relax */
-int bmg_relax3d_rb_ok (int n);
-int bmg_launch_relax3d_rb (int st, bmg_geom g, void * out, const void * in, const void * rhs,
-                           const bmg_coef * alpha, bmg_coef lambda, double Delta,
-                           const bmg_bcdesc * bc, cudaStream_t s);
-
 /* one level of the single-CTA bottom solve */
 typedef struct {
   bmg_geom g;
