@@ -398,7 +398,7 @@ static int block_coefs (bmg_grid * g, const struct Poisson * p, blk_t * k)
 
 /* max over the blocks of their residual maxima (non-negative doubles, or
    NaN, compared by their bits as the kernels' atomicMax does) */
-static int residual_all (bmg_shard * s, blk_t * k, double * maxres)
+static int residual_all (bmg_shard * s, blk_t * k, double * maxres, cudaEvent_t done)
 {
   const int L = s->blk[0]->depth;
   int r = exchange (s, L, ptr_a, k);
@@ -410,6 +410,17 @@ static int residual_all (bmg_shard * s, blk_t * k, double * maxres)
     CLS (bmg_launch_residual (g->dim, BMG_ST_F64, g->g64[L], g->g64[L], k[b].a->lv[L],
                               k[b].b->lv[L], k[b].alpha[L], k[b].lambda[L], delta_of (g, L),
                               bmg_i_ws64 (g, BMG_WS_RES, L), g->d_maxres, g->stream));
+  }
+  if (done) {
+    /* the end of the cycle's work on every device, on block 0's stream */
+    int r2 = sync_devices (s);
+    if (r2) return r2;
+    CKS (cudaSetDevice (s->blk[0]->device));
+    CKS (cudaEventRecord (done, s->blk[0]->stream));
+  }
+  for (int b = 0; b < s->nb; b++) {
+    bmg_grid * g = s->blk[b];
+    CKS (cudaSetDevice (g->device));
     CKS (cudaMemcpyAsync (g->h_pinned, g->d_maxres, sizeof (double),
                           cudaMemcpyDeviceToHost, g->stream));
   }
@@ -428,6 +439,31 @@ static int residual_all (bmg_shard * s, blk_t * k, double * maxres)
 
 /* mg_cycle (poisson.h:32-90) over the blocks, one pass per launch, with
    the boundary exchanges of the single-grid cycle */
+static long long cells_of (int dim, int l)
+{
+  long long c = 1;
+  for (int d = 0; d < dim; d++) c *= 1LL << l;
+  return c;
+}
+
+/* the algorithmic bytes of one cycle over all blocks (each array pass once,
+   8 bytes a value, ghosts excluded), as the single-grid solve counts them */
+static double cycle_bytes (const bmg_shard * s, const blk_t * k, int nrelax, int minlevel,
+                           int maxlevel)
+{
+  const int dim = s->dim, L = s->blk[0]->depth;
+  const double narr = 3. + (k->alpha_stored ? dim : 0) + (k->lambda_stored ? 1 : 0);
+  double b = 0.;
+  for (int l = L - 1; l >= minlevel; l--) b += 8.*(cells_of (dim, l + 1) + cells_of (dim, l));
+  for (int l = minlevel; l <= maxlevel; l++) {
+    b += 8.*cells_of (dim, l) + (l > minlevel ? 8.*cells_of (dim, l - 1) : 0.);
+    b += nrelax*narr*8.*cells_of (dim, l);
+  }
+  b += 24.*cells_of (dim, L);                                        /* a += da */
+  b += 8.*cells_of (dim, L)*(3. + (k->alpha_stored ? dim : 0) + (k->lambda_stored ? 1 : 0));
+  return b*s->nb;
+}
+
 static int shard_cycle (bmg_shard * s, blk_t * k, int nrelax, int minlevel, int maxlevel,
                         long long * launches)
 {
@@ -546,14 +582,30 @@ int bmg_shard_poisson (bmg_shard * s, struct Poisson p, mgstats * out)
   }
   if (r) { free (k); cudaSetDevice (cur); return FAIL (BMG_ECUDA); }
   st.nrelax = p.nrelax > 0 ? p.nrelax : 4;
-  r = residual_all (s, k, &st.resb);
+  r = residual_all (s, k, &st.resb, NULL);
   double resb = st.resa = st.resb;
   int status = BMG_OK;
+  bmg_grid * g0 = s->blk[0];
   for (st.i = 0; !r && st.i < NITERMAX && (st.i < NITERMIN || st.resa > tolerance); st.i++) {
-    r = shard_cycle (s, k, st.nrelax, minlevel, L, &launches);
-    if (!r) r = residual_all (s, k, &st.resa);
+    /* with timing on, the cycle and its residual between two events on
+       block 0's stream, which waits for every device at both ends */
+    if (g0->timing) {
+      r = sync_devices (s);
+      if (!r && (cudaSetDevice (g0->device) != cudaSuccess ||
+                 cudaEventRecord (g0->ev0, g0->stream) != cudaSuccess)) r = FAIL (BMG_ECUDA);
+    }
+    const double bytes = cycle_bytes (s, k, st.nrelax, minlevel, L);
+    if (!r) r = shard_cycle (s, k, st.nrelax, minlevel, L, &launches);
+    if (!r) r = residual_all (s, k, &st.resa, g0->timing ? g0->ev1 : NULL);
     if (r) break;
-    for (int b = 0; b < s->nb; b++) s->blk[b]->counters.cycles++;
+    g0->counters.cycles++;
+    g0->counters.bytes += bytes;
+    if (g0->timing) {
+      float ms = 0.f;
+      cudaSetDevice (g0->device);
+      if (cudaEventElapsedTime (&ms, g0->ev0, g0->ev1) != cudaSuccess) { r = FAIL (BMG_ECUDA); break; }
+      g0->counters.cycle_ms += ms;
+    }
     if (!isfinite (st.resa)) { status = BMG_ENAN; st.i++; break; }
     /* nrelax adaptation (poisson.h:198-204) */
     if (st.resa > tolerance) {

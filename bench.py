@@ -374,6 +374,38 @@ def run_workload(args, ws, rank, local):
                   "relax": "red-black Gauss-Seidel",
                   "lanes": "%d grids on their own streams, one host thread each" % args.lanes,
                   "parallelism": "replicas" if ws > 1 else "1 gpu"}
+    elif args.workload == "sharded_2d":
+        from basilisk_b200.shard import ShardedGrid, dims_create
+        import math
+        dims = dims_create(args.blocks, 2)
+        if dims[0] != dims[1] or dims[0] & (dims[0] - 1):
+            raise SystemExit("--blocks must give a square power-of-two arrangement (4, 16, ...)")
+        prob = problems.two_phase_2d(depth=DEPTH, seed=1 + rank)
+        ndev = torch.cuda.device_count()
+        devices = [d % ndev for d in range(args.blocks)] if ws == 1 else [local]
+        sg = ShardedGrid(2, DEPTH - int(math.log2(dims[0])), dims=dims, relax="rbgs",
+                         devices=devices)
+        a = sg.scalar()
+        for side in range(4):
+            a.bc(side, "dirichlet", 0.0)
+        b = sg.scalar(prob["b"])
+        alpha = sg.face_vector(prob["alpha"])
+        zero = np.zeros(prob["b"].shape)
+        tol, dtype = TOL, "f64"
+
+        def reset():
+            a.set(zero)
+
+        def solve():
+            return sg.poisson(a, b, alpha=alpha, tolerance=tol)
+        config = {"workload": "sharded_2d: the two_phase_2d problem (2048^2, tolerance 1e-6) "
+                              "decomposed into %dx%d blocks of %d^2 (grid/multigrid-mpi.h), FP64, "
+                              "ghost slabs exchanged after every pass" % (dims[0], dims[1],
+                                                                          2048 // dims[0]),
+                  "grid": "2048x2048 as %dx%d blocks" % dims, "relax": "red-black Gauss-Seidel",
+                  "devices": "%d block(s) per device on %d device(s)"
+                             % (max(1, args.blocks // max(1, len(set(devices)))), len(set(devices))),
+                  "parallelism": "replicas" if ws > 1 else "1 process"}
     elif args.workload == "viscosity_2d":
         depth = 11
         n = 1 << depth
@@ -428,7 +460,12 @@ def run_workload(args, ws, rank, local):
                   "grid": "256^3 (depth 8)", "form": args.precision,
                   "relax": "red-black Gauss-Seidel",
                   "parallelism": "replicas" if ws > 1 else "1 gpu"}
-    grids = [ln.grid for ln in pr.lanes] if args.workload == "random_field_batch" else [g]
+    if args.workload == "random_field_batch":
+        grids = [ln.grid for ln in pr.lanes]
+    elif args.workload == "sharded_2d":
+        grids = sg.blocks
+    else:
+        grids = [g]
     for gg in grids:
         gg.set_timing(True)
     clocks.start()
@@ -616,11 +653,13 @@ def main():
                     help="profiling run: only this form, no e2e, no CPU baseline, no JSON")
     ap.add_argument("--depth", type=int, default=DEPTH, help="grid depth (profiling runs)")
     ap.add_argument("--workload", choices=["two_phase_2d", "two_phase_tree", "helmholtz_3d",
-                                           "random_field_batch", "viscosity_2d"],
+                                           "random_field_batch", "viscosity_2d", "sharded_2d"],
                     default="two_phase_2d",
                     help="two_phase_2d: the headline; the others print their own line")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64",
                     help="form of the helmholtz_3d and random_field_batch workloads")
+    ap.add_argument("--blocks", type=int, default=4,
+                    help="sharded_2d: number of blocks (a square power-of-two arrangement)")
     ap.add_argument("--lanes", type=int, default=8,
                     help="random_field_batch: grids solving instances concurrently")
     args = ap.parse_args()
