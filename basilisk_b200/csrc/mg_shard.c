@@ -49,6 +49,17 @@
 #include "mg_grid.h"
 
 #define MAXB 4096
+#define NSGRAPH 8
+
+/* a captured iteration (cycle and residual) and what it depends on */
+typedef struct { int nrelax, minlevel; unsigned long long h; } skey;
+struct sgraph {
+  int valid;
+  skey key;
+  cudaGraphExec_t exec;
+  long long launches;
+  unsigned long long stamp;
+};
 
 struct bmg_shard {
   int dim, nb, dims[3], periodic[3];
@@ -59,6 +70,8 @@ struct bmg_shard {
   cudaStream_t stream[16];    /* one stream per device */
   cudaEvent_t ev[16];
   int * bdev;                 /* device slot of each block */
+  struct sgraph graphs[NSGRAPH];   /* one device: iterations captured in CUDA graphs */
+  unsigned long long clock;
 };
 
 #define FAIL(s) bmg_i_fail (s)
@@ -146,6 +159,8 @@ void bmg_shard_free (bmg_shard * s)
       cudaStreamSynchronize (s->blk[b]->stream);
       bmg_set_stream (s->blk[b], NULL);
     }
+  for (int i = 0; i < NSGRAPH; i++)
+    if (s->graphs[i].valid) cudaGraphExecDestroy (s->graphs[i].exec);
   for (int k = 0; k < s->ndev; k++) {
     cudaSetDevice (s->dev[k]);
     if (s->stream[k]) cudaStreamDestroy (s->stream[k]);
@@ -396,9 +411,10 @@ static int block_coefs (bmg_grid * g, const struct Poisson * p, blk_t * k)
   return BMG_OK;
 }
 
-/* max over the blocks of their residual maxima (non-negative doubles, or
-   NaN, compared by their bits as the kernels' atomicMax does) */
-static int residual_all (bmg_shard * s, blk_t * k, double * maxres, cudaEvent_t done)
+/* the residual of every block (after the exchange of a), each block's
+   maximum into its pinned host word; with done, an event on block 0's
+   stream after every device's residual */
+static int residual_issue (bmg_shard * s, blk_t * k, cudaEvent_t done)
 {
   const int L = s->blk[0]->depth;
   int r = exchange (s, L, ptr_a, k);
@@ -412,7 +428,6 @@ static int residual_all (bmg_shard * s, blk_t * k, double * maxres, cudaEvent_t 
                               bmg_i_ws64 (g, BMG_WS_RES, L), g->d_maxres, g->stream));
   }
   if (done) {
-    /* the end of the cycle's work on every device, on block 0's stream */
     int r2 = sync_devices (s);
     if (r2) return r2;
     CKS (cudaSetDevice (s->blk[0]->device));
@@ -424,6 +439,13 @@ static int residual_all (bmg_shard * s, blk_t * k, double * maxres, cudaEvent_t 
     CKS (cudaMemcpyAsync (g->h_pinned, g->d_maxres, sizeof (double),
                           cudaMemcpyDeviceToHost, g->stream));
   }
+  return BMG_OK;
+}
+
+/* max over the blocks of their residual maxima (non-negative doubles, or
+   NaN, compared by their bits as the kernels' atomicMax does) */
+static int residual_collect (bmg_shard * s, double * maxres)
+{
   unsigned long long m = 0;
   for (int b = 0; b < s->nb; b++) {
     bmg_grid * g = s->blk[b];
@@ -435,6 +457,12 @@ static int residual_all (bmg_shard * s, blk_t * k, double * maxres, cudaEvent_t 
   }
   memcpy (maxres, &m, sizeof m);
   return BMG_OK;
+}
+
+static int residual_all (bmg_shard * s, blk_t * k, double * maxres, cudaEvent_t done)
+{
+  int r = residual_issue (s, k, done);
+  return r ? r : residual_collect (s, maxres);
 }
 
 /* mg_cycle (poisson.h:32-90) over the blocks, one pass per launch, with
@@ -535,6 +563,57 @@ static int shard_cycle (bmg_shard * s, blk_t * k, int nrelax, int minlevel, int 
   return BMG_OK;
 }
 
+/* one iteration (cycle and residual) when every block lives on one device
+   (one stream): captured into a CUDA graph once per key -- nrelax,
+   minlevel and everything the launches read (the blocks' fields,
+   coefficients and boundary conditions, hashed) -- and replayed; returns
+   the number of operations it stands for in *launches */
+static unsigned long long hash_blocks (const blk_t * k, int nb)
+{
+  unsigned long long h = 1469598103934665603ULL;
+  const unsigned char * c = (const unsigned char *) k;
+  for (size_t i = 0; i < (size_t) nb*sizeof (blk_t); i++) { h ^= c[i]; h *= 1099511628211ULL; }
+  return h;
+}
+
+static int iteration_graph (bmg_shard * s, blk_t * k, int nrelax, int minlevel,
+                            long long * launches)
+{
+  const int L = s->blk[0]->depth;
+  skey key;
+  memset (&key, 0, sizeof key);
+  key.nrelax = nrelax; key.minlevel = minlevel; key.h = hash_blocks (k, s->nb);
+  struct sgraph * e = NULL, * victim = &s->graphs[0];
+  for (int i = 0; i < NSGRAPH; i++) {
+    struct sgraph * q = &s->graphs[i];
+    if (q->valid && !memcmp (&q->key, &key, sizeof key)) { e = q; break; }
+    if (!q->valid || q->stamp < victim->stamp) victim = q;
+  }
+  CKS (cudaSetDevice (s->dev[0]));
+  if (!e) {
+    if (victim->valid) { cudaGraphExecDestroy (victim->exec); victim->valid = 0; }
+    long long nl = 0;
+    cudaGraph_t graph;
+    CKS (cudaStreamBeginCapture (s->stream[0], cudaStreamCaptureModeThreadLocal));
+    int r = shard_cycle (s, k, nrelax, minlevel, L, &nl);
+    if (!r) r = residual_issue (s, k, NULL);
+    cudaError_t ee = cudaStreamEndCapture (s->stream[0], &graph);
+    if (r) { if (ee == cudaSuccess) cudaGraphDestroy (graph); return r; }
+    CKS (ee);
+    cudaError_t ie = cudaGraphInstantiate (&victim->exec, graph, 0);
+    cudaGraphDestroy (graph);
+    CKS (ie);
+    victim->key = key;
+    victim->launches = nl + 3*s->nb;
+    victim->valid = 1;
+    e = victim;
+  }
+  e->stamp = ++s->clock;
+  CKS (cudaGraphLaunch (e->exec, s->stream[0]));
+  *launches += e->launches;
+  return BMG_OK;
+}
+
 int bmg_shard_poisson (bmg_shard * s, struct Poisson p, mgstats * out)
 {
   if (!s || !out) return FAIL (BMG_EINVAL);
@@ -595,8 +674,17 @@ int bmg_shard_poisson (bmg_shard * s, struct Poisson p, mgstats * out)
                  cudaEventRecord (g0->ev0, g0->stream) != cudaSuccess)) r = FAIL (BMG_ECUDA);
     }
     const double bytes = cycle_bytes (s, k, st.nrelax, minlevel, L);
-    if (!r) r = shard_cycle (s, k, st.nrelax, minlevel, L, &launches);
-    if (!r) r = residual_all (s, k, &st.resa, g0->timing ? g0->ev1 : NULL);
+    if (s->ndev == 1 && g0->use_graphs) {
+      /* one stream: the iteration as a captured graph */
+      if (!r) r = iteration_graph (s, k, st.nrelax, minlevel, &launches);
+      if (!r && g0->timing && cudaEventRecord (g0->ev1, g0->stream) != cudaSuccess)
+        r = FAIL (BMG_ECUDA);
+      if (!r) r = residual_collect (s, &st.resa);
+    }
+    else {
+      if (!r) r = shard_cycle (s, k, st.nrelax, minlevel, L, &launches);
+      if (!r) r = residual_all (s, k, &st.resa, g0->timing ? g0->ev1 : NULL);
+    }
     if (r) break;
     g0->counters.cycles++;
     g0->counters.bytes += bytes;
