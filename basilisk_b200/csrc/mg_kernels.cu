@@ -926,6 +926,45 @@ __global__ void k_project_faces (bmg_geom g, int e, double * __restrict__ u, Coe
   }
 }
 
+/* ---------------------------------------------------------------- */
+/* ghost slabs of a decomposed domain                                */
+/* ---------------------------------------------------------------- */
+
+/* at most this many blocks per launch (the descriptors go by value) */
+#define HALO_BATCH 128
+struct HaloBatch { bmg_halo h[HALO_BATCH]; };
+
+/* element offset of position t of the slab at index i of direction e: the
+   slab spans -1..n of each other direction (ghosts included) */
+template <int DIM>
+__device__ __forceinline__ long long slab_elem (const bmg_geom & g, int e, int i, int t)
+{
+  if (DIM == 1) return (long long) g.xo + i;
+  const int w = g.n + 2;
+  if (DIM == 2)
+    return e == 0 ? (long long) (i + 1)*g.P + g.xo + (t - 1) : (long long) t*g.P + g.xo + i;
+  const int u = t/w, v = t - u*w;      /* the two other directions, in order */
+  if (e == 0) return (long long) (i + 1)*g.plane + (long long) u*g.P + g.xo + (v - 1);
+  if (e == 1) return (long long) u*g.plane + (long long) (i + 1)*g.P + g.xo + (v - 1);
+  return (long long) u*g.plane + (long long) v*g.P + g.xo + i;
+}
+
+/* blockIdx.y: the block; blockIdx.z: the side (0: ghost slab -1 from the
+   low neighbour's slab n - 1, 1: ghost slab n from the high neighbour's
+   slab 0) */
+template <int DIM>
+__global__ void k_halo (bmg_geom g, int e, HaloBatch hb)
+{
+  const bmg_halo & h = hb.h[blockIdx.y];
+  const double * src = blockIdx.z ? h.hi : h.lo;
+  if (!src) return;
+  const long long S = DIM == 1 ? 1 : DIM == 2 ? g.n + 2 : (long long) (g.n + 2)*(g.n + 2);
+  const long long t = (long long) blockIdx.x*blockDim.x + threadIdx.x;
+  if (t >= S) return;
+  const int gi = blockIdx.z ? g.n : -1, si = blockIdx.z ? 0 : g.n - 1;
+  h.dst[slab_elem<DIM> (g, e, gi, (int) t)] = src[slab_elem<DIM> (g, e, si, (int) t)];
+}
+
 } // namespace
 
 
@@ -1158,6 +1197,24 @@ int bmg_launch_fill (int dim, int st, bmg_geom g, void * f, double v, cudaStream
   if (st == BMG_ST_F64) k_fill<double><<<nb, 256, 0, s>>> ((double *) f, g.size, v);
   else k_fill<float><<<nb, 256, 0, s>>> ((float *) f, g.size, (float) v);
   return status_of_launch ();
+}
+
+int bmg_launch_halo (int dim, bmg_geom g, int e, const bmg_halo * blocks, int nb, cudaStream_t s)
+{
+  const long long S = dim == 1 ? 1 : dim == 2 ? g.n + 2 : (long long) (g.n + 2)*(g.n + 2);
+  const int gx = (int) ((S + 255)/256);
+  for (int b0 = 0; b0 < nb; b0 += HALO_BATCH) {
+    HaloBatch hb;
+    const int m = nb - b0 < HALO_BATCH ? nb - b0 : HALO_BATCH;
+    for (int k = 0; k < m; k++) hb.h[k] = blocks[b0 + k];
+    dim3 grid (gx, m, 2);
+    if (dim == 1) k_halo<1><<<grid, 256, 0, s>>> (g, e, hb);
+    else if (dim == 2) k_halo<2><<<grid, 256, 0, s>>> (g, e, hb);
+    else k_halo<3><<<grid, 256, 0, s>>> (g, e, hb);
+    const int st = status_of_launch ();
+    if (st) return st;
+  }
+  return 0;
 }
 
 int bmg_launch_face_wrap (int dim, bmg_geom g, int face_dim, double * f, cudaStream_t s)

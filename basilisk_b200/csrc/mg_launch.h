@@ -122,6 +122,16 @@ int bmg_launch_adjoint_cells (int dim, bmg_geom g, const double * mu, const doub
 
 int bmg_launch_face_wrap (int dim, bmg_geom g, int face_dim, double * f, cudaStream_t s);
 
+/* ghost slabs of direction e of nb blocks' level arrays (geometry g), for
+   the decomposed solve: the ghost slab -1 of dst takes slab n - 1 of lo,
+   the ghost slab n takes slab 0 of hi (NULL: that side is not
+   exchanged); a slab spans -1..n of the other directions, ghosts included,
+   so that exchanging the directions in order fills edges and corners from
+   the diagonal blocks.  lo and hi may be another device's memory (peer
+   access enabled). */
+typedef struct { double * dst; const double * lo, * hi; } bmg_halo;
+int bmg_launch_halo (int dim, bmg_geom g, int e, const bmg_halo * blocks, int nb, cudaStream_t s);
+
 /* fused red-black relaxation (mg_fused.cu) */
 int bmg_tile_sweeps (int st, int n);   /* sweeps one tile launch can do on an n x n level */
 /* whether the tile launch of an n x n level can apply the correction: with

@@ -16,13 +16,13 @@
  *
  * Here every block is a bmg_grid on a CUDA device, and one host thread
  * drives all the blocks of the decomposition: the blocks of one device
- * share one stream, the exchange is a set of device copies (each ghost
- * slab copied straight from the neighbour's level array into the
- * receiver's: cudaMemcpyAsync for the contiguous x slabs, cudaMemcpy2DAsync
- * for the strided y and z slabs; peer copies over NVLink when the
- * neighbour lives on another device), ordered across devices by events,
- * and the reductions are the maximum / sum of the blocks' values on the
- * host, which reads them back every cycle as the single-grid solve does.
+ * share one stream, the exchange of a direction is one kernel per device
+ * (bmg_launch_halo) that copies every neighbour's edge slab straight into
+ * its blocks' ghost slabs -- reading the neighbour by peer access over
+ * NVLink when it lives on another device -- ordered across devices by
+ * events, and the reductions are the maximum / sum of the blocks' values
+ * on the host, which reads them back every cycle as the single-grid solve
+ * does.
  *
  * Boundary conditions: a side of a block that faces another block keeps
  * the field's box condition type (its kernels write box images there,
@@ -49,17 +49,6 @@
 #include "mg_grid.h"
 
 #define MAXB 4096
-#define NSGRAPH 8
-
-/* a captured iteration (cycle and residual) and what it depends on */
-typedef struct { int nrelax, minlevel; unsigned long long h; } skey;
-struct sgraph {
-  int valid;
-  skey key;
-  cudaGraphExec_t exec;
-  long long launches;
-  unsigned long long stamp;
-};
 
 struct bmg_shard {
   int dim, nb, dims[3], periodic[3];
@@ -70,8 +59,8 @@ struct bmg_shard {
   cudaStream_t stream[16];    /* one stream per device */
   cudaEvent_t ev[16];
   int * bdev;                 /* device slot of each block */
-  struct sgraph graphs[NSGRAPH];   /* one device: iterations captured in CUDA graphs */
-  unsigned long long clock;
+  bmg_halo * halo;            /* exchange descriptors, one per block */
+  long long nhalo;            /* exchange launches */
 };
 
 #define FAIL(s) bmg_i_fail (s)
@@ -159,14 +148,12 @@ void bmg_shard_free (bmg_shard * s)
       cudaStreamSynchronize (s->blk[b]->stream);
       bmg_set_stream (s->blk[b], NULL);
     }
-  for (int i = 0; i < NSGRAPH; i++)
-    if (s->graphs[i].valid) cudaGraphExecDestroy (s->graphs[i].exec);
   for (int k = 0; k < s->ndev; k++) {
     cudaSetDevice (s->dev[k]);
     if (s->stream[k]) cudaStreamDestroy (s->stream[k]);
     if (s->ev[k]) cudaEventDestroy (s->ev[k]);
   }
-  free (s->blk); free (s->nbr); free (s->bdev);
+  free (s->blk); free (s->nbr); free (s->bdev); free (s->halo);
   free (s);
 }
 
@@ -203,7 +190,8 @@ int bmg_shard_new (bmg_shard ** out, bmg_grid * const * blocks, const int * dims
   s->blk = calloc (nb, sizeof (bmg_grid *));
   s->nbr = calloc (nb, sizeof *s->nbr);
   s->bdev = calloc (nb, sizeof (int));
-  if (!s->blk || !s->nbr || !s->bdev) { bmg_shard_free (s); return FAIL (BMG_ENOMEM); }
+  s->halo = calloc (nb, sizeof (bmg_halo));
+  if (!s->blk || !s->nbr || !s->bdev || !s->halo) { bmg_shard_free (s); return FAIL (BMG_ENOMEM); }
   for (int b = 0; b < nb; b++) {
     int k = devslot (s, blocks[b]->device);
     if (k < 0) {
@@ -265,67 +253,37 @@ static int sync_devices (bmg_shard * s)
   return BMG_OK;
 }
 
-/* the element offset of slab index i (-1..n) of direction e in a level,
-   and its copy shape: height rows of width elements, pitch elements apart */
-typedef struct { long long off; size_t width, height, pitch; } slab_t;
-
-static slab_t slab_of (int dim, const bmg_geom * g, int e, int i)
-{
-  slab_t r;
-  const int n = g->n;
-  if (dim == 1) {
-    r.off = g->xo + i; r.width = 1; r.height = 1; r.pitch = 1;
-  }
-  else if (e == 0) {
-    /* x: the whole padded slab of the first index (a row in 2D, a plane in 3D) */
-    r.off = (long long) (i + 1)*g->plane; r.width = (size_t) g->plane; r.height = 1; r.pitch = 0;
-  }
-  else if (dim == 2) {
-    /* y of 2D: column j = i, rows -1..n */
-    r.off = g->xo + i; r.width = 1; r.height = n + 2; r.pitch = g->P;
-  }
-  else if (e == 1) {
-    /* y of 3D: for each x slab, the row j = i with its k ghosts */
-    r.off = (long long) (i + 1)*g->P + g->xo - 1; r.width = n + 2; r.height = n + 2;
-    r.pitch = (size_t) g->plane;
-  }
-  else {
-    /* z of 3D: element k = i of every row (plane = (n + 2) P) */
-    r.off = g->xo + i; r.width = 1; r.height = (size_t) (n + 2)*(n + 2); r.pitch = g->P;
-  }
-  return r;
-}
-
 /* mpi_boundary_level (multigrid-mpi.h:52-85) of a level array of every
-   block: ptr (b) is the level-l array of block b */
+   block: ptr (b) is the level-l array of block b.  Direction by direction,
+   one bmg_launch_halo per device copies the neighbours' edge slabs into
+   the ghost slabs of its blocks (reading a neighbour on another device by
+   peer access); every device has finished a direction before any starts
+   the next, so that the slabs of the later directions carry the ghosts of
+   the earlier ones (edges and corners). */
 typedef double * (*lvptr_t) (bmg_shard * s, int b, int l, void * data);
 
 static int exchange (bmg_shard * s, int l, lvptr_t ptr, void * data)
 {
+  const bmg_geom g = s->blk[0]->g64[l];
   for (int e = 0; e < s->dim; e++) {
     if (s->dims[e] == 1) continue;     /* nothing to exchange: box or own periodic images */
     int r = sync_devices (s);
     if (r) return r;
-    for (int b = 0; b < s->nb; b++) {
-      const bmg_geom * g = &s->blk[b]->g64[l];
-      const int n = g->n;
-      double * dst = ptr (s, b, l, data);
-      for (int hi = 0; hi < 2; hi++) {
-        const int nb = s->nbr[b][2*e + (hi ? 0 : 1)];
-        if (nb < 0) continue;
-        /* my ghost slab (n or -1) <- the neighbour's first or last slab */
-        const slab_t sd = slab_of (s->dim, g, e, hi ? n : -1);
-        const slab_t ss = slab_of (s->dim, g, e, hi ? 0 : n - 1);
-        const double * src = ptr (s, nb, l, data);
-        CKS (cudaSetDevice (s->blk[b]->device));
-        if (sd.height == 1)
-          CKS (cudaMemcpyAsync (dst + sd.off, src + ss.off, sd.width*sizeof (double),
-                                cudaMemcpyDefault, s->stream[s->bdev[b]]));
-        else
-          CKS (cudaMemcpy2DAsync (dst + sd.off, sd.pitch*sizeof (double), src + ss.off,
-                                  ss.pitch*sizeof (double), sd.width*sizeof (double),
-                                  sd.height, cudaMemcpyDefault, s->stream[s->bdev[b]]));
+    for (int k = 0; k < s->ndev; k++) {
+      int m = 0;
+      for (int b = 0; b < s->nb; b++) {
+        if (s->bdev[b] != k) continue;
+        const int lo = s->nbr[b][2*e + 1], hi = s->nbr[b][2*e];
+        if (lo < 0 && hi < 0) continue;
+        s->halo[m].dst = ptr (s, b, l, data);
+        s->halo[m].lo = lo >= 0 ? ptr (s, lo, l, data) : NULL;
+        s->halo[m].hi = hi >= 0 ? ptr (s, hi, l, data) : NULL;
+        m++;
       }
+      if (!m) continue;
+      CKS (cudaSetDevice (s->dev[k]));
+      CLS (bmg_launch_halo (s->dim, g, e, s->halo, m, s->stream[k]));
+      s->nhalo++;
     }
     r = sync_devices (s);
     if (r) return r;
@@ -563,57 +521,6 @@ static int shard_cycle (bmg_shard * s, blk_t * k, int nrelax, int minlevel, int 
   return BMG_OK;
 }
 
-/* one iteration (cycle and residual) when every block lives on one device
-   (one stream): captured into a CUDA graph once per key -- nrelax,
-   minlevel and everything the launches read (the blocks' fields,
-   coefficients and boundary conditions, hashed) -- and replayed; returns
-   the number of operations it stands for in *launches */
-static unsigned long long hash_blocks (const blk_t * k, int nb)
-{
-  unsigned long long h = 1469598103934665603ULL;
-  const unsigned char * c = (const unsigned char *) k;
-  for (size_t i = 0; i < (size_t) nb*sizeof (blk_t); i++) { h ^= c[i]; h *= 1099511628211ULL; }
-  return h;
-}
-
-static int iteration_graph (bmg_shard * s, blk_t * k, int nrelax, int minlevel,
-                            long long * launches)
-{
-  const int L = s->blk[0]->depth;
-  skey key;
-  memset (&key, 0, sizeof key);
-  key.nrelax = nrelax; key.minlevel = minlevel; key.h = hash_blocks (k, s->nb);
-  struct sgraph * e = NULL, * victim = &s->graphs[0];
-  for (int i = 0; i < NSGRAPH; i++) {
-    struct sgraph * q = &s->graphs[i];
-    if (q->valid && !memcmp (&q->key, &key, sizeof key)) { e = q; break; }
-    if (!q->valid || q->stamp < victim->stamp) victim = q;
-  }
-  CKS (cudaSetDevice (s->dev[0]));
-  if (!e) {
-    if (victim->valid) { cudaGraphExecDestroy (victim->exec); victim->valid = 0; }
-    long long nl = 0;
-    cudaGraph_t graph;
-    CKS (cudaStreamBeginCapture (s->stream[0], cudaStreamCaptureModeThreadLocal));
-    int r = shard_cycle (s, k, nrelax, minlevel, L, &nl);
-    if (!r) r = residual_issue (s, k, NULL);
-    cudaError_t ee = cudaStreamEndCapture (s->stream[0], &graph);
-    if (r) { if (ee == cudaSuccess) cudaGraphDestroy (graph); return r; }
-    CKS (ee);
-    cudaError_t ie = cudaGraphInstantiate (&victim->exec, graph, 0);
-    cudaGraphDestroy (graph);
-    CKS (ie);
-    victim->key = key;
-    victim->launches = nl + 3*s->nb;
-    victim->valid = 1;
-    e = victim;
-  }
-  e->stamp = ++s->clock;
-  CKS (cudaGraphLaunch (e->exec, s->stream[0]));
-  *launches += e->launches;
-  return BMG_OK;
-}
-
 int bmg_shard_poisson (bmg_shard * s, struct Poisson p, mgstats * out)
 {
   if (!s || !out) return FAIL (BMG_EINVAL);
@@ -647,6 +554,7 @@ int bmg_shard_poisson (bmg_shard * s, struct Poisson p, mgstats * out)
   mgstats st;
   memset (&st, 0, sizeof st);
   long long launches = 0;
+  s->nhalo = 0;
   /* the sum of b over every block (an MPI_Allreduce in the reference) */
   for (int b = 0; b < s->nb && !r; b++) {
     bmg_grid * g = s->blk[b];
@@ -674,17 +582,8 @@ int bmg_shard_poisson (bmg_shard * s, struct Poisson p, mgstats * out)
                  cudaEventRecord (g0->ev0, g0->stream) != cudaSuccess)) r = FAIL (BMG_ECUDA);
     }
     const double bytes = cycle_bytes (s, k, st.nrelax, minlevel, L);
-    if (s->ndev == 1 && g0->use_graphs) {
-      /* one stream: the iteration as a captured graph */
-      if (!r) r = iteration_graph (s, k, st.nrelax, minlevel, &launches);
-      if (!r && g0->timing && cudaEventRecord (g0->ev1, g0->stream) != cudaSuccess)
-        r = FAIL (BMG_ECUDA);
-      if (!r) r = residual_collect (s, &st.resa);
-    }
-    else {
-      if (!r) r = shard_cycle (s, k, st.nrelax, minlevel, L, &launches);
-      if (!r) r = residual_all (s, k, &st.resa, g0->timing ? g0->ev1 : NULL);
-    }
+    if (!r) r = shard_cycle (s, k, st.nrelax, minlevel, L, &launches);
+    if (!r) r = residual_all (s, k, &st.resa, g0->timing ? g0->ev1 : NULL);
     if (r) break;
     g0->counters.cycles++;
     g0->counters.bytes += bytes;
@@ -704,7 +603,8 @@ int bmg_shard_poisson (bmg_shard * s, struct Poisson p, mgstats * out)
     }
     resb = st.resa;
   }
-  s->blk[0]->counters.launches += launches;
+  s->blk[0]->counters.launches += launches + s->nhalo;
+  s->nhalo = 0;
   if (!r) {
     st.minlevel = minlevel;
     if (st.resa > tolerance) {
