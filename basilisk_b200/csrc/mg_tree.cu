@@ -469,7 +469,13 @@ __device__ __forceinline__ void field_op (const bmg_tree_op & op, long gt, long 
    form, whose correction da, restricted residual res and Jacobi temporary
    are FP32 with FP32 coefficients (rax, ray, rlam), while a, b and the
    residual itself (ax, ay, lam) stay FP64 and res receives the FP64
-   residual rounded to FP32. */
+   residual rounded to FP32.
+   A local operation (few items, most of a tree boundary's stages) runs on
+   the first CTA alone; two consecutive local operations are separated by
+   that CTA's barrier (its own global writes are visible to it after
+   bar.sync), and a cluster barrier separates every other pair, so the
+   other CTAs wait at the cluster barrier that ends a run of local
+   operations. */
 template <int C, typename R, typename CO>
 __global__ void __launch_bounds__ (1024, 1)
 k_tree_interp (const bmg_tree_op * __restrict__ ops, int nops, TL Tp, double * fa, R * fda,
@@ -502,26 +508,31 @@ k_tree_interp (const bmg_tree_op * __restrict__ ops, int nops, TL Tp, double * f
       unsigned long long * dst = (unsigned long long *) sops;
       for (int w = threadIdx.x; w < words; w += blockDim.x) dst[w] = src[w];
       __syncthreads ();
-      if (gt < sops[0].n && sops[0].list) first = sops[0].list[gt];
+      const long n0 = sops[0].local ? (rank == 0 ? (long) threadIdx.x : 1L << 62) : gt;
+      if (n0 < sops[0].n && sops[0].list) first = sops[0].list[n0];
     }
     const bmg_tree_op & op = sops[o % CH];
     const uint32_t * list = op.list;
-#define ENTRY(k) ((k) == gt ? first : list[k])
+    /* the items of this CTA: the whole cluster's share, or all of a local
+       operation on the first CTA (none on the others) */
+    const long g0 = op.local ? (rank == 0 ? (long) threadIdx.x : 1L << 62) : gt;
+    const long gsx = op.local ? (long) blockDim.x : gs;
+#define ENTRY(k) ((k) == g0 ? first : list[k])
     switch (op.type) {
     case BMG_TI_SET:
     case BMG_TI_PROLONG:
     case BMG_TI_RESTRICT:
     case BMG_TI_STAGE:
-      if (op.field == 0) field_op (op, gt, gs, first, T, fa, B[op.bcsel]);
-      else field_op (op, gt, gs, first, T, F[op.field], B[op.bcsel]);
+      if (op.field == 0) field_op (op, g0, gsx, first, T, fa, B[op.bcsel]);
+      else field_op (op, g0, gsx, first, T, F[op.field], B[op.bcsel]);
       break;
     case BMG_TI_RELAX:
-      for (long k = gt; k < op.n; k += gs)
+      for (long k = g0; k < op.n; k += gsx)
         relax_item<true> (ENTRY (k), T, (const R *) fda, (const R *) fres, rax, ray, rlam,
                           op.sub ? ftmp : fda);
       break;
     case BMG_TI_JACOBI:
-      for (long k = gt; k < op.n; k += gs) {
+      for (long k = g0; k < op.n; k += gsx) {
         int l, i, j;
         unpack (ENTRY (k), l, i, j);
         const long long id = gidx (T, l, i, j);
@@ -529,7 +540,7 @@ k_tree_interp (const bmg_tree_op * __restrict__ ops, int nops, TL Tp, double * f
       }
       break;
     case BMG_TI_ADD:
-      for (long k = gt; k < op.n; k += gs) {
+      for (long k = g0; k < op.n; k += gsx) {
         int l, i, j;
         unpack (ENTRY (k), l, i, j);
         const long long id = gidx (T, l, i, j);
@@ -537,7 +548,7 @@ k_tree_interp (const bmg_tree_op * __restrict__ ops, int nops, TL Tp, double * f
       }
       break;
     case BMG_TI_RESIDUAL:
-      for (long k = gt; k < op.n; k += gs) {
+      for (long k = g0; k < op.n; k += gsx) {
         const double ar = fabs (residual_item<true> (ENTRY (k), T, fl, fa, b, ax, ay, lam, fres));
         if (m == m && !(ar <= m)) m = ar;   /* a NaN sticks */
       }
@@ -545,13 +556,21 @@ k_tree_interp (const bmg_tree_op * __restrict__ ops, int nops, TL Tp, double * f
     }
 #undef ENTRY
     /* the next operation's first list entry of this thread (the lists are
-       constant during the launch), then the barrier */
+       constant during the launch), then the barrier: a CTA barrier of the
+       first CTA between two local operations, else a cluster barrier */
+    const int nlocal = o + 1 < nops ? ((o + 1) % CH ? sops[(o + 1) % CH].local
+                                                    : __ldg (&ops[o + 1].local)) : 0;
     if (o + 1 < nops && (o + 1) % CH != 0) {
       const bmg_tree_op & nx = sops[(o + 1) % CH];
-      if (gt < nx.n && nx.list) first = nx.list[gt];
+      const long n0 = nx.local ? (rank == 0 ? (long) threadIdx.x : 1L << 62) : gt;
+      if (n0 < nx.n && nx.list) first = nx.list[n0];
     }
-    asm volatile ("barrier.cluster.arrive.release.aligned;\n"
-                  "barrier.cluster.wait.acquire.aligned;\n" ::: "memory");
+    if (op.local && nlocal) {
+      if (rank == 0) __syncthreads ();
+    }
+    else
+      asm volatile ("barrier.cluster.arrive.release.aligned;\n"
+                    "barrier.cluster.wait.acquire.aligned;\n" ::: "memory");
   }
   for (int o = 16; o > 0; o >>= 1) {
     const double v = __shfl_down_sync (0xffffffffu, m, o);

@@ -105,7 +105,10 @@ int bmg_tree_launch_add (const uint32_t * leaves, long n, const bmg_tree_levels 
    (0 a, 1 da, 2 res, 3 the Jacobi temporary), the boundary conditions of a
    ghost rule (bcsel: 0 those of a, 1 those of da) and whether they are
    homogeneous; sub is a stage's operation, or for a relaxation 1 when it
-   writes the Jacobi temporary; v is the value of a set */
+   writes the Jacobi temporary; v is the value of a set; local marks an
+   operation small enough for one CTA (the interpreter runs it on the
+   cluster's first CTA alone and separates two consecutive local
+   operations by a CTA barrier instead of a cluster barrier) */
 enum { BMG_TI_SET = 0, BMG_TI_PROLONG, BMG_TI_RESTRICT, BMG_TI_STAGE, BMG_TI_RELAX,
        BMG_TI_JACOBI, BMG_TI_ADD, BMG_TI_RESIDUAL };
 typedef struct {
@@ -113,7 +116,7 @@ typedef struct {
   long long n;
   const bmg_tree_rule * rules;
   long long nr;
-  int type, sub, field, bcsel, homog, pad_;
+  int type, sub, field, bcsel, homog, local;
   double v;
 } bmg_tree_op;
 /* the operations ops[0..nops) in order, in one launch of one thread-block

@@ -733,6 +733,8 @@ static void r_push (opvec * o, int type, int field, int sub, int homog, const ui
   memset (q, 0, sizeof *q);
   q->type = type; q->field = field; q->sub = sub; q->homog = homog; q->bcsel = 0;
   q->list = list; q->n = n; q->rules = rules; q->nr = nr; q->v = v;
+  /* at most two items a thread of one 1024-thread CTA: run on one CTA */
+  q->local = items + nr <= 2048;
 }
 
 static void r_boundary (struct bmg_tree * t, opvec * o, int field, int l, int homog, int kind)
