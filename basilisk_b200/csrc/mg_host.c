@@ -747,7 +747,7 @@ static int residual_max (bmg_grid * g, field_t * a, const double * b, const coef
 /* the residual of an mg_solve iteration: on 2D grids fused with the
    restriction of res into the level below, which the next cycle then
    skips (returns 1 when it restricted) */
-static int fused_tail (const bmg_grid * g) { return g->dim == 2 && g->depth >= 1; }
+static int fused_tail (const bmg_grid * g) { return g->dim >= 2 && g->depth >= 1; }
 
 static int residual_tail (bmg_grid * g, field_t * a, const double * b, const coefs_t * c,
                           const levels_t * lv, double * maxres, int sync, work_t * w)
@@ -756,10 +756,16 @@ static int residual_tail (bmg_grid * g, field_t * a, const double * b, const coe
   if (!fused_tail (g))
     return residual_max (g, a, b, c, lv->res[L], lv->st[L], maxres, sync, w);
   CK (cudaMemsetAsync (g->d_maxres, 0, sizeof (unsigned long long), g->stream));
-  CL (bmg_launch_residual_restrict (lv->st[L], lv->st[L - 1], g->g64[L], geom_st (g, L, lv->st[L]),
-                                    geom_st (g, L - 1, lv->st[L - 1]), a->lv[L], b,
-                                    c->alpha64[L], c->lambda64[L], delta_of (g, L),
-                                    lv->res[L], lv->res[L - 1], g->d_maxres, g->stream));
+  if (g->dim == 2)
+    CL (bmg_launch_residual_restrict (lv->st[L], lv->st[L - 1], g->g64[L], geom_st (g, L, lv->st[L]),
+                                      geom_st (g, L - 1, lv->st[L - 1]), a->lv[L], b,
+                                      c->alpha64[L], c->lambda64[L], delta_of (g, L),
+                                      lv->res[L], lv->res[L - 1], g->d_maxres, g->stream));
+  else
+    CL (bmg_launch_residual_restrict3d (lv->st[L], lv->st[L - 1], g->g64[L], geom_st (g, L, lv->st[L]),
+                                        geom_st (g, L - 1, lv->st[L - 1]), a->lv[L], b,
+                                        c->alpha64[L], c->lambda64[L], delta_of (g, L),
+                                        lv->res[L], lv->res[L - 1], g->d_maxres, g->stream));
   w->launches += 1;
   w->bytes += ncells (g, L)*(8.*(2. + (c->alpha_stored ? g->dim : 0) +
                                  (c->lambda_stored ? 1 : 0)) + es_of (lv->st[L])) +

@@ -136,6 +136,52 @@ __global__ void k_prolong2d_blk (bmg_geom gc, bmg_geom gf, const TC * __restrict
   }
 }
 
+/* the 3D trilinear prolongation by coarse cell: one thread reads the
+   3 x 3 x 3 coarse neighbourhood (ghosts included) once and writes the
+   eight children, each with k_prolong's expression and order
+   (bit-identical); children along the contiguous axis are written in
+   pairs */
+template <typename TC, typename TF>
+__global__ void k_prolong3d_blk (bmg_geom gc, bmg_geom gf, const TC * __restrict__ s,
+                                 TF * __restrict__ f, BCH bc)
+{
+  pdl_wait ();
+  pdl_trigger ();
+  const int ck = blockIdx.x*blockDim.x + threadIdx.x;
+  const int cj = blockIdx.y*blockDim.y + threadIdx.y;
+  const int ci = blockIdx.z*blockDim.z + threadIdx.z;
+  if (ci >= gc.n || cj >= gc.n || ck >= gc.n) return;
+  TC m[3][3][3];
+#pragma unroll
+  for (int di = 0; di < 3; di++)
+#pragma unroll
+    for (int dj = 0; dj < 3; dj++)
+#pragma unroll
+      for (int dk = 0; dk < 3; dk++)
+        m[di][dj][dk] = s[cidx<3> (gc, ci + di - 1, cj + dj - 1, ck + dk - 1)];
+#pragma unroll
+  for (int a = 0; a < 2; a++)
+#pragma unroll
+    for (int b = 0; b < 2; b++) {
+      TF w[2];
+#pragma unroll
+      for (int c = 0; c < 2; c++) {
+        const int cx = a ? 2 : 0, cy = b ? 2 : 0, cz = c ? 2 : 0;
+        const TC v = (TC(27)*m[1][1][1] +
+                      TC(9)*(m[cx][1][1] + m[1][cy][1] + m[1][1][cz]) +
+                      TC(3)*(m[cx][cy][1] + m[cx][1][cz] + m[1][cy][cz]) +
+                      m[cx][cy][cz])/TC(64);
+        w[c] = (TF) v;
+      }
+      const int i = 2*ci + a, j = 2*cj + b, k = 2*ck;
+      TF * q = f + cidx<3> (gf, i, j, k);
+      q[0] = w[0];
+      q[1] = w[1];
+      ghosts_homog<3, TF> (f, gf, i, j, k, w[0], bc);
+      ghosts_homog<3, TF> (f, gf, i, j, k + 1, w[1], bc);
+    }
+}
+
 /* coarse = mean of the children, summed in foreach_child order */
 template <int DIM, typename TF, typename TC>
 __global__ void k_restrict (bmg_geom gf, bmg_geom gc, const TF * __restrict__ f,
@@ -330,6 +376,60 @@ __global__ void k_residual_restrict2d (bmg_geom g, bmg_geom gr, bmg_geom gc,
         m = nanmax (m, fabs (r));
       }
     resc[cidx<2> (gc, ci, cj, 0)] = sum/TC(4);
+  }
+  block_max_atomic (m, maxres);
+}
+
+/* the same in 3D: each thread computes the eight residuals of one coarse
+   cell's children (k_residual's expression and order), stores them, and
+   stores their mean in k_restrict's order (children a, b, d nested as in
+   foreach_child, from the stored values): bit-identical to k_residual
+   followed by k_restrict */
+template <typename TR, typename TC, bool POW2>
+__global__ void k_residual_restrict3d (bmg_geom g, bmg_geom gr, bmg_geom gc,
+                                       const double * __restrict__ a,
+                                       const double * __restrict__ b, Coef<double> ax,
+                                       Coef<double> ay, Coef<double> az, Coef<double> lam,
+                                       double Delta, TR * __restrict__ res, TC * __restrict__ resc,
+                                       unsigned long long * maxres)
+{
+  pdl_wait ();
+  pdl_trigger ();
+  const int ck = blockIdx.x*blockDim.x + threadIdx.x;
+  const int cj = blockIdx.y*blockDim.y + threadIdx.y;
+  const int ci = blockIdx.z*blockDim.z + threadIdx.z;
+  double m = 0.;
+  const double rD = 1./Delta;
+  if (ci < gc.n && cj < gc.n && ck < gc.n) {
+    TC sum = TC(0);
+#pragma unroll
+    for (int u = 0; u < 2; u++)
+#pragma unroll
+      for (int v = 0; v < 2; v++)
+#pragma unroll
+        for (int w = 0; w < 2; w++) {
+          const int i = 2*ci + u, j = 2*cj + v, k = 2*ck + w;
+          const long long id = cidx<3> (g, i, j, k);
+          const double ac = a[id];
+          double r = b[id] - lam.at (id)*ac;
+          {
+            const long long s = g.plane;
+            r += over_delta<POW2> (ax.at (id)*over_delta<POW2> (ac - a[id - s], Delta, rD) -
+                                   ax.at (id + s)*over_delta<POW2> (a[id + s] - ac, Delta, rD), Delta, rD);
+          }
+          {
+            const long long s = g.P;
+            r += over_delta<POW2> (ay.at (id)*over_delta<POW2> (ac - a[id - s], Delta, rD) -
+                                   ay.at (id + s)*over_delta<POW2> (a[id + s] - ac, Delta, rD), Delta, rD);
+          }
+          r += over_delta<POW2> (az.at (id)*over_delta<POW2> (ac - a[id - 1], Delta, rD) -
+                                 az.at (id + 1)*over_delta<POW2> (a[id + 1] - ac, Delta, rD), Delta, rD);
+          const TR rs = (TR) r;
+          res[cidx<3> (gr, i, j, k)] = rs;
+          sum += (TC) rs;
+          m = nanmax (m, fabs (r));
+        }
+    resc[cidx<3> (gc, ci, cj, ck)] = sum/TC(8);
   }
   block_max_atomic (m, maxres);
 }
@@ -566,6 +666,18 @@ void prolong_dim (int stc, int stf, bmg_geom gc, bmg_geom gf, const void * c, vo
       pdl_launch (k_prolong2d_blk<float, double>, gb, bb, 0, s, gc, gf, (const float *) c, (double *) f, h);
     return;
   }
+  if (DIM == 3 && !zero && gf.n == 2*gc.n) {
+    dim3 gb = grid_shape<3> (gc.n), bb = block_shape<3> ();
+    if (stc == BMG_ST_F64 && stf == BMG_ST_F64)
+      pdl_launch (k_prolong3d_blk<double, double>, gb, bb, 0, s, gc, gf, (const double *) c, (double *) f, h);
+    else if (stc == BMG_ST_F32 && stf == BMG_ST_F32)
+      pdl_launch (k_prolong3d_blk<float, float>, gb, bb, 0, s, gc, gf, (const float *) c, (float *) f, h);
+    else if (stc == BMG_ST_F64 && stf == BMG_ST_F32)
+      pdl_launch (k_prolong3d_blk<double, float>, gb, bb, 0, s, gc, gf, (const double *) c, (float *) f, h);
+    else
+      pdl_launch (k_prolong3d_blk<float, double>, gb, bb, 0, s, gc, gf, (const float *) c, (double *) f, h);
+    return;
+  }
   dim3 gb = grid_shape<DIM> (gf.n), bb = block_shape<DIM> ();
   if (stc == BMG_ST_F64 && stf == BMG_ST_F64)
     pdl_launch (k_prolong<DIM, double, double>, gb, bb, 0, s, gc, gf, (const double *) c, (double *) f, h, zero);
@@ -635,6 +747,25 @@ void residual_restrict_2d (bmg_geom g, bmg_geom gr, bmg_geom gc, const double * 
   else
     pdl_launch (k_residual_restrict2d<TR, TC, false>, gb, bb, 0, s, g, gr, gc, a, b, ax, ay, lam,
                 Delta, (TR *) res, (TC *) resc, maxres);
+}
+
+template <typename TR, typename TC>
+void residual_restrict_3d (bmg_geom g, bmg_geom gr, bmg_geom gc, const double * a,
+                           const double * b, const bmg_coef * alpha, bmg_coef lambda,
+                           double Delta, void * res, void * resc, unsigned long long * maxres,
+                           cudaStream_t s)
+{
+  Coef<double> ax = coef_of<double> (alpha[0]), ay = coef_of<double> (alpha[1]),
+    az = coef_of<double> (alpha[2]), lam = coef_of<double> (lambda);
+  const dim3 bb = block_shape<3> (), gb = grid_shape<3> (gc.n);
+  int ex;
+  const bool pow2 = Delta > 0. && frexp (Delta, &ex) == 0.5 && ex > -1000 && ex < 1000;
+  if (pow2)
+    pdl_launch (k_residual_restrict3d<TR, TC, true>, gb, bb, 0, s, g, gr, gc, a, b, ax, ay, az,
+                lam, Delta, (TR *) res, (TC *) resc, maxres);
+  else
+    pdl_launch (k_residual_restrict3d<TR, TC, false>, gb, bb, 0, s, g, gr, gc, a, b, ax, ay, az,
+                lam, Delta, (TR *) res, (TC *) resc, maxres);
 }
 
 template <int DIM>
@@ -1134,6 +1265,25 @@ int bmg_launch_residual_restrict (int st_res, int st_coarse, bmg_geom g, bmg_geo
     residual_restrict_2d<float, double> (g, gres, gcoarse, a, b, alpha, lambda, Delta, res, coarse, maxres, s);
   else
     residual_restrict_2d<double, float> (g, gres, gcoarse, a, b, alpha, lambda, Delta, res, coarse, maxres, s);
+  cudaError_t r = cudaGetLastError ();
+  return r == cudaSuccess ? 0 : (int) r;
+}
+
+int bmg_launch_residual_restrict3d (int st_res, int st_coarse, bmg_geom g, bmg_geom gres,
+                                    bmg_geom gcoarse, const double * a, const double * b,
+                                    const bmg_coef * alpha, bmg_coef lambda, double Delta,
+                                    void * res, void * coarse, unsigned long long * maxres,
+                                    cudaStream_t s)
+{
+  if (g.n < 2 || gcoarse.n*2 != g.n) return (int) cudaErrorInvalidValue;
+  if (st_res == BMG_ST_F64 && st_coarse == BMG_ST_F64)
+    residual_restrict_3d<double, double> (g, gres, gcoarse, a, b, alpha, lambda, Delta, res, coarse, maxres, s);
+  else if (st_res == BMG_ST_F32 && st_coarse == BMG_ST_F32)
+    residual_restrict_3d<float, float> (g, gres, gcoarse, a, b, alpha, lambda, Delta, res, coarse, maxres, s);
+  else if (st_res == BMG_ST_F32 && st_coarse == BMG_ST_F64)
+    residual_restrict_3d<float, double> (g, gres, gcoarse, a, b, alpha, lambda, Delta, res, coarse, maxres, s);
+  else
+    residual_restrict_3d<double, float> (g, gres, gcoarse, a, b, alpha, lambda, Delta, res, coarse, maxres, s);
   cudaError_t r = cudaGetLastError ();
   return r == cudaSuccess ? 0 : (int) r;
 }

@@ -90,6 +90,13 @@ int bmg_launch_residual_restrict (int st_res, int st_coarse, bmg_geom g, bmg_geo
                                   void * res, void * coarse, unsigned long long * maxres,
                                   cudaStream_t s);
 
+/* the same for the finest 3D level (eight children per coarse cell) */
+int bmg_launch_residual_restrict3d (int st_res, int st_coarse, bmg_geom g, bmg_geom gres,
+                                    bmg_geom gcoarse, const double * a, const double * b,
+                                    const bmg_coef * alpha, bmg_coef lambda, double Delta,
+                                    void * res, void * coarse, unsigned long long * maxres,
+                                    cudaStream_t s);
+
 int bmg_launch_correct (int dim, int st_da, bmg_geom g, bmg_geom gda, double * a,
                         const void * da, const bmg_bcdesc * bc, cudaStream_t s);
 
