@@ -30,7 +30,12 @@ def sharded(prob, dims, relax):
     b = sg.scalar(prob["b"])
     alpha = sg.face_vector(prob["alpha"]) if prob["alpha"] is not None else None
     lam = prob["lambda"]
-    lam_f = None if lam is None else sg.const_scalar(float(lam))
+    if lam is None:
+        lam_f = None
+    elif np.isscalar(lam):
+        lam_f = sg.const_scalar(float(lam))
+    else:
+        lam_f = sg.scalar(lam)
     return sg, a, b, alpha, lam_f
 
 
@@ -68,6 +73,18 @@ def test_sixteen_blocks_bit_identical():
     """4 x 4 blocks of 64^2: interior blocks with four neighbours, corner
     ghosts from the diagonal blocks."""
     compare(problems.two_phase_2d(depth=8, seed=6), (4, 4), "rbgs", 1e-6)
+
+
+def test_mixed_conditions_and_lambda_field_bit_identical():
+    """Inhomogeneous Dirichlet on two sides, Neumann on the others (each
+    block keeps the condition of the domain's sides it touches), a stored
+    lambda field: 2x2 blocks against one grid."""
+    import helpers
+    rng = np.random.default_rng(21)
+    prob = helpers.random_problem(2, 7, rng, bc={0: ("dirichlet", 0.5), 1: ("neumann", -0.25),
+                                                 2: ("dirichlet", -1.0), 3: ("neumann", 0.75)},
+                                  lam="field")
+    compare(prob, (2, 2), "rbgs", 1e-9)
 
 
 def test_helmholtz_3d_2x2x2_blocks_bit_identical():
