@@ -957,8 +957,17 @@ static int cycle_launches (bmg_grid * g, field_t * a, const levels_t * lv, const
         else {
           CL (bmg_launch_relax (dim, st, BMG_SWEEP_RED, gl, cur[l], cur[l], lv->res[l], al, la,
                                 delta_of (g, l), dabc, s));
-          CL (bmg_launch_relax (dim, st, BMG_SWEEP_BLACK, gl, cur[l], cur[l], lv->res[l], al, la,
-                                delta_of (g, l), dabc, s));
+          if (dim == 3 && l == L && maxlevel == L && i == nrelax - 1) {
+            /* the finest level's last pass also applies a += da */
+            CL (bmg_launch_relax_correct3d (st, gl, cur[l], cur[l], lv->res[l], al, la,
+                                            delta_of (g, l), dabc, a->lv[L], g->g64[L], &abc, s));
+            corrected = 1;
+            bytes += ncells (g, L)*16.;
+            if (timed) w->relax_bytes += ncells (g, L)*16.;
+          }
+          else
+            CL (bmg_launch_relax (dim, st, BMG_SWEEP_BLACK, gl, cur[l], cur[l], lv->res[l], al, la,
+                                  delta_of (g, l), dabc, s));
           launches += 2;
         }
       }

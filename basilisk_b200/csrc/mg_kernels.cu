@@ -37,6 +37,7 @@
 #include <stdio.h>
 #include "mg_launch.h"
 
+#include <string.h>
 #include <type_traits>
 #include "mg_device.cuh"
 
@@ -68,9 +69,10 @@ __global__ void k_relax (bmg_geom g, T * out, const T * in, const T * __restrict
    colour MODE with relax_value's expression and order (bit-identical to
    k_relax); every array is read as aligned pairs, which halves the load
    instructions per byte moved */
-template <typename T, int MODE>
+template <typename T, int MODE, bool COR>
 __global__ void k_relax3_pair (bmg_geom g, T * out, const T * in, const T * __restrict__ rhs,
-                               Coef<T> ax, Coef<T> ay, Coef<T> az, Coef<T> lam, T Delta, BCH bc)
+                               Coef<T> ax, Coef<T> ay, Coef<T> az, Coef<T> lam, T Delta, BCH bc,
+                               double * acor, bmg_geom ga, bmg_bcdesc abc)
 {
   typedef typename std::conditional<sizeof (T) == 8, double2, float2>::type T2;
   const int q = blockIdx.x*blockDim.x + threadIdx.x;
@@ -116,6 +118,18 @@ __global__ void k_relax3_pair (bmg_geom g, T * out, const T * in, const T * __re
   const T v = nn/d;
   out[id] = v;
   ghosts_homog<3, T> (out, g, i, j, 2*q + o, v, bc);
+  if (COR) {
+    /* the last pass of the finest level: both cells of the pair are final
+       (the other one since the previous pass), so a += da for the pair,
+       with k_correct's expression and the ghost images of a */
+    const T d0 = o ? c0.x : v, d1 = o ? v : c0.y;
+    const long long ia = cidx<3> (ga, i, j, 2*q);
+    const double2 av = *(const double2 *) (acor + ia);
+    const double a0 = av.x + (double) d0, a1 = av.y + (double) d1;
+    *(double2 *) (acor + ia) = make_double2 (a0, a1);
+    ghosts_inhomog<3> (acor, ga, i, j, 2*q, a0, abc);
+    ghosts_inhomog<3> (acor, ga, i, j, 2*q + 1, a1, abc);
+  }
 }
 
 /* ---------------------------------------------------------------- */
@@ -681,12 +695,14 @@ void relax_dim (int mode, bmg_geom g, void * out, const void * in, const void * 
     az = coef_of<T> (alpha[2]), lam = coef_of<T> (lambda);
   if (DIM == 3 && mode != BMG_SWEEP_JACOBI && g.n >= 2) {
     const dim3 bb (32, 4, 2), gb ((g.n/2 + 31)/32, (g.n + 3)/4, (g.n + 1)/2);
+    bmg_bcdesc none;
+    memset (&none, 0, sizeof none);
     if (mode == BMG_SWEEP_RED)
-      k_relax3_pair<T, BMG_SWEEP_RED><<<gb, bb, 0, s>>> (g, (T *) out, (const T *) in,
-                                                         (const T *) rhs, ax, ay, az, lam, (T) Delta, h);
+      k_relax3_pair<T, BMG_SWEEP_RED, false><<<gb, bb, 0, s>>> (
+        g, (T *) out, (const T *) in, (const T *) rhs, ax, ay, az, lam, (T) Delta, h, NULL, g, none);
     else
-      k_relax3_pair<T, BMG_SWEEP_BLACK><<<gb, bb, 0, s>>> (g, (T *) out, (const T *) in,
-                                                           (const T *) rhs, ax, ay, az, lam, (T) Delta, h);
+      k_relax3_pair<T, BMG_SWEEP_BLACK, false><<<gb, bb, 0, s>>> (
+        g, (T *) out, (const T *) in, (const T *) rhs, ax, ay, az, lam, (T) Delta, h, NULL, g, none);
     return;
   }
   dim3 gb = grid_shape<DIM> (g.n), bb = block_shape<DIM> ();
@@ -1352,6 +1368,27 @@ int bmg_launch_residual_restrict3d (int st_res, int st_coarse, bmg_geom g, bmg_g
     residual_restrict_3d<double, float> (g, gres, gcoarse, a, b, alpha, lambda, Delta, res, coarse, maxres, s);
   cudaError_t r = cudaGetLastError ();
   return r == cudaSuccess ? 0 : (int) r;
+}
+
+int bmg_launch_relax_correct3d (int st, bmg_geom g, void * out, const void * in, const void * rhs,
+                                const bmg_coef * alpha, bmg_coef lambda, double Delta,
+                                const bmg_bcdesc * bc, double * acor, bmg_geom ga,
+                                const bmg_bcdesc * abc, cudaStream_t s)
+{
+  if (g.n < 2 || g.n != ga.n || !acor || !abc) return (int) cudaErrorInvalidValue;
+  BCH h = bch_of (bc);
+  const dim3 bb (32, 4, 2), gb ((g.n/2 + 31)/32, (g.n + 3)/4, (g.n + 1)/2);
+  if (st == BMG_ST_F64)
+    k_relax3_pair<double, BMG_SWEEP_BLACK, true><<<gb, bb, 0, s>>> (
+      g, (double *) out, (const double *) in, (const double *) rhs, coef_of<double> (alpha[0]),
+      coef_of<double> (alpha[1]), coef_of<double> (alpha[2]), coef_of<double> (lambda),
+      Delta, h, acor, ga, *abc);
+  else
+    k_relax3_pair<float, BMG_SWEEP_BLACK, true><<<gb, bb, 0, s>>> (
+      g, (float *) out, (const float *) in, (const float *) rhs, coef_of<float> (alpha[0]),
+      coef_of<float> (alpha[1]), coef_of<float> (alpha[2]), coef_of<float> (lambda),
+      (float) Delta, h, acor, ga, *abc);
+  return status_of_launch ();
 }
 
 int bmg_launch_correct (int dim, int st_da, bmg_geom g, bmg_geom gda, double * a,

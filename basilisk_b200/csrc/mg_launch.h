@@ -97,6 +97,15 @@ int bmg_launch_residual_restrict3d (int st_res, int st_coarse, bmg_geom g, bmg_g
                                     void * res, void * coarse, unsigned long long * maxres,
                                     cudaStream_t s);
 
+/* the black pass of a 3D red-black sweep (in place, out == in) that also
+   applies a += out to the FP64 finest level acor (geometry ga) with the
+   ghost images of its boundary conditions abc: the last pass of a cycle's
+   finest level, bit-identical to the pass followed by bmg_launch_correct */
+int bmg_launch_relax_correct3d (int st, bmg_geom g, void * out, const void * in, const void * rhs,
+                                const bmg_coef * alpha, bmg_coef lambda, double Delta,
+                                const bmg_bcdesc * bc, double * acor, bmg_geom ga,
+                                const bmg_bcdesc * abc, cudaStream_t s);
+
 int bmg_launch_correct (int dim, int st_da, bmg_geom g, bmg_geom gda, double * a,
                         const void * da, const bmg_bcdesc * bc, cudaStream_t s);
 

@@ -180,6 +180,24 @@ def test_tree_mixed_form_against_the_oracle():
     assert errs["mixed_1e-9"] <= 1e-6, errs
 
 
+def test_tree_mixed_form_jacobi_reaches_the_tolerance():
+    """The mixed form with the reference's weighted-Jacobi smoother on the
+    tree (the interpreter's FP32 Jacobi temporary): it reaches the
+    tolerance (1e-4: the reference's Jacobi branch stalls near 2e-5 on this
+    problem), and both forms' solutions agree to the accuracy that residual
+    pins."""
+    depth, base = 8, 4
+    sols = {}
+    for prec in ("fp64", "mixed"):
+        tg = c4_problem(lambda d, o: GpuTree(d, o, relax="jacobi", precision=prec), depth, base)
+        st = tg.poisson(tolerance=1e-4, nrelax=4, minlevel=1)
+        assert st["resa"] <= 1e-4, (prec, st)
+        sols[prec] = leaf_values(tg, ot.A)
+        tg.close()
+    rel = float(np.abs(sols["mixed"] - sols["fp64"]).max() / np.abs(sols["fp64"]).max())
+    assert rel <= 1e-3, rel
+
+
 def _cpu_rbgs(depth, origin):
     t = ot.Tree(depth, 1.0, origin)
     t.set_relax(ot.RELAX_RBGS)
