@@ -800,7 +800,9 @@ static int bottom_top (const bmg_grid * g, const levels_t * lv, const coefs_t * 
 {
   int top = minlevel - 1;
   for (int l = minlevel; l <= maxlevel; l++) {
-    if (l > minlevel && ncells (g, l) > BMG_BOTTOM_CELLS) break;
+    /* in 3D a 16^3 level is 4096 cells of one CTA's generic passes: the
+       one-pass launches over the whole device are faster from 16^3 up */
+    if (l > minlevel && ncells (g, l) > (g->dim == 3 ? 512 : BMG_BOTTOM_CELLS)) break;
     /* a level that has a cluster kernel is relaxed by it, not by the
        single CTA */
     if (use_cluster (g, lv, l, minlevel, maxlevel)) break;
