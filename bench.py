@@ -25,6 +25,7 @@ workload (about 20 s each on 8 cores).
 """
 import argparse
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -376,7 +377,6 @@ def run_workload(args, ws, rank, local):
                   "parallelism": "replicas" if ws > 1 else "1 gpu"}
     elif args.workload == "sharded_2d":
         from basilisk_b200.shard import ShardedGrid, dims_create
-        import math
         dims = dims_create(args.blocks, 2)
         if dims[0] != dims[1] or dims[0] & (dims[0] - 1):
             raise SystemExit("--blocks must give a square power-of-two arrangement (4, 16, ...)")
@@ -570,6 +570,23 @@ def run_workload(args, ws, rank, local):
                                           "instances (lexicographic GS, %d OpenMP threads, %.1f s), "
                                           "scaled to 16; the face gradients are not timed"
                                           % (threads, t_cpu)}
+    if not args.no_cpu and args.workload == "sharded_2d":
+        # the reference's MPI multigrid runs this decomposition on 2x2 ranks;
+        # its CPU restatement here is the single-domain oracle with the same
+        # coarsest level (a block's level 1 is the domain's level 1 + log2 dims)
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        from oracle import oracle
+        from helpers import oracle_grid
+        threads = os.cpu_count()
+        o = oracle_grid(prob, relax=oracle.RELAX_GS, threads=threads)
+        t0 = time.perf_counter()
+        cst = o.poisson(tolerance=tol, minlevel=1 + int(math.log2(dims[0])))
+        dt = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": 1.0 / dt, "unit": "solves/s", "cores": threads,
+                                "kind": "port",
+                                "sample": "1 full solve of the same problem on one domain with the "
+                                          "blocks' coarsest level (%d V-cycles), lexicographic GS, "
+                                          "%d OpenMP threads" % (cst["i"], threads)}
     if not args.no_cpu and args.workload == "two_phase_tree":
         sys.path.insert(0, os.path.join(ROOT, "tests"))
         from oracle import tree as otree
