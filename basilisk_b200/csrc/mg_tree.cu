@@ -413,6 +413,16 @@ __global__ void k_sum_final (const double * __restrict__ partials, int np, doubl
    them.  Every item is computed by the function the one-operation kernel
    uses, so the results are bit-identical.  The residual's maximum is
    reduced per warp into maxres (zeroed before the launch). */
+/* How the interpreter loads field values that earlier operations of the
+   launch wrote: plain (L1-cached) loads.  Every operation is separated
+   from the next by a cluster barrier with release/acquire semantics at
+   cluster scope, or, between two operations the first CTA runs alone, by
+   that CTA's barrier; under the PTX memory model these order every write
+   of one operation before every read of the next (the program has no data
+   race), so weak loads observe them -- the L1 of an SM cannot serve a
+   value older than the acquire. */
+constexpr bool ICG = false;
+
 /* The list operations that work on one field s of the scalar type S: a
    set, prolongation, restriction or boundary stage (the interpreter's
    field 0, a, is FP64; the cycle's fields have the cycle's type) */
@@ -434,19 +444,19 @@ __device__ __forceinline__ void field_op (const bmg_tree_op & op, long gt, long 
     for (long k = gt; k < op.n; k += gs) {
       int l, i, j;
       unpack (ENTRY (k), l, i, j);
-      s[gidx (T, l, i, j)] = bilinear<true> (T, s, l, i, j);
+      s[gidx (T, l, i, j)] = bilinear<ICG> (T, s, l, i, j);
     }
     break;
   case BMG_TI_RESTRICT:
     for (long k = gt; k < op.n; k += gs)
-      restrict_cell<true> (list, k, T, s);
+      restrict_cell<ICG> (list, k, T, s);
     break;
   case BMG_TI_STAGE: {
     const long w = op.sub == BMG_T_OP_HALO ? 4*op.n : op.sub == BMG_T_OP_RESTRICT ? op.n : 0;
     for (long k = gt; k < w + op.nr; k += gs) {
-      if (k >= w) ghost_value<true> (op.rules[k - w], T, s, bc, op.homog);
-      else if (op.sub == BMG_T_OP_HALO) halo_child<true> (list, k, T, s);
-      else restrict_cell<true> (list, k, T, s);
+      if (k >= w) ghost_value<ICG> (op.rules[k - w], T, s, bc, op.homog);
+      else if (op.sub == BMG_T_OP_HALO) halo_child<ICG> (list, k, T, s);
+      else restrict_cell<ICG> (list, k, T, s);
     }
     break;
   }
@@ -528,7 +538,7 @@ k_tree_interp (const bmg_tree_op * __restrict__ ops, int nops, TL Tp, double * f
       break;
     case BMG_TI_RELAX:
       for (long k = g0; k < op.n; k += gsx)
-        relax_item<true> (ENTRY (k), T, (const R *) fda, (const R *) fres, rax, ray, rlam,
+        relax_item<ICG> (ENTRY (k), T, (const R *) fda, (const R *) fres, rax, ray, rlam,
                           op.sub ? ftmp : fda);
       break;
     case BMG_TI_JACOBI:
@@ -536,7 +546,7 @@ k_tree_interp (const bmg_tree_op * __restrict__ ops, int nops, TL Tp, double * f
         int l, i, j;
         unpack (ENTRY (k), l, i, j);
         const long long id = gidx (T, l, i, j);
-        fda[id] = (ldf<true> (fda + id) + (R) 2*ldf<true> (ftmp + id))/(R) 3;
+        fda[id] = (ldf<ICG> (fda + id) + (R) 2*ldf<ICG> (ftmp + id))/(R) 3;
       }
       break;
     case BMG_TI_ADD:
@@ -544,12 +554,12 @@ k_tree_interp (const bmg_tree_op * __restrict__ ops, int nops, TL Tp, double * f
         int l, i, j;
         unpack (ENTRY (k), l, i, j);
         const long long id = gidx (T, l, i, j);
-        fa[id] = ldf<true> (fa + id) + (double) ldf<true> (fda + id);
+        fa[id] = ldf<ICG> (fa + id) + (double) ldf<ICG> (fda + id);
       }
       break;
     case BMG_TI_RESIDUAL:
       for (long k = g0; k < op.n; k += gsx) {
-        const double ar = fabs (residual_item<true> (ENTRY (k), T, fl, fa, b, ax, ay, lam, fres));
+        const double ar = fabs (residual_item<ICG> (ENTRY (k), T, fl, fa, b, ax, ay, lam, fres));
         if (m == m && !(ar <= m)) m = ar;   /* a NaN sticks */
       }
       break;

@@ -570,6 +570,30 @@ def run_workload(args, ws, rank, local):
                                           "instances (lexicographic GS, %d OpenMP threads, %.1f s), "
                                           "scaled to 16; the face gradients are not timed"
                                           % (threads, t_cpu)}
+    if not args.no_cpu and args.workload == "viscosity_2d":
+        # the oracle's viscosity () (viscosity.h:169-183 restated, the
+        # reference's lexicographic GS relax_viscosity) on the same fields
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        from oracle import oracle
+        threads = os.cpu_count()
+        o = oracle.Grid(2, depth, relax=oracle.RELAX_GS, threads=threads)
+        for comp in range(2):
+            for side in range(4):
+                o.set_visc_bc(comp, side, oracle.DIRICHLET, 0.0)
+        o.set_u(u0)
+        o.set_mu([0.01 / ax, 0.01 / ay])
+        o.set_rho(f * (1.0 - 1000.0) + 1000.0)
+        oracle.set_globals(2, tolerance=tol)
+        try:
+            t0 = time.perf_counter()
+            cst = o.viscosity(dt=1e-3)
+            dt_cpu = time.perf_counter() - t0
+        finally:
+            oracle.set_globals(2, tolerance=1e-3)
+        line["cpu_baseline"] = {"value": 1.0 / dt_cpu, "unit": "solves/s", "cores": threads,
+                                "kind": "port",
+                                "sample": "1 viscous step of the same fields (%d V-cycles), "
+                                          "lexicographic GS, %d OpenMP threads" % (cst["i"], threads)}
     if not args.no_cpu and args.workload == "sharded_2d":
         # the reference's MPI multigrid runs this decomposition on 2x2 ranks;
         # its CPU restatement here is the single-domain oracle with the same
