@@ -733,7 +733,9 @@ static void r_push (opvec * o, int type, int field, int sub, int homog, const ui
   memset (q, 0, sizeof *q);
   q->type = type; q->field = field; q->sub = sub; q->homog = homog; q->bcsel = 0;
   q->list = list; q->n = n; q->rules = rules; q->nr = nr; q->v = v;
-  /* at most two items a thread of one 1024-thread CTA: run on one CTA */
+  /* at most two items a thread of one 1024-thread CTA: run on one CTA
+     (measured on the depth-11 band tree: 772 ms per solve with no local
+     operations, 645-684 with at most 1024-2048 items, 690-1034 above) */
   q->local = items + nr <= 2048;
 }
 
