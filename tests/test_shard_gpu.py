@@ -87,6 +87,20 @@ def test_mixed_conditions_and_lambda_field_bit_identical():
     compare(prob, (2, 2), "rbgs", 1e-9)
 
 
+def test_one_block_is_the_grid():
+    """dims (1, 1): one block, nothing to exchange (its periodic directions
+    are its own), the grid's solve with minlevel 1."""
+    compare(problems.poisson_periodic_2d(depth=7, seed=9), (1, 1), "rbgs", 1e-8)
+
+
+def test_1d_two_blocks_bit_identical():
+    """One dimension, two blocks: single-cell ghost slabs."""
+    import helpers
+    rng = np.random.default_rng(13)
+    prob = helpers.random_problem(1, 9, rng, bc={0: ("dirichlet", 1.0), 1: ("dirichlet", -0.5)})
+    compare(prob, (2,), "rbgs", 1e-10)
+
+
 def test_helmholtz_3d_2x2x2_blocks_bit_identical():
     """Periodic 3D Helmholtz (viscosity.h form) on eight blocks of 16^3:
     x slabs, strided y and z slabs."""
