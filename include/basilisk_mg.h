@@ -79,7 +79,11 @@ enum { BMG_RELAX_RBGS = 0, BMG_RELAX_JACOBI = 1 };
 
 /* arithmetic of the solve: FP64 throughout, or FP32 cycles inside an FP64
    iterative-refinement loop (outer residual, accumulation, compatibility
-   projection and coarsest level in FP64). */
+   projection and coarsest level in FP64).  On a quadtree the mixed form
+   runs its cycle in FP32 on every level, keeps the residual and a += da
+   in FP64, does not project b, and needs the schedule interpreter's
+   thread-block cluster (16 or 8 CTAs of 1024 threads): without it the
+   solve returns BMG_EUNSUPPORTED. */
 enum { BMG_FP64 = 0, BMG_MIXED = 1 };
 
 /* where the pointers given to bmg_field_set / get / bmg_bc point */
