@@ -291,8 +291,9 @@ int bmg_restore (bmg_grid * grid, const char * file, const bmg_scalar * list,
    blocks.  Blocks may live on different CUDA devices (each created with its
    device current); the decomposition puts the blocks of a device on one
    stream of its own, and gives them their own streams back when it is
-   freed.  Every block must create its fields in the same order, so that a
-   field has the same handle in every block.  The solve is FP64. */
+   freed, so free the decomposition before its blocks.  Every block must
+   create its fields in the same order, so that a field has the same handle
+   in every block.  The solve is FP64. */
 typedef struct bmg_shard bmg_shard;
 int bmg_shard_new (bmg_shard ** shard, bmg_grid * const * blocks, const int * dims,
                    const int * periodic);
