@@ -53,8 +53,9 @@ def load_peaks():
 
 
 # dram__bytes_read.sum + dram__bytes_write.sum of one k_relax_tile2d_w launch on
-# the 2048^2 level (ncu, 68.3 + 5.8 MB)
-TILE_LAUNCH_DRAM_BYTES = 74.1e6
+# the 2048^2 level (ncu, 102.2 + 18.2 MB, the first launch of a cycle's finest
+# level, cold)
+TILE_LAUNCH_DRAM_BYTES = 120.4e6
 
 
 class ClockSampler:

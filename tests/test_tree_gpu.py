@@ -198,6 +198,26 @@ def test_tree_mixed_form_jacobi_reaches_the_tolerance():
     assert rel <= 1e-3, rel
 
 
+def test_tree_mixed_form_needs_the_interpreter():
+    """A tree built without the schedule interpreter (BMG_NO_TREE_INTERP set
+    when it is refined) solves in FP64, and refuses the mixed form with
+    BMG_EUNSUPPORTED instead of computing anything else."""
+    import basilisk_b200 as bmg
+    os.environ["BMG_NO_TREE_INTERP"] = "1"
+    try:
+        t = GpuTree(7, (0.0, 0.0), relax="rbgs", precision="mixed")
+        t.refine(gd.band_refinement(7, 4))
+    finally:
+        os.environ.pop("BMG_NO_TREE_INTERP", None)
+    gd.two_phase_tree(t, seed=2)
+    st = t.g.poisson(t.f[ot.A], t.f[ot.B], alpha=t.alpha, tolerance=1e-6, check_status=False)
+    assert st["status"] == bmg._lib.EUNSUPPORTED, st
+    t.g.set_precision("fp64")
+    st = t.g.poisson(t.f[ot.A], t.f[ot.B], alpha=t.alpha, tolerance=1e-6, check_status=False)
+    assert st["status"] == 0 and st["resa"] <= 1e-6, st
+    t.close()
+
+
 def _cpu_rbgs(depth, origin):
     t = ot.Tree(depth, 1.0, origin)
     t.set_relax(ot.RELAX_RBGS)
