@@ -2,8 +2,11 @@
 discrete solution, and the CUDA path gives the oracle's result bit for bit
 (FP64, same smoother).  The reference's own tests of viscosity () are full
 physics programs (test/axi.c, fall.c, gaussian.c) outside this path, so
-the operator is pinned by restatement (viscosity.h:25-160, in the oracle)
-and checked for consistency here."""
+the operator (viscosity.h:25-160, restated in the oracle) is pinned by a
+closed-form known answer: on a periodic box a sum of Fourier modes is
+mapped by the discrete operator to M U cos(phi) with M the operator's
+symbol, so both the oracle and the CUDA path must return the mode sum from
+its image (fourier_case)."""
 import numpy as np
 import pytest
 
