@@ -189,6 +189,39 @@ __device__ __forceinline__ void put_quad (T * a0, T * a1, int off, const Quad<T>
   *(T2 *) (a1 + off) = o;
 }
 
+/* The bilinear prolongation (multigrid-common.h:124-140) of fine cell
+   (i, j) from the coarse level c (geometry gc, ghosts filled), with
+   k_prolong2d_blk's expression and order, so that a tile launch that
+   stages it instead of the iterate gives the values the prolongation
+   launch would have written (bit-identical in FP64). */
+template <typename T>
+__device__ __forceinline__ T prolong_cell (const T * __restrict__ c, const bmg_geom & gc, int i, int j)
+{
+  const int ci = i >> 1, cj = j >> 1, cx = (i & 1) ? 1 : -1, cy = (j & 1) ? 1 : -1;
+  const T m = c[cidx<2> (gc, ci, cj, 0)], mx = c[cidx<2> (gc, ci + cx, cj, 0)];
+  const T my = c[cidx<2> (gc, ci, cj + cy, 0)], mxy = c[cidx<2> (gc, ci + cx, cj + cy, 0)];
+  return (T(9)*m + T(3)*(mx + my) + mxy)/T(16);
+}
+
+/* the same for the K fine cells (i, j0) .. (i, j0 + K - 1) of one row, j0
+   even: the K/2 + 2 coarse values of the two coarse rows involved read
+   once */
+template <typename T, int K>
+__device__ __forceinline__ void prolong_row (const T * __restrict__ c, const bmg_geom & gc, int i, int j0,
+                                             T * v)
+{
+  const int ci = i >> 1, cx = (i & 1) ? 1 : -1, cb = (j0 >> 1) - 1;
+  const T * c0 = c + cidx<2> (gc, ci, cb, 0), * c1 = c + cidx<2> (gc, ci + cx, cb, 0);
+  T r0[K/2 + 2], r1[K/2 + 2];
+#pragma unroll
+  for (int u = 0; u < K/2 + 2; u++) { r0[u] = c0[u]; r1[u] = c1[u]; }
+#pragma unroll
+  for (int q = 0; q < K; q++) {
+    const int u = 1 + (q >> 1), cy = (q & 1) ? 1 : -1;
+    v[q] = (T(9)*r0[u] + T(3)*(r1[u] + r0[u + cy]) + r1[u + cy])/T(16);
+  }
+}
+
 /* BX x BY threads: thread (tx, ty) updates the CPT = 2 cells 2 tx, 2 tx + 1
    of each colour of row ty + lo in every colour pass; MINB CTAs per SM bound
    the registers */
@@ -502,7 +535,7 @@ __global__ void __launch_bounds__ (tw::BX*tw::BY, 2)
 k_relax_tile2d_w (bmg_geom g, float * __restrict__ out, const float * __restrict__ in,
                   const float * __restrict__ res, Coef<float> ax, Coef<float> ay, Coef<float> lam,
                   float Delta, BCH bc, int nsweeps, double * __restrict__ acor, bmg_geom ga,
-                  bmg_bcdesc abc)
+                  bmg_bcdesc abc, const float * __restrict__ coarse, bmg_geom gc)
 {
   using namespace tw;
   constexpr int H = Tile<TS>::H;
@@ -573,7 +606,27 @@ k_relax_tile2d_w (bmg_geom g, float * __restrict__ out, const float * __restrict
      before the weights are computed, so that both round trips overlap */
   grid_dependency_wait ();
   const int cq = (base + p) & 1;                /* colour of the even columns */
-  if (inner) {
+  if (coarse) {
+    /* the level's first launch: the iterate is the prolongation of the
+       coarse level, computed here instead of by its own launch */
+    if (inner) {
+      float v8[8];
+      prolong_row<float, 8> (coarse, gc, gi, j0 + q0, v8);
+      const Quad<float> va = {v8[0], v8[1], v8[2], v8[3]}, vb = {v8[4], v8[5], v8[6], v8[7]};
+      put_quad (sa + cq*WM, sa + (cq ^ 1)*WM, p*M + m0, va);
+      put_quad (sa + cq*WM, sa + (cq ^ 1)*WM, p*M + m0 + 2, vb);
+    }
+    else {
+      const int ri = real_index (gi, n, px);
+#pragma unroll
+      for (int q = 0; q < 8; q++) {
+        const int rj = real_index (j0 + q0 + q, n, py);
+        sa[((cq + q) & 1)*WM + p*M + ((q0 + q) >> 1)] =
+          ri >= 0 && rj >= 0 ? prolong_cell<float> (coarse, gc, ri, rj) : 0.f;
+      }
+    }
+  }
+  else if (inner) {
     const long long id = cidx<2> (g, gi, j0 + q0, 0);
     const Quad<float> va = load_quad (in + id), vb = load_quad (in + id + 4);
     put_quad (sa + cq*WM, sa + (cq ^ 1)*WM, p*M + m0, va);
@@ -1121,7 +1174,8 @@ template <int TS, bool LAM>
 __global__ void __launch_bounds__ (tx4::BX*tx4::BY, 1)
 k_relax_tile2d_x4 (bmg_geom g, double * __restrict__ out, const double * __restrict__ in,
                    const double * __restrict__ res, Coef<double> ax, Coef<double> ay, Coef<double> lam,
-                   double Delta, BCH bc, int nsweeps, double * __restrict__ acor, bmg_bcdesc abc)
+                   double Delta, BCH bc, int nsweeps, double * __restrict__ acor, bmg_bcdesc abc,
+                   const double * __restrict__ coarse, bmg_geom gc)
 {
   using namespace tx4;
   constexpr int H = (W - TS)/2;
@@ -1180,7 +1234,26 @@ k_relax_tile2d_x4 (bmg_geom g, double * __restrict__ out, const double * __restr
   }
   grid_dependency_wait ();
   const int cq = (base + p) & 1;
-  if (inner) {
+  if (coarse) {
+    /* the level's first launch: the iterate is the prolongation of the
+       coarse level (bit-identical to the prolongation launch) */
+    if (inner) {
+      double v4[4];
+      prolong_row<double, 4> (coarse, gc, gi, j0 + q0, v4);
+      const Quad<double> va = {v4[0], v4[1], v4[2], v4[3]};
+      put_quad (sa + cq*WM, sa + (cq ^ 1)*WM, p*M + m0, va);
+    }
+    else {
+      const int ri = real_index (gi, n, px);
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const int rj = real_index (j0 + q0 + q, n, py);
+        sa[((cq + q) & 1)*WM + p*M + ((q0 + q) >> 1)] =
+          ri >= 0 && rj >= 0 ? prolong_cell<double> (coarse, gc, ri, rj) : 0.;
+      }
+    }
+  }
+  else if (inner) {
     const long long id = cidx<2> (g, gi, j0 + q0, 0);
     const Quad<double> va = load_quad (in + id);
     put_quad (sa + cq*WM, sa + (cq ^ 1)*WM, p*M + m0, va);
@@ -1609,7 +1682,8 @@ int launch_level_cluster_x (bmg_geom g, double * out, const double * res, const 
 template <bool LAM>
 int launch_tile_x4 (bmg_geom g, void * out, const void * in, const void * res,
                     const bmg_coef * alpha, bmg_coef lambda, double Delta, BCH h, int nsweeps,
-                    double * acor, const bmg_bcdesc & abc, cudaStream_t s)
+                    double * acor, const bmg_bcdesc & abc, const void * coarse, bmg_geom gc,
+                    cudaStream_t s)
 {
   using namespace tx4;
   constexpr int TS = 48;
@@ -1627,14 +1701,16 @@ int launch_tile_x4 (bmg_geom g, void * out, const void * in, const void * res,
   return (int) cudaLaunchKernelEx (&cfg, k_relax_tile2d_x4<TS, LAM>, g, (double *) out,
                                    (const double *) in, (const double *) res,
                                    coef_of<double> (alpha[0]), coef_of<double> (alpha[1]),
-                                   coef_of<double> (lambda), Delta, h, nsweeps, acor, abc);
+                                   coef_of<double> (lambda), Delta, h, nsweeps, acor, abc,
+                                   (const double *) coarse, gc);
 }
 
 
 template <int TS, bool LAM>
 int launch_tile_w (bmg_geom g, void * out, const void * in, const void * res,
                    const bmg_coef * alpha, bmg_coef lambda, double Delta, BCH h, int nsweeps,
-                   double * acor, bmg_geom ga, const bmg_bcdesc & abc, cudaStream_t s)
+                   double * acor, bmg_geom ga, const bmg_bcdesc & abc, const void * coarse,
+                   bmg_geom gc, cudaStream_t s)
 {
   using namespace tw;
   cudaLaunchConfig_t cfg;
@@ -1651,7 +1727,8 @@ int launch_tile_w (bmg_geom g, void * out, const void * in, const void * res,
   return (int) cudaLaunchKernelEx (&cfg, k_relax_tile2d_w<TS, LAM>, g, (float *) out, (const float *) in,
                                    (const float *) res, coef_of<float> (alpha[0]),
                                    coef_of<float> (alpha[1]), coef_of<float> (lambda),
-                                   (float) Delta, h, nsweeps, acor, ga, abc);
+                                   (float) Delta, h, nsweeps, acor, ga, abc,
+                                   (const float *) coarse, gc);
 }
 
 /* ---------------------------------------------------------------- */
@@ -2310,13 +2387,21 @@ int bmg_tile_corrects (int st, int n)
   return n > BMG_SMALL_TILE_N;
 }
 
+int bmg_tile_prolongs (int st, int n)
+{
+  (void) st;
+  return n > BMG_SMALL_TILE_N;
+}
+
 int bmg_launch_relax_tile (int dim, int st, bmg_geom g, void * out, const void * in,
                            const void * res, const bmg_coef * alpha, bmg_coef lambda,
                            double Delta, const bmg_bcdesc * bc, int nsweeps, double * acor,
-                           bmg_geom ga, const bmg_bcdesc * abc, cudaStream_t s)
+                           bmg_geom ga, const bmg_bcdesc * abc, const void * coarse, bmg_geom gc,
+                           cudaStream_t s)
 {
   if (dim != 2 || nsweeps < 1 || nsweeps > bmg_tile_sweeps (st, g.n)) return (int) cudaErrorInvalidValue;
   if (acor && (!abc || !bmg_tile_corrects (st, g.n))) return (int) cudaErrorInvalidValue;
+  if (coarse && (!bmg_tile_prolongs (st, g.n) || 2*gc.n != g.n)) return (int) cudaErrorInvalidValue;
   BCH h = bch_of (bc);
   bmg_bcdesc abc0;
   memset (&abc0, 0, sizeof abc0);
@@ -2329,15 +2414,15 @@ int bmg_launch_relax_tile (int dim, int st, bmg_geom g, void * out, const void *
   const bool small = g.n <= BMG_SMALL_TILE_N;
   if (st == BMG_ST_F64)
     e = small ? launch_tile<double, 16, 4, 8, 32> (g, out, in, res, alpha, lambda, Delta, h, nsweeps, s)
-      : lambda.p ? launch_tile_x4<true> (g, out, in, res, alpha, lambda, Delta, h, nsweeps, acor, ab, s)
-      : launch_tile_x4<false> (g, out, in, res, alpha, lambda, Delta, h, nsweeps, acor, ab, s);
+      : lambda.p ? launch_tile_x4<true> (g, out, in, res, alpha, lambda, Delta, h, nsweeps, acor, ab, coarse, gc, s)
+      : launch_tile_x4<false> (g, out, in, res, alpha, lambda, Delta, h, nsweeps, acor, ab, coarse, gc, s);
   else
     e = small ? launch_tile<float, 16, 4, 8, 32> (g, out, in, res, alpha, lambda, Delta, h, nsweeps, s)
       : g.n == BMG_DEEP_TILE_N ?
-        (lambda.p ? launch_tile_w<32, true> (g, out, in, res, alpha, lambda, Delta, h, nsweeps, acor, ga, ab, s)
-                  : launch_tile_w<32, false> (g, out, in, res, alpha, lambda, Delta, h, nsweeps, acor, ga, ab, s))
-      : lambda.p ? launch_tile_w<48, true> (g, out, in, res, alpha, lambda, Delta, h, nsweeps, acor, ga, ab, s)
-      : launch_tile_w<48, false> (g, out, in, res, alpha, lambda, Delta, h, nsweeps, acor, ga, ab, s);
+        (lambda.p ? launch_tile_w<32, true> (g, out, in, res, alpha, lambda, Delta, h, nsweeps, acor, ga, ab, coarse, gc, s)
+                  : launch_tile_w<32, false> (g, out, in, res, alpha, lambda, Delta, h, nsweeps, acor, ga, ab, coarse, gc, s))
+      : lambda.p ? launch_tile_w<48, true> (g, out, in, res, alpha, lambda, Delta, h, nsweeps, acor, ga, ab, coarse, gc, s)
+      : launch_tile_w<48, false> (g, out, in, res, alpha, lambda, Delta, h, nsweeps, acor, ga, ab, coarse, gc, s);
   if (e) return e;
   cudaError_t r = cudaGetLastError ();
   return r == cudaSuccess ? 0 : (int) r;

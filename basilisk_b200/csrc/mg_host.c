@@ -911,33 +911,43 @@ static int cycle_launches (bmg_grid * g, field_t * a, const levels_t * lv, const
         continue;
       }
     }
+    /* the prolongation goes into the level's first tile launch where that
+       launch can stage it (red-black tiles, same storage type) */
+    const int tiled = g->relax == BMG_RELAX_RBGS && dim == 2;
+    const int pfused = tiled && l > minlevel && lv->st[l - 1] == st && bmg_tile_prolongs (st, gl.n);
     if (l == minlevel) {
       /* zero on the coarsest level (poisson.h:54-58) */
       CL (bmg_launch_prolong (dim, st, st, gl, gl, NULL, cur[l], dabc, 1, s));
       bytes += ncells (g, l)*es_of (st);
+      launches++;
     }
+    else if (pfused)
+      bytes += ncells (g, l - 1)*es_of (st);
     else {
       /* bilinear from the coarser level (poisson.h:64-68) */
       const int stc = lv->st[l - 1];
       CL (bmg_launch_prolong (dim, stc, st, geom_st (g, l - 1, stc), gl, cur[l - 1], cur[l], dabc, 0, s));
       bytes += ncells (g, l - 1)*es_of (stc) + ncells (g, l)*es_of (st);
+      launches++;
     }
-    launches++;
     const bmg_coef * al = st == BMG_ST_F64 ? c->alpha64[l] : c->alpha32[l];
     const bmg_coef la = st == BMG_ST_F64 ? c->lambda64[l] : c->lambda32[l];
     const int timed = g->timing && l == L && maxlevel == L;
     if (timed) CK (record_event (g->evr0, s));
-    if (g->relax == BMG_RELAX_RBGS && dim == 2) {
+    if (tiled) {
       /* several complete red-black sweeps per launch, ping-pong buffers;
-         the last launch of the finest level also applies a += da */
+         the first launch of a level stages its prolongation (pfused), the
+         last launch of the finest level also applies a += da */
       const int S = bmg_tile_sweeps (st, gl.n);
       const int fuse = l == L && maxlevel == L && bmg_tile_corrects (st, gl.n);
       for (int done = 0; done < nrelax; ) {
         const int k = nrelax - done < S ? nrelax - done : S;
         const int last = fuse && done + k >= nrelax;
+        const int pro = pfused && done == 0;
         CL (bmg_launch_relax_tile (dim, st, gl, oth[l], cur[l], lv->res[l], al, la,
                                    delta_of (g, l), dabc, k, last ? a->lv[L] : NULL,
-                                   g->g64[L], last ? &abc : NULL, s));
+                                   g->g64[L], last ? &abc : NULL, pro ? cur[l - 1] : NULL,
+                                   geom_st (g, l - 1, st), s));
         void * t = cur[l]; cur[l] = oth[l]; oth[l] = t;
         launches++;
         done += k;

@@ -155,10 +155,18 @@ int bmg_tile_sweeps (int st, int n);   /* sweeps one tile launch can do on an n 
    abc) the launch also does a += out on every cell it writes, with the
    ghost images of a (poisson.h:84-89) */
 int bmg_tile_corrects (int st, int n);
+/* whether the tile launch of an n x n level can stage the level's
+   prolongation itself: with coarse != NULL (the level below, of the same
+   storage type, geometry gc, ghosts filled) the launch relaxes the bilinear
+   prolongation of coarse (multigrid-common.h:124-140, the values
+   bmg_launch_prolong would write) instead of in, so that the level's first
+   launch replaces its prolongation launch */
+int bmg_tile_prolongs (int st, int n);
 int bmg_launch_relax_tile (int dim, int st, bmg_geom g, void * out, const void * in,
                            const void * res, const bmg_coef * alpha, bmg_coef lambda,
                            double Delta, const bmg_bcdesc * bc, int nsweeps, double * acor,
-                           bmg_geom ga, const bmg_bcdesc * abc, cudaStream_t s);
+                           bmg_geom ga, const bmg_bcdesc * abc, const void * coarse, bmg_geom gc,
+                           cudaStream_t s);
 
 /* all nrelax red-black sweeps of a 2D level (FP32: 64^2 to 256^2; FP64,
    bit-identical: 64^2 and 128^2) in one launch of one thread-block

@@ -89,6 +89,9 @@ LARGE = [
     (2, 9, (0, 1), {}, "field", -2.0),
     (2, 8, (1,), {0: ("dirichlet", 1.0), 1: ("neumann", -0.5)}, "field", "field"),
     (2, 10, (0,), {2: ("neumann", 0.0), 3: ("dirichlet", 0.0)}, 1.0, None),
+    # stored lambda on a 512^2 level (its first tile launch stages the
+    # prolongation and lambda), periodic across one axis
+    (2, 9, (1,), {0: ("dirichlet", 0.5), 1: ("neumann", 0.25)}, "field", "field"),
 ]
 
 
